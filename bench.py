@@ -1,0 +1,348 @@
+"""Benchmark: BLS12-381 G1 MSM at n = 2^22 (the headline), one GPU per rank.
+
+A step is one full MSM (sum of 2^22 scalar * point products, uniform Fr
+scalars, points s_i * G1 with seeded s_i) with inputs resident in HBM.
+Inputs are 512 MiB (> 126 MB L2), so no L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is Mpts/s over all ranks (each rank
+runs its own independent MSM: replicas, weak scaling).  `e2e` is the same
+metric through the drop-in C ABI (gpukit_multi_pippenger) from pinned host
+buffers, host<->device copies included.  `--impl reference` times the
+reference's own CPU MSM (gpukit_multi_pippenger_cpu, built from its sources
+into oracle/_ref) on all host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CURVE = 2
+LOGN = 22
+PB = 96
+N_LIMBS = 12
+SM_COUNT = 148
+IMAD_PER_CLK_SM = 64
+
+
+def mont_imad(nlimbs: int) -> int:
+    return 4 * nlimbs * nlimbs + nlimbs
+
+
+def w_msm(n: int, nlimbs: int) -> int:
+    """Algorithmic IMAD of an MSM: 6 Montgomery products per bucket addition
+    (batch-affine), min over c in [4,16] of ceil(256/c) * (n + 2^c)."""
+    best = min(((256 + c - 1) // c) * (n + (1 << c)) for c in range(4, 17))
+    return 6 * mont_imad(nlimbs) * best
+
+
+def load_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            pass
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), parts[4:8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v == "Active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def setup_dist():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v: float) -> float:
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference_msm(pts: bytes, scs: bytes, n: int, threads: int) -> float:
+    """Seconds for the reference CPU MSM (composed over `threads` slices)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import _oracle as O
+    out = ctypes.create_string_buffer(PB)
+    t0 = time.perf_counter()
+    if threads <= 1:
+        rc = O.ref().ref_msm(CURVE, scs, pts, n, out)
+    else:
+        rc = O.ref().ref_msm_parallel(CURVE, scs, pts, n, out, threads)
+    dt = time.perf_counter() - t0
+    assert rc == 0
+    return dt
+
+
+def make_inputs(n: int, seed: int):
+    """Seeded uniform Fr scalars and points s_i * G1 (s_i seeded), on device."""
+    import torch
+    import crypto_b200 as kb
+    sc = kb.gen_scalars(CURVE, seed, n)
+    ks = kb.gen_scalars(CURVE, seed + 1000, n)
+    d_sc = torch.frombuffer(bytearray(sc), dtype=torch.uint8).cuda()
+    d_ks = torch.frombuffer(bytearray(ks), dtype=torch.uint8).cuda()
+    d_pts = torch.empty(n * PB, dtype=torch.uint8, device="cuda")
+    rc = kb.lib().kb200_g1_fixed_base_device(CURVE, d_ks.data_ptr(), n, d_pts.data_ptr(),
+                                             ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0, kb.last_error()
+    torch.cuda.synchronize()
+    del d_ks
+    return d_sc, d_pts
+
+
+def run_reference(args, ws, rank):
+    n_sample = 1 << args.ref_logn
+    threads = os.cpu_count() or 1
+    if rank != 0:
+        return
+    import crypto_b200 as kb
+    d_sc, d_pts = make_inputs(n_sample, seed=1)
+    pts = d_pts.cpu().numpy().tobytes()
+    scs = d_sc.cpu().numpy().tobytes()
+    for _ in range(args.warmup and 1):
+        cpu_reference_msm(pts, scs, n_sample, threads)
+    times = [cpu_reference_msm(pts, scs, n_sample, threads) for _ in range(args.steps)]
+    t = sum(times) / len(times)
+    v = n_sample / t / 1e6
+    line = {
+        "impl": "reference", "metric": "G1 MSM Mpts/s @2^22", "value": v, "unit": "Mpts/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"BLS12-381 G1 MSM, bounded sample n=2^{args.ref_logn} of the "
+                               "2^22 workload (uniform Fr scalars, seeded points)",
+                   "curve": "BLS12-381", "n": n_sample},
+        "cpu_baseline": {"value": v, "unit": "Mpts/s", "cores": threads, "kind": "reference",
+                         "sample": f"gpukit_multi_pippenger_cpu on {threads} contiguous slices of "
+                                   f"n=2^{args.ref_logn}, slice results summed with the reference g1_add"},
+        "e2e": {"value": v, "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    import crypto_b200 as kb
+    n = 1 << args.logn
+    d_sc, d_pts = make_inputs(n, seed=1 + rank)
+    d_out = torch.empty(PB, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    L = kb.lib()
+
+    def step():
+        rc = L.kb200_msm_device(CURVE, d_sc.data_ptr(), d_pts.data_ptr(), n, d_out.data_ptr(), sp)
+        assert rc == 0, kb.last_error()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # correctness spot check of the device path against the C ABI drop-in
+    host_sc = d_sc.cpu().numpy().tobytes()
+    host_pts = d_pts.cpu().numpy().tobytes()
+    want = kb.gpukit_multi_pippenger(CURVE, host_sc, host_pts, n)
+    assert d_out.cpu().numpy().tobytes() == want, "device path differs from C ABI path"
+
+    kb.profile_enable(True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    launches0 = kb.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = kb.launch_count() - launches0
+    barrier(ws)
+    stage = kb.msm_stage_ms(CURVE)
+    kb.profile_enable(False)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = max_over_ranks(ws, ms)
+    value = n * ws / (ms / 1e3) / 1e6
+
+    # e2e through the drop-in C ABI with pinned host buffers
+    h_sc = torch.frombuffer(bytearray(host_sc), dtype=torch.uint8).pin_memory()
+    h_pts = torch.frombuffer(bytearray(host_pts), dtype=torch.uint8).pin_memory()
+    out = ctypes.create_string_buffer(PB)
+    e2e_steps = max(1, min(args.steps, 5))
+    L.gpukit_multi_pippenger(CURVE, ctypes.c_char_p(h_sc.data_ptr()),
+                             ctypes.c_char_p(h_pts.data_ptr()), n, out)
+    barrier(ws)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        rc = L.gpukit_multi_pippenger(CURVE, ctypes.c_char_p(h_sc.data_ptr()),
+                                      ctypes.c_char_p(h_pts.data_ptr()), n, out)
+        assert rc == 0, kb.last_error()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    e2e_ms = max_over_ranks(ws, e2e_ms)
+    assert out.raw == want
+
+    peaks = load_peaks()
+    clocks = clk.summary()
+    sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    peak_imad = SM_COUNT * IMAD_PER_CLK_SM * sm_mhz * 1e6
+    # dominant kernel: bucket accumulation (one launch per MSM)
+    plan_c = kb.msm_window(CURVE, n)
+    windows = (257 + plan_c - 1) // plan_c
+    entries = n * windows * (1 - 2.0 ** -plan_c)
+    acc_ms = stage.get("accumulate")
+    acc_imad = entries * 6 * mont_imad(N_LIMBS)
+    roofline = None
+    if acc_ms and acc_ms > 0:
+        ach = acc_imad / (acc_ms / 1e3)
+        roofline = {"bound": "int", "kernel": "k_accumulate", "achieved": ach / 1e12,
+                    "peak": peak_imad / 1e12, "unit": "TIMAD/s", "frac": ach / peak_imad,
+                    "traffic": None,
+                    "peak_source": f"derived: {SM_COUNT} SMs x {IMAD_PER_CLK_SM} IMAD/clk x "
+                                   f"{sm_mhz:.0f} MHz (MEASURED_PEAKS sm_max_mhz)",
+                    "work_per_launch": f"{entries:.3e} bucket additions x 6 x {mont_imad(N_LIMBS)} IMAD"}
+    msm_w = w_msm(n, N_LIMBS)
+    msm_roof = {"achieved": msm_w / (ms / 1e3) / 1e12, "peak": peak_imad / 1e12, "unit": "TIMAD/s",
+                "frac": msm_w / (ms / 1e3) / peak_imad, "work": f"W_msm(2^{args.logn}) = {msm_w:.3e} IMAD"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        import _oracle as O  # noqa: F401  (tests/ on sys.path inside cpu_reference_msm)
+        ns = 1 << args.ref_logn
+        threads = os.cpu_count() or 1
+        t = cpu_reference_msm(host_pts[:PB * ns], host_sc[:32 * ns], ns, threads)
+        cpu = {"value": ns / t / 1e6, "unit": "Mpts/s", "cores": threads, "kind": "reference",
+               "sample": f"gpukit_multi_pippenger_cpu on {threads} slices of n=2^{args.ref_logn} "
+                         "(first 2^%d inputs of the workload), summed with the reference g1_add" % args.ref_logn}
+
+    if rank == 0:
+        line = {
+            "metric": "G1 MSM Mpts/s @2^22", "value": value, "unit": "Mpts/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic",
+            "config": {"workload": f"BLS12-381 G1 MSM n=2^{args.logn}, uniform Fr scalars, "
+                                   "points s_i*G1 with seeded s_i (fixed-base on device)",
+                       "curve": "BLS12-381", "n": n, "window_bits": plan_c,
+                       "l2": "inputs 512 MiB > L2 (no flush)", "parallelism": f"replicas x{ws}"},
+            "e2e": {"value": n * ws / (e2e_ms / 1e3) / 1e6, "unit": "Mpts/s",
+                    "h2d_bytes_per_step": n * (32 + PB), "d2h_bytes_per_step": PB,
+                    "ms_per_step": e2e_ms, "api": "gpukit_multi_pippenger"},
+            "gpu_launches": launches,
+            "roofline": roofline,
+            "msm_roofline": msm_roof,
+            "stage_ms": stage,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--logn", type=int, default=LOGN)
+    ap.add_argument("--ref-logn", type=int, default=17)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    sys.path.insert(0, str(ROOT / "tests"))
+    ws, rank, local = setup_dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,179 @@
+"""kinet-b200: B200-native polynomial-commitment path (Fr NTT, G1 MSM, KZG).
+
+Thin Python binding over the C ABI in include/kinet_b200/crypto_b200.h.  The
+compute lives in the CUDA library crypto_b200/_lib/libkinet_b200.so; this
+module only marshals bytes.  There is no CPU fallback: loading fails loudly
+if the library is missing, and every call reports the library's error code.
+
+Wire formats (same as the reference's gpukit / crypto C ABI):
+  scalar / Fr element : 32 bytes little-endian
+  G1 point            : x || y big-endian (96 B BLS12-381, 64 B BN254),
+                        all-zero = infinity
+  compressed G1       : 48 bytes (BLS12-381)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+CURVE_BN254 = 1
+CURVE_BLS12_381 = 2
+POINT_BYTES = {CURVE_BN254: 64, CURVE_BLS12_381: 96}
+
+GPUKIT_OK = 0
+CRYPTO_OK = 0
+
+_LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libkinet_b200.so"
+_lib: ctypes.CDLL | None = None
+
+
+class KinetB200Error(RuntimeError):
+    def __init__(self, fn: str, rc: int, msg: str):
+        super().__init__(f"{fn} returned {rc}: {msg}")
+        self.rc = rc
+
+
+def lib() -> ctypes.CDLL:
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        path = os.environ.get("KINET_B200_LIB", str(_LIB_PATH))
+        if not Path(path).exists():
+            raise ImportError(f"kinet-b200 CUDA library not built: {path} "
+                              "(run `python -m crypto_b200.build`)")
+        L = ctypes.CDLL(path)
+        c = ctypes
+        sz, u8p, vp = c.c_size_t, c.c_char_p, c.c_void_p
+        sigs = {
+            "gpukit_multi_pippenger": (c.c_int, [c.c_uint32, u8p, u8p, sz, vp]),
+            "gpukit_multi_pippenger_cuda": (c.c_int, [c.c_uint32, u8p, u8p, sz, vp]),
+            "ntt_fr_forward": (c.c_int, [c.c_int, vp, sz, c.c_int]),
+            "ntt_fr_inverse": (c.c_int, [c.c_int, vp, sz, c.c_int]),
+            "kzg_srs_load_g1": (c.c_int, [u8p, sz]),
+            "kzg_srs_generate_g1": (c.c_int, [u8p, sz]),
+            "kzg_srs_read_g1": (c.c_int, [vp, sz, sz]),
+            "kzg_srs_size": (sz, []),
+            "kzg_commit_fr": (c.c_int, [u8p, sz, vp]),
+            "kzg_commit_batch": (c.c_int, [u8p, c.POINTER(sz), sz, vp]),
+            "kb200_msm_device": (c.c_int, [c.c_uint32, vp, vp, sz, vp, vp]),
+            "kb200_ntt_device": (c.c_int, [c.c_int, vp, sz, c.c_int, c.c_int, sz, vp]),
+            "kb200_g1_fixed_base_device": (c.c_int, [c.c_uint32, vp, sz, vp, vp]),
+            "kb200_fr_powers_device": (c.c_int, [c.c_int, vp, sz, vp, vp]),
+            "kb200_kzg_commit_device": (c.c_int, [vp, sz, vp, vp]),
+            "kb200_gen_scalars": (c.c_int, [c.c_int, c.c_uint64, sz, c.c_int, vp]),
+            "kb200_last_error": (c.c_char_p, []),
+            "kb200_device_available": (c.c_int, []),
+            "kb200_msm_window": (c.c_int, [c.c_uint32, sz]),
+            "kb200_launch_count": (c.c_ulonglong, []),
+            "kb200_profile_enable": (None, [c.c_int]),
+            "kb200_msm_stage_ms": (c.c_int, [c.c_uint32, c.POINTER(c.c_float), c.c_int]),
+        }
+        for name, (res, args) in sigs.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(fn: str, rc: int) -> None:
+    if rc != 0:
+        raise KinetB200Error(fn, rc, lib().kb200_last_error().decode(errors="replace"))
+
+
+def last_error() -> str:
+    return lib().kb200_last_error().decode(errors="replace")
+
+
+def device_available() -> bool:
+    return bool(lib().kb200_device_available())
+
+
+# ---- MSM --------------------------------------------------------------------
+
+def gpukit_multi_pippenger(curve: int, scalars: bytes, points: bytes, n: int) -> bytes:
+    """sum_i scalars[i] * points[i]; mirrors gpukit_multi_pippenger."""
+    out = ctypes.create_string_buffer(POINT_BYTES.get(curve, 96))
+    _check("gpukit_multi_pippenger",
+           lib().gpukit_multi_pippenger(curve, scalars, points, n, out))
+    return out.raw
+
+
+def msm_rc(curve: int, scalars, points, n: int, out) -> int:
+    """Raw call returning the status code (for error-behaviour tests)."""
+    return lib().gpukit_multi_pippenger(curve, scalars, points, n, out)
+
+
+# ---- NTT --------------------------------------------------------------------
+
+def ntt_fr(curve: int, data: bytes, inverse: bool = False, coset: bool = False) -> bytes:
+    n = len(data) // 32
+    buf = ctypes.create_string_buffer(bytes(data), len(data))
+    fn = lib().ntt_fr_inverse if inverse else lib().ntt_fr_forward
+    _check("ntt_fr_inverse" if inverse else "ntt_fr_forward", fn(curve, buf, n, int(coset)))
+    return buf.raw
+
+
+# ---- KZG --------------------------------------------------------------------
+
+def kzg_srs_generate(tau: bytes, n: int) -> None:
+    _check("kzg_srs_generate_g1", lib().kzg_srs_generate_g1(tau, n))
+
+
+def kzg_srs_load(points: bytes) -> None:
+    _check("kzg_srs_load_g1", lib().kzg_srs_load_g1(points, len(points) // 96))
+
+
+def kzg_srs_read(offset: int, count: int) -> bytes:
+    out = ctypes.create_string_buffer(96 * count)
+    _check("kzg_srs_read_g1", lib().kzg_srs_read_g1(out, offset, count))
+    return out.raw
+
+
+def kzg_srs_size() -> int:
+    return int(lib().kzg_srs_size())
+
+
+def kzg_commit(evals: bytes) -> bytes:
+    out = ctypes.create_string_buffer(48)
+    _check("kzg_commit_fr", lib().kzg_commit_fr(evals, len(evals) // 32, out))
+    return out.raw
+
+
+def kzg_commit_batch(evals: bytes, sizes: list[int]) -> list[bytes]:
+    arr = (ctypes.c_size_t * len(sizes))(*sizes)
+    out = ctypes.create_string_buffer(48 * len(sizes))
+    _check("kzg_commit_batch", lib().kzg_commit_batch(evals, arr, len(sizes), out))
+    return [out.raw[48 * i:48 * i + 48] for i in range(len(sizes))]
+
+
+# ---- inputs -----------------------------------------------------------------
+
+def gen_scalars(curve: int, seed: int, n: int, kind: int = 0) -> bytes:
+    """Seeded xorshift64* Fr scalars (kind 0 uniform, 1 skewed)."""
+    out = ctypes.create_string_buffer(32 * n)
+    _check("kb200_gen_scalars", lib().kb200_gen_scalars(curve, seed, n, kind, out))
+    return out.raw
+
+
+def msm_window(curve: int, n: int) -> int:
+    return int(lib().kb200_msm_window(curve, n))
+
+
+def launch_count() -> int:
+    """Kernel launches issued by this library since it was loaded."""
+    return int(lib().kb200_launch_count())
+
+
+def profile_enable(on: bool) -> None:
+    lib().kb200_profile_enable(int(on))
+
+
+MSM_STAGES = ("wire_to_table", "recode", "sort", "accumulate", "fold", "reduce_combine")
+
+
+def msm_stage_ms(curve: int) -> dict[str, float]:
+    buf = (ctypes.c_float * 8)()
+    k = lib().kb200_msm_stage_ms(curve, buf, 8)
+    return {MSM_STAGES[i]: float(buf[i]) for i in range(max(k, 0))}

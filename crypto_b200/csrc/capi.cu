@@ -1,0 +1,429 @@
+// C ABI: host-side glue between the reference-shaped entry points and the
+// device engines.  Per device there is one context (stream, engines, I/O
+// staging, resident SRS) guarded by a mutex.
+#include "../../include/kinet_b200/crypto_b200.h"
+#include "curve.cuh"
+#include "kzg.cuh"
+#include "msm.cuh"
+#include "ntt.cuh"
+#include "runtime.cuh"
+
+#include <atomic>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+
+namespace kb200 {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+static std::atomic<unsigned long long> g_launches{0};
+static std::atomic<bool> g_profile{false};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+bool profiling_enabled() { return g_profile.load(std::memory_order_relaxed); }
+
+struct DeviceCtx {
+    int dev = -1;
+    std::mutex mu;
+    cudaStream_t stream = nullptr;
+    MsmEngine* msm[3] = {nullptr, nullptr, nullptr};
+    NttEngine* ntt[3] = {nullptr, nullptr, nullptr};
+    FixedBase* fb[3] = {nullptr, nullptr, nullptr};
+    DevBuf d_a, d_b, d_out, d_srs, d_tmp;
+    HostBuf h_a, h_b, h_out;
+    size_t srs_n = 0;
+
+    MsmEngine* msm_for(int curve) {
+        if (!msm[curve]) msm[curve] = msm_engine_create(curve);
+        return msm[curve];
+    }
+    NttEngine* ntt_for(int curve) {
+        if (!ntt[curve]) ntt[curve] = ntt_engine_create(curve);
+        return ntt[curve];
+    }
+    FixedBase* fb_for(int curve) {
+        if (!fb[curve]) fb[curve] = fixed_base_create(curve, stream);
+        return fb[curve];
+    }
+};
+
+static std::mutex g_ctx_mu;
+static std::map<int, std::unique_ptr<DeviceCtx>> g_ctx;
+
+static DeviceCtx* get_ctx() {
+    int count = 0;
+    cudaError_t err = cudaGetDeviceCount(&count);
+    if (err != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        throw CudaError(err == cudaSuccess ? cudaErrorNoDevice : err,
+                        "no usable CUDA device (kinet-b200 has no CPU fallback)");
+    }
+    int dev = 0;
+    KB_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    auto& slot = g_ctx[dev];
+    if (!slot) {
+        auto c = std::make_unique<DeviceCtx>();
+        c->dev = dev;
+        KB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        slot = std::move(c);
+    }
+    return slot.get();
+}
+
+// Runs fn, mapping exceptions to the given error codes.
+template <class Fn>
+static int guarded(int backend_err, int size_err, int internal_err, Fn&& fn) {
+    try {
+        return fn();
+    } catch (const CudaError& e) {
+        set_last_error(e.what());
+        return backend_err;
+    } catch (const std::invalid_argument& e) {
+        set_last_error(e.what());
+        return size_err;
+    } catch (const std::bad_alloc& e) {
+        set_last_error("host allocation failed");
+        return internal_err;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return internal_err;
+    }
+}
+
+static int wire_bytes(uint32_t curve) { return curve == 2 ? 96 : 64; }
+
+static bool is_pow2(size_t n) { return n && !(n & (n - 1)); }
+
+// ---- MSM -------------------------------------------------------------------
+
+static int msm_host(uint32_t curve, const uint8_t* scalars, const uint8_t* points, size_t n,
+                    uint8_t* result) {
+    if (!result) return KB200_GPUKIT_ERR_NULL_ARG;
+    if (n > 0 && (!scalars || !points)) return KB200_GPUKIT_ERR_NULL_ARG;
+    if (curve == 0 || curve == 3) {
+        set_last_error("curve has no GPU body in kinet-b200 (secp256k1 / banderwagon)");
+        return KB200_GPUKIT_ERR_NOTIMPL;
+    }
+    if (curve != 1 && curve != 2) return KB200_GPUKIT_ERR_BACKEND;
+    return guarded(KB200_GPUKIT_ERR_DISPATCH, KB200_GPUKIT_ERR_BAD_SIZE, KB200_GPUKIT_ERR_DISPATCH,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       const size_t pb = (size_t)wire_bytes(curve);
+                       cudaStream_t st = c->stream;
+                       c->d_a.reserve(n * 32 + 16, st);
+                       c->d_b.reserve(n * pb + 16, st);
+                       c->d_out.reserve(256, st);
+                       c->h_out.reserve(256, st);
+                       if (n) {
+                           KB_CUDA(cudaMemcpyAsync(c->d_a.ptr, scalars, n * 32,
+                                                   cudaMemcpyHostToDevice, st));
+                           KB_CUDA(cudaMemcpyAsync(c->d_b.ptr, points, n * pb,
+                                                   cudaMemcpyHostToDevice, st));
+                       }
+                       MsmOptions opt;
+                       opt.ref_carry_quirk = true;
+                       msm_run_wire(c->msm_for((int)curve), c->d_a.as<uint8_t>(),
+                                    c->d_b.as<uint8_t>(), n, c->d_out.as<uint8_t>(), nullptr, st,
+                                    opt);
+                       KB_CUDA(cudaMemcpyAsync(c->h_out.ptr, c->d_out.ptr, pb,
+                                               cudaMemcpyDeviceToHost, st));
+                       KB_CUDA(cudaStreamSynchronize(st));
+                       std::memcpy(result, c->h_out.ptr, pb);
+                       return KB200_GPUKIT_OK;
+                   });
+}
+
+// ---- NTT -------------------------------------------------------------------
+
+static int ntt_host(int curve, uint8_t* data, size_t n, int inverse, int coset) {
+    if (!data) return KB200_CRYPTO_ERR_INPUT;
+    if (curve != 1 && curve != 2) return KB200_CRYPTO_ERR_INPUT;
+    if (!is_pow2(n) || n > ((size_t)1 << ntt_max_log(curve))) return KB200_CRYPTO_ERR_LENGTH;
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_LENGTH, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       cudaStream_t st = c->stream;
+                       c->d_a.reserve(n * 32 + 16, st);
+                       KB_CUDA(cudaMemcpyAsync(c->d_a.ptr, data, n * 32, cudaMemcpyHostToDevice, st));
+                       ntt_run(c->ntt_for(curve), c->d_a.as<uint32_t>(), n, inverse, coset, 1, st);
+                       KB_CUDA(cudaMemcpyAsync(data, c->d_a.ptr, n * 32, cudaMemcpyDeviceToHost, st));
+                       KB_CUDA(cudaStreamSynchronize(st));
+                       return KB200_CRYPTO_OK;
+                   });
+}
+
+// ---- KZG -------------------------------------------------------------------
+
+static void commit_on_device(DeviceCtx* c, uint32_t* d_evals, size_t n, uint8_t* d_out48,
+                             cudaStream_t st) {
+    if (!is_pow2(n)) throw std::invalid_argument("kzg: n must be a power of two");
+    if (n > c->srs_n) throw std::invalid_argument("kzg: SRS shorter than the polynomial");
+    ntt_run(c->ntt_for(2), d_evals, n, /*inverse=*/1, /*coset=*/0, 1, st);
+    c->d_tmp.reserve(256, st);
+    MsmOptions opt;
+    msm_run_table(c->msm_for(2), reinterpret_cast<const uint8_t*>(d_evals),
+                  c->d_srs.as<uint32_t>(), n, c->d_tmp.as<uint8_t>(), d_out48, st, opt);
+}
+
+}  // namespace kb200
+
+using namespace kb200;
+
+extern "C" {
+
+int gpukit_multi_pippenger(uint32_t curve, const uint8_t* scalars, const uint8_t* points, size_t n,
+                           uint8_t* result) {
+    return msm_host(curve, scalars, points, n, result);
+}
+
+int gpukit_multi_pippenger_cuda(uint32_t curve, const uint8_t* scalars, const uint8_t* points,
+                                size_t n, uint8_t* result) {
+    return msm_host(curve, scalars, points, n, result);
+}
+
+int ntt_fr_forward(int curve, uint8_t* coeffs32le, size_t n, int coset) {
+    return ntt_host(curve, coeffs32le, n, 0, coset);
+}
+
+int ntt_fr_inverse(int curve, uint8_t* coeffs32le, size_t n, int coset) {
+    return ntt_host(curve, coeffs32le, n, 1, coset);
+}
+
+int kzg_srs_load_g1(const uint8_t* points96be, size_t n) {
+    if (!points96be && n) return KB200_CRYPTO_ERR_INPUT;
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_LENGTH, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       cudaStream_t st = c->stream;
+                       c->d_b.reserve(n * 96 + 16, st);
+                       c->d_srs.reserve(n * (size_t)table_words(2) * 4 + 16, st);
+                       if (n) {
+                           KB_CUDA(cudaMemcpyAsync(c->d_b.ptr, points96be, n * 96,
+                                                   cudaMemcpyHostToDevice, st));
+                           points_wire_to_table(2, c->d_b.as<uint8_t>(), c->d_srs.as<uint32_t>(), n, st);
+                       }
+                       KB_CUDA(cudaStreamSynchronize(st));
+                       c->srs_n = n;
+                       return KB200_CRYPTO_OK;
+                   });
+}
+
+int kzg_srs_generate_g1(const uint8_t tau32le[32], size_t n) {
+    if (!tau32le) return KB200_CRYPTO_ERR_INPUT;
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_LENGTH, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       cudaStream_t st = c->stream;
+                       c->d_a.reserve(n * 32 + 64, st);
+                       c->d_srs.reserve(n * (size_t)table_words(2) * 4 + 16, st);
+                       uint8_t* d_tau = c->d_a.as<uint8_t>() + n * 32;
+                       KB_CUDA(cudaMemcpyAsync(d_tau, tau32le, 32, cudaMemcpyHostToDevice, st));
+                       fr_powers(2, d_tau, n, c->d_a.as<uint8_t>(), st);
+                       fixed_base_mul(c->fb_for(2), c->d_a.as<uint8_t>(), n, c->d_srs.as<uint32_t>(),
+                                      nullptr, st);
+                       KB_CUDA(cudaStreamSynchronize(st));
+                       c->srs_n = n;
+                       return KB200_CRYPTO_OK;
+                   });
+}
+
+int kzg_srs_read_g1(uint8_t* points96be, size_t offset, size_t count) {
+    if (!points96be && count) return KB200_CRYPTO_ERR_INPUT;
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_LENGTH, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       if (offset + count > c->srs_n) return KB200_CRYPTO_ERR_LENGTH;
+                       cudaStream_t st = c->stream;
+                       c->d_b.reserve(count * 96 + 16, st);
+                       points_table_to_wire(2, c->d_srs.as<uint32_t>() + offset * table_words(2),
+                                            c->d_b.as<uint8_t>(), count, st);
+                       KB_CUDA(cudaMemcpyAsync(points96be, c->d_b.ptr, count * 96,
+                                               cudaMemcpyDeviceToHost, st));
+                       KB_CUDA(cudaStreamSynchronize(st));
+                       return KB200_CRYPTO_OK;
+                   });
+}
+
+size_t kzg_srs_size(void) {
+    try {
+        DeviceCtx* c = get_ctx();
+        std::lock_guard<std::mutex> lk(c->mu);
+        return c->srs_n;
+    } catch (...) {
+        return 0;
+    }
+}
+
+int kzg_commit_fr(const uint8_t* evals32le, size_t n, uint8_t commit48[48]) {
+    if (!evals32le || !commit48) return KB200_CRYPTO_ERR_INPUT;
+    if (!is_pow2(n)) return KB200_CRYPTO_ERR_LENGTH;
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_LENGTH, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       if (n > c->srs_n) return KB200_CRYPTO_ERR_LENGTH;
+                       cudaStream_t st = c->stream;
+                       c->d_a.reserve(n * 32 + 16, st);
+                       c->d_out.reserve(256, st);
+                       c->h_out.reserve(256, st);
+                       KB_CUDA(cudaMemcpyAsync(c->d_a.ptr, evals32le, n * 32,
+                                               cudaMemcpyHostToDevice, st));
+                       commit_on_device(c, c->d_a.as<uint32_t>(), n, c->d_out.as<uint8_t>(), st);
+                       KB_CUDA(cudaMemcpyAsync(c->h_out.ptr, c->d_out.ptr, 48,
+                                               cudaMemcpyDeviceToHost, st));
+                       KB_CUDA(cudaStreamSynchronize(st));
+                       std::memcpy(commit48, c->h_out.ptr, 48);
+                       return KB200_CRYPTO_OK;
+                   });
+}
+
+int kzg_commit_batch(const uint8_t* evals32le, const size_t* sizes, size_t count,
+                     uint8_t* commits48) {
+    if (count && (!evals32le || !sizes || !commits48)) return KB200_CRYPTO_ERR_INPUT;
+    size_t total = 0;
+    for (size_t i = 0; i < count; ++i) {
+        if (!is_pow2(sizes[i])) return KB200_CRYPTO_ERR_LENGTH;
+        total += sizes[i];
+    }
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_LENGTH, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       for (size_t i = 0; i < count; ++i)
+                           if (sizes[i] > c->srs_n) return KB200_CRYPTO_ERR_LENGTH;
+                       cudaStream_t st = c->stream;
+                       c->d_a.reserve(total * 32 + 16, st);
+                       c->d_out.reserve(count * 48 + 256, st);
+                       c->h_out.reserve(count * 48 + 256, st);
+                       if (total)
+                           KB_CUDA(cudaMemcpyAsync(c->d_a.ptr, evals32le, total * 32,
+                                                   cudaMemcpyHostToDevice, st));
+                       size_t off = 0;
+                       for (size_t i = 0; i < count; ++i) {
+                           commit_on_device(c, c->d_a.as<uint32_t>() + off * 8, sizes[i],
+                                            c->d_out.as<uint8_t>() + 48 * i, st);
+                           off += sizes[i];
+                       }
+                       KB_CUDA(cudaMemcpyAsync(c->h_out.ptr, c->d_out.ptr, count * 48,
+                                               cudaMemcpyDeviceToHost, st));
+                       KB_CUDA(cudaStreamSynchronize(st));
+                       std::memcpy(commits48, c->h_out.ptr, count * 48);
+                       return KB200_CRYPTO_OK;
+                   });
+}
+
+int kb200_msm_device(uint32_t curve, const void* d_scalars, const void* d_points, size_t n,
+                     void* d_result, void* stream) {
+    if (!d_result || (n && (!d_scalars || !d_points))) return KB200_GPUKIT_ERR_NULL_ARG;
+    if (curve != 1 && curve != 2) return KB200_GPUKIT_ERR_BACKEND;
+    return guarded(KB200_GPUKIT_ERR_DISPATCH, KB200_GPUKIT_ERR_BAD_SIZE, KB200_GPUKIT_ERR_DISPATCH,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       MsmOptions opt;
+                       opt.ref_carry_quirk = true;
+                       msm_run_wire(c->msm_for((int)curve), (const uint8_t*)d_scalars,
+                                    (const uint8_t*)d_points, n, (uint8_t*)d_result, nullptr,
+                                    (cudaStream_t)stream, opt);
+                       return KB200_GPUKIT_OK;
+                   });
+}
+
+int kb200_ntt_device(int curve, void* d_data, size_t n, int inverse, int coset, size_t batch,
+                     void* stream) {
+    if (!d_data) return KB200_CRYPTO_ERR_INPUT;
+    if (curve != 1 && curve != 2) return KB200_CRYPTO_ERR_INPUT;
+    if (!is_pow2(n) || n > ((size_t)1 << ntt_max_log(curve))) return KB200_CRYPTO_ERR_LENGTH;
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_LENGTH, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       ntt_run(c->ntt_for(curve), (uint32_t*)d_data, n, inverse, coset, batch,
+                               (cudaStream_t)stream);
+                       return KB200_CRYPTO_OK;
+                   });
+}
+
+int kb200_g1_fixed_base_device(uint32_t curve, const void* d_scalars, size_t n,
+                               void* d_out_points, void* stream) {
+    if (n && (!d_scalars || !d_out_points)) return KB200_GPUKIT_ERR_NULL_ARG;
+    if (curve != 1 && curve != 2) return KB200_GPUKIT_ERR_BACKEND;
+    return guarded(KB200_GPUKIT_ERR_DISPATCH, KB200_GPUKIT_ERR_BAD_SIZE, KB200_GPUKIT_ERR_DISPATCH,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       FixedBase* fb = c->fb_for((int)curve);
+                       fixed_base_mul(fb, (const uint8_t*)d_scalars, n, nullptr,
+                                      (uint8_t*)d_out_points, (cudaStream_t)stream);
+                       return KB200_GPUKIT_OK;
+                   });
+}
+
+int kb200_fr_powers_device(int curve, const void* d_tau, size_t n, void* d_out, void* stream) {
+    if (n && (!d_tau || !d_out)) return KB200_CRYPTO_ERR_INPUT;
+    if (curve != 1 && curve != 2) return KB200_CRYPTO_ERR_INPUT;
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_LENGTH, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       fr_powers(curve, (const uint8_t*)d_tau, n, (uint8_t*)d_out,
+                                 (cudaStream_t)stream);
+                       return KB200_CRYPTO_OK;
+                   });
+}
+
+int kb200_kzg_commit_device(void* d_evals, size_t n, void* d_commit48, void* stream) {
+    if (!d_evals || !d_commit48) return KB200_CRYPTO_ERR_INPUT;
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_LENGTH, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       commit_on_device(c, (uint32_t*)d_evals, n, (uint8_t*)d_commit48,
+                                        (cudaStream_t)stream);
+                       return KB200_CRYPTO_OK;
+                   });
+}
+
+const char* kb200_last_error(void) { return g_last_error.c_str(); }
+
+int kb200_device_available(void) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return count > 0 ? 1 : 0;
+}
+
+unsigned long long kb200_launch_count(void) { return g_launches.load(); }
+
+void kb200_profile_enable(int on) { g_profile.store(on != 0); }
+
+int kb200_msm_stage_ms(uint32_t curve, float* out, int max) {
+    if (!out || max <= 0 || (curve != 1 && curve != 2)) return -1;
+    try {
+        DeviceCtx* c = get_ctx();
+        std::lock_guard<std::mutex> lk(c->mu);
+        if (!c->msm[curve]) return 0;
+        return msm_stage_ms(c->msm[curve], out, max);
+    } catch (...) {
+        return -1;
+    }
+}
+
+int kb200_msm_window(uint32_t curve, size_t n) {
+    MsmOptions opt;
+    return make_msm_plan((int)curve, n, opt).c;
+}
+
+}  // extern "C"

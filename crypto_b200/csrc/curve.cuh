@@ -1,0 +1,278 @@
+// G1 group arithmetic on device for the two a = 0 short-Weierstrass curves:
+//   BLS12-381 G1 : y^2 = x^3 + 4 over FpBLS   (bls/cpp/bls12_381_g1.hpp)
+//   BN254 G1     : y^2 = x^3 + 3 over FpBN    (bn254/cpp/bn254_g1.hpp)
+//
+// Coordinates: accumulators are extended Jacobian "XYZZ" points
+// (x = X/ZZ, y = Y/ZZZ, ZZ^3 = ZZZ^2, infinity <=> ZZ = 0), using the
+// published Explicit-Formulas-Database formulas madd-2008-s, add-2008-s,
+// dbl-2008-s-1 and mdbl-2008-s-1 for a = 0.  Inputs are affine points in
+// Montgomery form.  Exceptional cases (P = Q, P = -Q, infinity operands) are
+// handled explicitly, so every result is the exact group element; the final
+// affine encoding is therefore identical to the reference's Jacobian path.
+#pragma once
+#include "field.cuh"
+
+namespace kb200 {
+
+struct G1BLS {
+    using F = FpBLS;
+    static constexpr uint32_t B = 4;
+    static constexpr int WIRE = 96;  // x || y, 48-byte big-endian each
+    static constexpr int CURVE_ID = 2;
+};
+struct G1BN {
+    using F = FpBN;
+    static constexpr uint32_t B = 3;
+    static constexpr int WIRE = 64;  // x || y, 32-byte big-endian each
+    static constexpr int CURVE_ID = 1;
+};
+
+template <class F>
+struct Affine {
+    Fe<F> x, y;
+};
+template <class F>
+struct Xyzz {
+    Fe<F> X, Y, ZZ, ZZZ;
+};
+
+// Internal affine table entries are 2N words (x then y, Montgomery form).
+// The top bit of x's most significant word flags the point at infinity; it
+// is free because every modulus here is below 2^(32N - 1).
+constexpr uint32_t INF_FLAG = 0x80000000u;
+
+template <class F>
+KB_DEV bool aff_is_inf_words(const uint32_t* w) {
+    return (w[F::N - 1] & INF_FLAG) != 0;
+}
+
+template <class F>
+KB_DEV void xyzz_set_inf(Xyzz<F>& p) {
+    fe_zero(p.X);
+    fe_zero(p.Y);
+    fe_zero(p.ZZ);
+    fe_zero(p.ZZZ);
+}
+template <class F>
+KB_DEV bool xyzz_is_inf(const Xyzz<F>& p) {
+    return fe_is_zero(p.ZZ);
+}
+template <class F>
+KB_DEV void xyzz_from_affine(Xyzz<F>& p, const Affine<F>& a) {
+    p.X = a.x;
+    p.Y = a.y;
+    fe_one(p.ZZ);
+    fe_one(p.ZZZ);
+}
+
+// dbl-2008-s-1 with a = 0.
+template <class F>
+KB_DEV void xyzz_dbl(Xyzz<F>& r, const Xyzz<F>& p) {
+    Fe<F> U, V, W, S, M, t;
+    fe_dbl(U, p.Y);
+    fe_sqr(V, U);
+    fe_mul(W, U, V);
+    fe_mul(S, p.X, V);
+    fe_sqr(t, p.X);
+    fe_dbl(M, t);
+    fe_add(M, M, t);
+    Fe<F> X3, Y3;
+    fe_sqr(X3, M);
+    fe_sub(X3, X3, S);
+    fe_sub(X3, X3, S);
+    fe_sub(t, S, X3);
+    fe_mul(Y3, M, t);
+    fe_mul(t, W, p.Y);
+    fe_sub(Y3, Y3, t);
+    fe_mul(r.ZZ, V, p.ZZ);
+    fe_mul(r.ZZZ, W, p.ZZZ);
+    r.X = X3;
+    r.Y = Y3;
+}
+
+// mdbl-2008-s-1: r = 2 * (affine a).
+template <class F>
+KB_DEV void xyzz_mdbl(Xyzz<F>& r, const Affine<F>& a) {
+    Fe<F> U, V, W, S, M, t;
+    fe_dbl(U, a.y);
+    fe_sqr(V, U);
+    fe_mul(W, U, V);
+    fe_mul(S, a.x, V);
+    fe_sqr(t, a.x);
+    fe_dbl(M, t);
+    fe_add(M, M, t);
+    fe_sqr(r.X, M);
+    fe_sub(r.X, r.X, S);
+    fe_sub(r.X, r.X, S);
+    fe_sub(t, S, r.X);
+    fe_mul(r.Y, M, t);
+    fe_mul(t, W, a.y);
+    fe_sub(r.Y, r.Y, t);
+    r.ZZ = V;
+    r.ZZZ = W;
+}
+
+// madd-2008-s: p += a, with a a finite affine point.
+template <class F>
+KB_DEV void xyzz_add_affine(Xyzz<F>& p, const Affine<F>& a) {
+    if (xyzz_is_inf(p)) {
+        xyzz_from_affine(p, a);
+        return;
+    }
+    Fe<F> U2, S2, P, R;
+    fe_mul(U2, a.x, p.ZZ);
+    fe_mul(S2, a.y, p.ZZZ);
+    fe_sub(P, U2, p.X);
+    fe_sub(R, S2, p.Y);
+    if (fe_is_zero(P)) {
+        if (fe_is_zero(R))
+            xyzz_mdbl(p, a);
+        else
+            xyzz_set_inf(p);
+        return;
+    }
+    Fe<F> PP, PPP, Q, t;
+    fe_sqr(PP, P);
+    fe_mul(PPP, P, PP);
+    fe_mul(Q, p.X, PP);
+    Fe<F> X3;
+    fe_sqr(X3, R);
+    fe_sub(X3, X3, PPP);
+    fe_sub(X3, X3, Q);
+    fe_sub(X3, X3, Q);
+    fe_sub(t, Q, X3);
+    fe_mul(t, R, t);
+    Fe<F> Y3;
+    fe_mul(Y3, p.Y, PPP);
+    fe_sub(Y3, t, Y3);
+    fe_mul(p.ZZ, p.ZZ, PP);
+    fe_mul(p.ZZZ, p.ZZZ, PPP);
+    p.X = X3;
+    p.Y = Y3;
+}
+
+// add-2008-s: p += q, both XYZZ (either may be infinity).
+template <class F>
+KB_DEV void xyzz_add(Xyzz<F>& p, const Xyzz<F>& q) {
+    if (xyzz_is_inf(q)) return;
+    if (xyzz_is_inf(p)) {
+        p = q;
+        return;
+    }
+    Fe<F> U1, U2, S1, S2, P, R;
+    fe_mul(U1, p.X, q.ZZ);
+    fe_mul(U2, q.X, p.ZZ);
+    fe_mul(S1, p.Y, q.ZZZ);
+    fe_mul(S2, q.Y, p.ZZZ);
+    fe_sub(P, U2, U1);
+    fe_sub(R, S2, S1);
+    if (fe_is_zero(P)) {
+        if (fe_is_zero(R))
+            xyzz_dbl(p, p);
+        else
+            xyzz_set_inf(p);
+        return;
+    }
+    Fe<F> PP, PPP, Q, t;
+    fe_sqr(PP, P);
+    fe_mul(PPP, P, PP);
+    fe_mul(Q, U1, PP);
+    Fe<F> X3;
+    fe_sqr(X3, R);
+    fe_sub(X3, X3, PPP);
+    fe_sub(X3, X3, Q);
+    fe_sub(X3, X3, Q);
+    fe_sub(t, Q, X3);
+    fe_mul(t, R, t);
+    Fe<F> Y3;
+    fe_mul(Y3, S1, PPP);
+    fe_sub(Y3, t, Y3);
+    fe_mul(p.ZZ, p.ZZ, q.ZZ);
+    fe_mul(p.ZZ, p.ZZ, PP);
+    fe_mul(p.ZZZ, p.ZZZ, q.ZZZ);
+    fe_mul(p.ZZZ, p.ZZZ, PPP);
+    p.X = X3;
+    p.Y = Y3;
+}
+
+template <class F>
+KB_DEV void xyzz_neg(Xyzz<F>& p) {
+    fe_neg(p.Y, p.Y);
+}
+
+// Affine result (Montgomery form); returns false for infinity.
+template <class F>
+KB_DEV bool xyzz_to_affine(Affine<F>& a, const Xyzz<F>& p) {
+    if (xyzz_is_inf(p)) return false;
+    Fe<F> t, inv;
+    fe_mul(t, p.ZZ, p.ZZZ);
+    fe_inv(inv, t);           // 1 / (ZZ * ZZZ)
+    Fe<F> izz, izzz;
+    fe_mul(izz, inv, p.ZZZ);  // 1 / ZZ
+    fe_mul(izzz, inv, p.ZZ);  // 1 / ZZZ
+    fe_mul(a.x, p.X, izz);
+    fe_mul(a.y, p.Y, izzz);
+    return true;
+}
+
+// Memory helpers for XYZZ points stored as 4N consecutive words.
+template <class F>
+KB_DEV void xyzz_load(Xyzz<F>& p, const uint32_t* w) {
+    fe_load(p.X, w);
+    fe_load(p.Y, w + F::N);
+    fe_load(p.ZZ, w + 2 * F::N);
+    fe_load(p.ZZZ, w + 3 * F::N);
+}
+template <class F>
+KB_DEV void xyzz_store(uint32_t* w, const Xyzz<F>& p) {
+    fe_store(w, p.X);
+    fe_store(w + F::N, p.Y);
+    fe_store(w + 2 * F::N, p.ZZ);
+    fe_store(w + 3 * F::N, p.ZZZ);
+}
+
+// Affine table entry (2N words) -> Affine<F>; the infinity flag is masked.
+template <class F>
+KB_DEV void aff_load(Affine<F>& a, const uint32_t* w) {
+    fe_load(a.x, w);
+    a.x.v[F::N - 1] &= ~INF_FLAG;
+    fe_load(a.y, w + F::N);
+}
+
+// Wire (big-endian x || y, all-zero = infinity) -> internal table entry.
+template <class C>
+KB_DEV void wire_to_table(uint32_t* dst, const uint8_t* wire) {
+    using F = typename C::F;
+    uint32_t any = 0;
+    for (int i = 0; i < C::WIRE; ++i) any |= wire[i];
+    if (!any) {
+        for (int i = 0; i < 2 * F::N; ++i) dst[i] = 0;
+        dst[F::N - 1] = INF_FLAG;
+        return;
+    }
+    Fe<F> x, y;
+    fe_from_be_bytes(x, wire);
+    fe_from_be_bytes(y, wire + F::BYTES);
+    fe_to_mont(x, x);
+    fe_to_mont(y, y);
+    fe_store(dst, x);
+    fe_store(dst + F::N, y);
+}
+
+// XYZZ -> wire bytes (canonical affine big-endian, zeros for infinity).
+template <class C>
+KB_DEV void xyzz_to_wire(uint8_t* wire, const Xyzz<typename C::F>& p) {
+    using F = typename C::F;
+    Affine<F> a;
+    if (!xyzz_to_affine(a, p)) {
+        for (int i = 0; i < C::WIRE; ++i) wire[i] = 0;
+        return;
+    }
+    Fe<F> x, y;
+    fe_from_mont(x, a.x);
+    fe_from_mont(y, a.y);
+    fe_to_be_bytes(wire, x);
+    fe_to_be_bytes(wire + F::BYTES, y);
+}
+
+}  // namespace kb200

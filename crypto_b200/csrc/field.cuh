@@ -1,0 +1,387 @@
+// Montgomery field arithmetic on 32-bit limbs for sm_100a.
+//
+// Four prime fields, all with R = 2^(32N) (the same Montgomery domain as the
+// reference's 64-bit-limb code, so Montgomery images are bit-identical):
+//   FpBLS : BLS12-381 base field, N = 12   (bls/cpp/bls12_381_fp.hpp:83-98)
+//   FrBLS : BLS12-381 scalar field, N = 8  (kzg/cpp/kzg_oracle.hpp:66-90)
+//   FpBN  : BN254 base field, N = 8        (bn254/cpp/bn254_fp.hpp:75-89)
+//   FrBN  : BN254 scalar field, N = 8      (bn254/cpp/bn254_fp.hpp:79-97)
+//
+// Multiplication is CIOS (operand scanning): for each word b_i of b, the
+// product row a*b_i and the reduction row m*p are each accumulated as two
+// carry chains -- the even-indexed partial products (lo into t[j], hi into
+// t[j+1]) and then the odd-indexed ones -- written as consecutive
+// mad.lo.cc / madc.hi.cc instructions, so every row is 4N + 3 integer
+// multiply-adds and the whole product is 4N^2 + 3N of them.  Every value is
+// kept fully reduced in [0, p); all four moduli satisfy 2p < 2^(32N), which
+// is what lets the accumulator live in N+1 words with no overflow word.
+#pragma once
+#include <cstdint>
+
+#define KB_DEV __device__ __forceinline__
+#define KB_HD __host__ __device__ __forceinline__
+
+namespace kb200 {
+
+// ---------------------------------------------------------------------------
+// PTX carry-chain primitives.  volatile keeps the compiler from moving them
+// relative to one another, so a chain written as consecutive calls stays a
+// chain on the condition-code register.
+// ---------------------------------------------------------------------------
+KB_DEV uint32_t mad_lo_cc(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t r;
+    asm volatile("mad.lo.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+    return r;
+}
+KB_DEV uint32_t madc_lo_cc(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t r;
+    asm volatile("madc.lo.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+    return r;
+}
+KB_DEV uint32_t madc_hi_cc(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t r;
+    asm volatile("madc.hi.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+    return r;
+}
+KB_DEV uint32_t addc_u32(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm volatile("addc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+KB_DEV uint32_t add_cc(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+KB_DEV uint32_t addc_cc(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+KB_DEV uint32_t sub_cc(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm volatile("sub.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+KB_DEV uint32_t subc_cc(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm volatile("subc.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+KB_DEV uint32_t subc_u32(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm volatile("subc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// Field parameters.  Limbs are little-endian 32-bit words.
+// ---------------------------------------------------------------------------
+struct FpBLS {
+    static constexpr int N = 12;
+    static constexpr int BYTES = 48;
+    static constexpr uint32_t M0 = 0xfffcfffdu;  // -p^-1 mod 2^32
+    KB_HD static constexpr uint32_t P(int i) {
+        constexpr uint32_t t[12] = {0xffffaaab, 0xb9feffff, 0xb153ffff, 0x1eabfffe,
+                                    0xf6b0f624, 0x6730d2a0, 0xf38512bf, 0x64774b84,
+                                    0x434bacd7, 0x4b1ba7b6, 0x397fe69a, 0x1a0111ea};
+        return t[i];
+    }
+    KB_HD static constexpr uint32_t R1(int i) {
+        constexpr uint32_t t[12] = {0x0002fffd, 0x76090000, 0xc40c0002, 0xebf4000b,
+                                    0x53c758ba, 0x5f489857, 0x70525745, 0x77ce5853,
+                                    0xa256ec6d, 0x5c071a97, 0xfa80e493, 0x15f65ec3};
+        return t[i];
+    }
+    KB_HD static constexpr uint32_t R2(int i) {
+        constexpr uint32_t t[12] = {0x1c341746, 0xf4df1f34, 0x09d104f1, 0x0a76e6a6,
+                                    0x4c95b6d5, 0x8de5476c, 0x939d83c0, 0x67eb88a9,
+                                    0xb519952d, 0x9a793e85, 0x92cae3aa, 0x11988fe5};
+        return t[i];
+    }
+};
+
+struct FrBLS {
+    static constexpr int N = 8;
+    static constexpr int BYTES = 32;
+    static constexpr uint32_t M0 = 0xffffffffu;
+    KB_HD static constexpr uint32_t P(int i) {
+        constexpr uint32_t t[8] = {0x00000001, 0xffffffff, 0xfffe5bfe, 0x53bda402,
+                                   0x09a1d805, 0x3339d808, 0x299d7d48, 0x73eda753};
+        return t[i];
+    }
+    KB_HD static constexpr uint32_t R1(int i) {
+        constexpr uint32_t t[8] = {0xfffffffe, 0x00000001, 0x00034802, 0x5884b7fa,
+                                   0xecbc4ff5, 0x998c4fef, 0xacc5056f, 0x1824b159};
+        return t[i];
+    }
+    KB_HD static constexpr uint32_t R2(int i) {
+        constexpr uint32_t t[8] = {0xf3f29c6d, 0xc999e990, 0x87925c23, 0x2b6cedcb,
+                                   0x7254398f, 0x05d31496, 0x9f59ff11, 0x0748d9d9};
+        return t[i];
+    }
+};
+
+struct FpBN {
+    static constexpr int N = 8;
+    static constexpr int BYTES = 32;
+    static constexpr uint32_t M0 = 0xe4866389u;
+    KB_HD static constexpr uint32_t P(int i) {
+        constexpr uint32_t t[8] = {0xd87cfd47, 0x3c208c16, 0x6871ca8d, 0x97816a91,
+                                   0x8181585d, 0xb85045b6, 0xe131a029, 0x30644e72};
+        return t[i];
+    }
+    KB_HD static constexpr uint32_t R1(int i) {
+        constexpr uint32_t t[8] = {0xc58f0d9d, 0xd35d438d, 0xf5c70b3d, 0x0a78eb28,
+                                   0x7879462c, 0x666ea36f, 0x9a07df2f, 0x0e0a77c1};
+        return t[i];
+    }
+    KB_HD static constexpr uint32_t R2(int i) {
+        constexpr uint32_t t[8] = {0x538afa89, 0xf32cfc5b, 0xd44501fb, 0xb5e71911,
+                                   0x0a417ff6, 0x47ab1eff, 0xcab8351f, 0x06d89f71};
+        return t[i];
+    }
+};
+
+struct FrBN {
+    static constexpr int N = 8;
+    static constexpr int BYTES = 32;
+    static constexpr uint32_t M0 = 0xefffffffu;
+    KB_HD static constexpr uint32_t P(int i) {
+        constexpr uint32_t t[8] = {0xf0000001, 0x43e1f593, 0x79b97091, 0x2833e848,
+                                   0x8181585d, 0xb85045b6, 0xe131a029, 0x30644e72};
+        return t[i];
+    }
+    KB_HD static constexpr uint32_t R1(int i) {
+        constexpr uint32_t t[8] = {0x4ffffffb, 0xac96341c, 0x9f60cd29, 0x36fc7695,
+                                   0x7879462e, 0x666ea36f, 0x9a07df2f, 0x0e0a77c1};
+        return t[i];
+    }
+    KB_HD static constexpr uint32_t R2(int i) {
+        constexpr uint32_t t[8] = {0xae216da7, 0x1bb8e645, 0xe35c59e3, 0x53fe3ab1,
+                                   0x53bb8085, 0x8c49833d, 0x7f4e44a5, 0x0216d0b1};
+        return t[i];
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Element type and arithmetic.
+// ---------------------------------------------------------------------------
+template <class F>
+struct Fe {
+    uint32_t v[F::N];
+};
+
+template <class F>
+KB_DEV void fe_zero(Fe<F>& a) {
+#pragma unroll
+    for (int i = 0; i < F::N; ++i) a.v[i] = 0;
+}
+template <class F>
+KB_DEV void fe_one(Fe<F>& a) {  // 1 in Montgomery form (R mod p)
+#pragma unroll
+    for (int i = 0; i < F::N; ++i) a.v[i] = F::R1(i);
+}
+template <class F>
+KB_DEV bool fe_is_zero(const Fe<F>& a) {
+    uint32_t acc = 0;
+#pragma unroll
+    for (int i = 0; i < F::N; ++i) acc |= a.v[i];
+    return acc == 0;
+}
+template <class F>
+KB_DEV bool fe_eq(const Fe<F>& a, const Fe<F>& b) {
+    uint32_t acc = 0;
+#pragma unroll
+    for (int i = 0; i < F::N; ++i) acc |= a.v[i] ^ b.v[i];
+    return acc == 0;
+}
+
+// t[0..N] += a * b for a word b; t holds N+1 words and the caller guarantees
+// the sum fits in them.
+template <int N>
+KB_DEV void mac_row(uint32_t (&t)[N + 1], const uint32_t (&a)[N], uint32_t b) {
+    t[0] = mad_lo_cc(a[0], b, t[0]);
+    t[1] = madc_hi_cc(a[0], b, t[1]);
+#pragma unroll
+    for (int j = 2; j < N; j += 2) {
+        t[j] = madc_lo_cc(a[j], b, t[j]);
+        t[j + 1] = madc_hi_cc(a[j], b, t[j + 1]);
+    }
+    t[N] = addc_u32(t[N], 0);
+    t[1] = mad_lo_cc(a[1], b, t[1]);
+    t[2] = madc_hi_cc(a[1], b, t[2]);
+#pragma unroll
+    for (int j = 3; j < N; j += 2) {
+        t[j] = madc_lo_cc(a[j], b, t[j]);
+        t[j + 1] = madc_hi_cc(a[j], b, t[j + 1]);
+    }
+}
+
+// r = t - p if t >= p else t (t < 2p, N words).
+template <class F>
+KB_DEV void reduce_once(Fe<F>& r, const uint32_t* t) {
+    constexpr int N = F::N;
+    uint32_t d[N];
+    d[0] = sub_cc(t[0], F::P(0));
+#pragma unroll
+    for (int i = 1; i < N; ++i) d[i] = subc_cc(t[i], F::P(i));
+    uint32_t borrow = subc_u32(0, 0);  // 0xffffffff if t < p
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.v[i] = borrow ? t[i] : d[i];
+}
+
+// r = a * b * R^-1 mod p, inputs and output in [0, p).
+template <class F>
+KB_DEV void fe_mul(Fe<F>& r, const Fe<F>& a, const Fe<F>& b) {
+    constexpr int N = F::N;
+    uint32_t p[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) p[i] = F::P(i);
+    uint32_t t[N + 1];
+#pragma unroll
+    for (int i = 0; i <= N; ++i) t[i] = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        mac_row<N>(t, a.v, b.v[i]);
+        uint32_t m = t[0] * F::M0;
+        mac_row<N>(t, p, m);
+#pragma unroll
+        for (int j = 0; j < N; ++j) t[j] = t[j + 1];
+        t[N] = 0;
+    }
+    reduce_once<F>(r, t);
+}
+
+template <class F>
+KB_DEV void fe_sqr(Fe<F>& r, const Fe<F>& a) {
+    fe_mul<F>(r, a, a);
+}
+
+template <class F>
+KB_DEV void fe_add(Fe<F>& r, const Fe<F>& a, const Fe<F>& b) {
+    constexpr int N = F::N;
+    uint32_t s[N];
+    s[0] = add_cc(a.v[0], b.v[0]);
+#pragma unroll
+    for (int i = 1; i < N; ++i) s[i] = addc_cc(a.v[i], b.v[i]);
+    reduce_once<F>(r, s);
+}
+
+template <class F>
+KB_DEV void fe_sub(Fe<F>& r, const Fe<F>& a, const Fe<F>& b) {
+    constexpr int N = F::N;
+    uint32_t d[N];
+    d[0] = sub_cc(a.v[0], b.v[0]);
+#pragma unroll
+    for (int i = 1; i < N; ++i) d[i] = subc_cc(a.v[i], b.v[i]);
+    uint32_t mask = subc_u32(0, 0);
+    r.v[0] = add_cc(d[0], F::P(0) & mask);
+#pragma unroll
+    for (int i = 1; i < N; ++i) r.v[i] = addc_cc(d[i], F::P(i) & mask);
+}
+
+template <class F>
+KB_DEV void fe_neg(Fe<F>& r, const Fe<F>& a) {
+    Fe<F> z;
+    fe_zero(z);
+    fe_sub<F>(r, z, a);
+}
+
+template <class F>
+KB_DEV void fe_dbl(Fe<F>& r, const Fe<F>& a) {
+    fe_add<F>(r, a, a);
+}
+
+// Conversions between canonical and Montgomery form.  to_mont accepts any
+// N-word value (it need not be below p): the CIOS bound keeps the product
+// below 2p because R^2 mod p < p, so the result is the canonical image of
+// (a mod p) -- the same reduction the reference's to_mont performs.
+template <class F>
+KB_DEV void fe_to_mont(Fe<F>& r, const Fe<F>& a) {
+    Fe<F> r2;
+#pragma unroll
+    for (int i = 0; i < F::N; ++i) r2.v[i] = F::R2(i);
+    fe_mul<F>(r, a, r2);
+}
+template <class F>
+KB_DEV void fe_from_mont(Fe<F>& r, const Fe<F>& a) {
+    Fe<F> one;
+    fe_zero(one);
+    one.v[0] = 1;
+    fe_mul<F>(r, a, one);
+}
+
+// Exponent word i of p - 2 (p is odd and its low word is >= 2 for all four
+// moduli, so only word 0 changes).
+template <class F>
+KB_HD constexpr uint32_t pm2_word(int i) {
+    return i == 0 ? F::P(0) - 2u : F::P(i);
+}
+
+// a^(p-2) by left-to-right square-and-multiply with 4-bit fixed windows.
+template <class F>
+__device__ __noinline__ void fe_inv(Fe<F>& r, const Fe<F>& a) {
+    Fe<F> tab[16];
+    fe_one(tab[0]);
+    tab[1] = a;
+#pragma unroll 1
+    for (int i = 2; i < 16; ++i) fe_mul<F>(tab[i], tab[i - 1], a);
+    Fe<F> acc;
+    fe_one(acc);
+    bool started = false;
+#pragma unroll 1
+    for (int w = F::N * 8 - 1; w >= 0; --w) {
+        const uint32_t word = pm2_word<F>(w >> 3);
+        const uint32_t nib = (word >> ((w & 7) * 4)) & 15u;
+        if (started) {
+#pragma unroll 1
+            for (int s = 0; s < 4; ++s) fe_sqr<F>(acc, acc);
+        }
+        if (nib) {
+            if (started) {
+                fe_mul<F>(acc, acc, tab[nib]);
+            } else {
+                acc = tab[nib];
+                started = true;
+            }
+        }
+    }
+    r = acc;
+}
+
+// Load / store helpers for canonical little-endian words.
+template <class F>
+KB_DEV void fe_load(Fe<F>& r, const uint32_t* src) {
+#pragma unroll
+    for (int i = 0; i < F::N; ++i) r.v[i] = src[i];
+}
+template <class F>
+KB_DEV void fe_store(uint32_t* dst, const Fe<F>& a) {
+#pragma unroll
+    for (int i = 0; i < F::N; ++i) dst[i] = a.v[i];
+}
+
+// Big-endian byte string (F::BYTES long) -> little-endian words.
+template <class F>
+KB_DEV void fe_from_be_bytes(Fe<F>& r, const uint8_t* b) {
+#pragma unroll
+    for (int i = 0; i < F::N; ++i) {
+        const uint8_t* q = b + F::BYTES - 4 * (i + 1);
+        r.v[i] = ((uint32_t)q[0] << 24) | ((uint32_t)q[1] << 16) | ((uint32_t)q[2] << 8) |
+                 (uint32_t)q[3];
+    }
+}
+template <class F>
+KB_DEV void fe_to_be_bytes(uint8_t* b, const Fe<F>& a) {
+#pragma unroll
+    for (int i = 0; i < F::N; ++i) {
+        uint8_t* q = b + F::BYTES - 4 * (i + 1);
+        q[0] = (uint8_t)(a.v[i] >> 24);
+        q[1] = (uint8_t)(a.v[i] >> 16);
+        q[2] = (uint8_t)(a.v[i] >> 8);
+        q[3] = (uint8_t)a.v[i];
+    }
+}
+
+}  // namespace kb200

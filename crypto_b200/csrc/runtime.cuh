@@ -1,0 +1,112 @@
+// Host-side runtime pieces shared by the kernels: error handling, grow-only
+// scratch buffers, and a device prefix sum.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace kb200 {
+
+struct CudaError : std::runtime_error {
+    cudaError_t code;
+    CudaError(cudaError_t c, const char* what) : std::runtime_error(what), code(c) {}
+};
+
+#define KB_CUDA(expr)                                                              \
+    do {                                                                           \
+        cudaError_t kb_err_ = (expr);                                              \
+        if (kb_err_ != cudaSuccess) {                                              \
+            char kb_buf_[256];                                                     \
+            std::snprintf(kb_buf_, sizeof kb_buf_, "%s failed: %s (%s:%d)", #expr, \
+                          cudaGetErrorString(kb_err_), __FILE__, __LINE__);        \
+            throw ::kb200::CudaError(kb_err_, kb_buf_);                            \
+        }                                                                          \
+    } while (0)
+
+// Every kernel launch site calls KB_LAUNCH_CHECK(): it checks the launch and
+// counts it (kb200_launch_count() reports the total, so a benchmark can state
+// how many of this library's kernels ran in its timed region).
+void count_launch();
+#define KB_LAUNCH_CHECK()             \
+    do {                              \
+        KB_CUDA(cudaGetLastError());  \
+        ::kb200::count_launch();      \
+    } while (0)
+
+// Optional per-stage timing (CUDA events on the work stream), off by default.
+bool profiling_enabled();
+
+// Records the most recent failure message so the C ABI can report it.
+void set_last_error(const std::string& msg);
+
+// A grow-only device buffer.  Growing synchronises the owning stream first,
+// because the old allocation may still be read by queued work.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    void reserve(size_t need, cudaStream_t stream) {
+        if (need <= bytes) return;
+        if (ptr) {
+            KB_CUDA(cudaStreamSynchronize(stream));
+            KB_CUDA(cudaFree(ptr));
+            ptr = nullptr;
+            bytes = 0;
+        }
+        size_t want = need + need / 8 + 256;
+        KB_CUDA(cudaMalloc(&ptr, want));
+        bytes = want;
+    }
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(ptr);
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+// Pinned host staging buffer (grow-only).
+struct HostBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    void reserve(size_t need, cudaStream_t stream) {
+        if (need <= bytes) return;
+        if (ptr) {
+            KB_CUDA(cudaStreamSynchronize(stream));
+            KB_CUDA(cudaFreeHost(ptr));
+            ptr = nullptr;
+            bytes = 0;
+        }
+        size_t want = need + need / 8 + 256;
+        KB_CUDA(cudaMallocHost(&ptr, want));
+        bytes = want;
+    }
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(ptr);
+    }
+    void release() {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+// Exclusive prefix sum of n 32-bit values: out[i] = sum_{j<i} f(in[j]) and
+// out[n] = total, where f is the identity (div == 0) or ceil(x / div).
+// tmp must hold scan_tmp_words(n) words.
+size_t scan_tmp_words(size_t n);
+void exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t div,
+                        uint32_t* tmp, cudaStream_t stream);
+
+inline unsigned ceil_div_u(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
+
+}  // namespace kb200

@@ -1,0 +1,153 @@
+/*
+ * kinet-b200: B200-native (sm_100a) polynomial-commitment path -- C ABI.
+ *
+ * Drop-in GPU bodies for the reference's C entry points on this path, plus
+ * the Fr-NTT, synthetic-SRS commit, batched-commit and serving entry points
+ * the reference does not have, named in its <alg>_<op> style.
+ *
+ * All entry points are synchronous unless their name ends in _device, take
+ * caller-owned buffers, allocate nothing the caller must free, and are safe
+ * to call from several host threads (calls on one device are serialised).
+ * There is no CPU fallback: without a usable CUDA device every entry point
+ * returns its backend error code and kb200_last_error() says why.
+ *
+ * Encodings at this boundary (all canonical, never Montgomery):
+ *   scalar / Fr element : 32 bytes little-endian
+ *   G1 affine point     : x || y big-endian; 96 B (BLS12-381), 64 B (BN254);
+ *                         all-zero bytes = point at infinity
+ *   compressed G1       : 48 bytes, ZCash/IETF flags (BLS12-381)
+ */
+#ifndef KINET_B200_CRYPTO_B200_H
+#define KINET_B200_CRYPTO_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+/* gpukit codes: gpukit/include/kinet/gpukit/gpukit.h:38-46 */
+#define KB200_GPUKIT_OK 0
+#define KB200_GPUKIT_ERR_NULL_ARG -1
+#define KB200_GPUKIT_ERR_BAD_SIZE -2
+#define KB200_GPUKIT_ERR_BACKEND -3
+#define KB200_GPUKIT_ERR_DISPATCH -4
+#define KB200_GPUKIT_ERR_NOTIMPL -5
+/* crypto.h codes: c-abi/crypto.h:60-66 */
+#define KB200_CRYPTO_OK 0
+#define KB200_CRYPTO_ERR_INPUT -1
+#define KB200_CRYPTO_ERR_LENGTH -2
+#define KB200_CRYPTO_ERR_VERIFY -3
+#define KB200_CRYPTO_ERR_BACKEND -4
+#define KB200_CRYPTO_ERR_NOTIMPL -5
+#define KB200_CRYPTO_ERR_INTERNAL -6
+
+/* Curve ids: gpukit_curve, gpukit/include/kinet/gpukit/multi_pippenger.h:51-56 */
+#define KB200_CURVE_BN254_G1 1
+#define KB200_CURVE_BLS12_381_G1 2
+
+/* ---- MSM: drop-in for gpukit ------------------------------------------- */
+
+/* result = sum_i scalars[i] * points[i].
+ * Replaces gpukit_multi_pippenger (gpukit/c-abi/c_multi_pippenger.cpp:9-41,
+ * declared at gpukit/include/kinet/gpukit/multi_pippenger.h:69-91) with a
+ * GPU-only body: same argument order and meaning, same wire formats, same
+ * null checks first, n == 0 gives the all-zero identity, and output bytes
+ * equal gpukit_multi_pippenger_cpu's (multi_pippenger.cpp:356-405) for every
+ * input, including its dropped top-window carry for scalars >= 2^255 when
+ * its window size is 4 or 8.  Curves: BN254 G1 (1) and BLS12-381 G1 (2);
+ * secp256k1 (0) and banderwagon (3) return GPUKIT_ERR_NOTIMPL so the
+ * reference dispatcher's CPU fallback still covers them; unknown ids return
+ * GPUKIT_ERR_BACKEND as the CPU body does.  Points must be on the curve
+ * (neither implementation checks; off-curve input is undefined). */
+int gpukit_multi_pippenger(uint32_t curve, const uint8_t* scalars, const uint8_t* points,
+                           size_t n, uint8_t* result);
+
+/* The CUDA body the reference declares at multi_pippenger.h:81-85 (and stubs
+ * to NOTIMPL at gpukit/gpu/cuda/multi_pippenger.cu:38-44).  Same contract. */
+int gpukit_multi_pippenger_cuda(uint32_t curve, const uint8_t* scalars,
+                                const uint8_t* points, size_t n, uint8_t* result);
+
+/* ---- Fr NTT (new; same style as ntt_forward/ntt_inverse, crypto.h:368-369) */
+
+/* In-place transform of n canonical Fr elements (32 B LE each), natural
+ * order in and out.  forward: X_k = sum_j x_j w^(jk); inverse: x_j = n^-1
+ * sum_k X_k w^(-jk); w = g^((r-1)/n), g = 7 (BLS12-381) or 5 (BN254).
+ * coset != 0 evaluates on g*H: forward pre-multiplies x_j by g^j, inverse
+ * post-multiplies by g^-j.  Inputs are reduced mod r.  n must be a power of
+ * two up to 2^28.  Returns CRYPTO_OK, CRYPTO_ERR_INPUT (null / bad curve),
+ * CRYPTO_ERR_LENGTH (bad n) or CRYPTO_ERR_BACKEND. */
+int ntt_fr_forward(int curve, uint8_t* coeffs32le, size_t n, int coset);
+int ntt_fr_inverse(int curve, uint8_t* coeffs32le, size_t n, int coset);
+
+/* ---- KZG over BLS12-381 with a resident SRS (new) ---------------------- */
+
+/* Load n monomial-basis SRS points [tau^i]G1 (96 B BE each) into device
+ * memory, replacing any resident SRS.  The reference loads its setup once
+ * per process (kzg/cpp/kzg_blob.cpp:23-65); this is the resident analogue. */
+int kzg_srs_load_g1(const uint8_t* points96be, size_t n);
+/* Build the synthetic SRS [tau^i]G1, i < n, on the device from a 32-byte LE
+ * tau (reduced mod r).  For tests and benchmarks. */
+int kzg_srs_generate_g1(const uint8_t tau32le[32], size_t n);
+/* Copy `count` resident SRS points starting at `offset` back to the host. */
+int kzg_srs_read_g1(uint8_t* points96be, size_t offset, size_t count);
+/* Number of resident SRS points (0 if none). */
+size_t kzg_srs_size(void);
+
+/* commit = [p(tau)]G1 for the polynomial p given by n evaluations
+ * (32 B LE Fr) at the n-th roots of unity, natural order: an inverse NTT to
+ * monomial coefficients, an MSM against the resident SRS, then the 48-byte
+ * compressed encoding.  n must be a power of two <= kzg_srs_size().  Returns
+ * CRYPTO_ERR_LENGTH if the SRS is too short or n is not a power of two. */
+int kzg_commit_fr(const uint8_t* evals32le, size_t n, uint8_t commit48[48]);
+
+/* `count` independent commits in one batched pass.  Polynomial c has
+ * sizes[c] evaluations, stored back to back in evals32le (in order);
+ * commits48 receives 48 * count bytes.  Byte-equal to count kzg_commit_fr
+ * calls. */
+int kzg_commit_batch(const uint8_t* evals32le, const size_t* sizes, size_t count,
+                     uint8_t* commits48);
+
+/* ---- Device-pointer entry points (inputs already resident in HBM) ------ */
+/* Pointers are device pointers (16-byte aligned), `stream` is a
+ * cudaStream_t (NULL = legacy default stream); work is queued, not
+ * synchronised.  Calls sharing a device must not overlap across streams. */
+int kb200_msm_device(uint32_t curve, const void* d_scalars, const void* d_points, size_t n,
+                     void* d_result, void* stream);
+int kb200_ntt_device(int curve, void* d_data, size_t n, int inverse, int coset, size_t batch,
+                     void* stream);
+/* d_out_points[i] = d_scalars[i] * G1 (wire encoding), fixed-base windows. */
+int kb200_g1_fixed_base_device(uint32_t curve, const void* d_scalars, size_t n,
+                               void* d_out_points, void* stream);
+/* d_out[i] = tau^i (32 B LE Fr). */
+int kb200_fr_powers_device(int curve, const void* d_tau, size_t n, void* d_out, void* stream);
+/* KZG commit on device buffers against the resident SRS (evals are consumed:
+ * the buffer is transformed in place). */
+int kb200_kzg_commit_device(void* d_evals, size_t n, void* d_commit48, void* stream);
+
+/* ---- Seeded synthetic inputs (host only, no GPU needed) ---------------- */
+/* xorshift64* streams; uniform Fr by rejection sampling of 255-bit (BLS12-381)
+ * or 254-bit (BN254) draws.  kind: 0 = uniform in [0, r); 1 = skewed
+ * (25% zero, 25% one, 20% uniform below 2^64, 30% uniform in [0, r)). */
+int kb200_gen_scalars(int curve, uint64_t seed, size_t n, int kind, uint8_t* out32le);
+
+/* ---- Introspection ------------------------------------------------------ */
+const char* kb200_last_error(void);
+/* 1 if a CUDA device is usable, else 0. */
+int kb200_device_available(void);
+/* Window size the MSM planner picks for n (for tests of the planner). */
+int kb200_msm_window(uint32_t curve, size_t n);
+/* Number of this library's kernel launches since load. */
+unsigned long long kb200_launch_count(void);
+/* Per-stage CUDA-event timing of MSMs (off by default). */
+void kb200_profile_enable(int on);
+/* Stage times (ms) of the last MSM on this device for the curve, in order:
+ * wire->table, recode, sort, accumulate, fold, reduce+combine.  Returns the
+ * number written (0 if none recorded), or -1. */
+int kb200_msm_stage_ms(uint32_t curve, float* out, int max);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,751 @@
+/*
+ * CPU oracle (TEST INFRASTRUCTURE ONLY) -- plain-C restatement of the
+ * reference's CPU path.  Never linked by the product library.
+ *
+ * Field arithmetic restates the reference's 64-bit-limb CIOS Montgomery code:
+ *   BLS12-381 Fp : bls/cpp/bls12_381_fp.hpp:83-245
+ *   BLS12-381 Fr : kzg/cpp/kzg_oracle.hpp:64-210
+ *   BN254 Fp, Fr : bn254/cpp/bn254_fp.hpp:75-263
+ * Group law (Jacobian, a = 0) restates add-2007-bl / dbl-2009-l as written in
+ *   bls/cpp/bls12_381_g1.hpp:57-151 and bn254/cpp/bn254_g1.hpp:51-170.
+ * Pippenger restates gpukit/cpp/cpu_reference/multi_pippenger.cpp:67-181.
+ * The NTT restates the radix-2 DIT order of ntt/cpp/ntt.cpp:128-172 over Fr.
+ */
+#include "oracle.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+typedef unsigned __int128 u128;
+typedef uint64_t u64;
+
+/* ------------------------------------------------------------------------ */
+/* Generic Montgomery field over up to 6 64-bit limbs.                      */
+/* ------------------------------------------------------------------------ */
+
+typedef struct { u64 l[6]; } fe;
+
+typedef struct {
+    int n;          /* 64-bit limbs */
+    int bytes;      /* canonical byte width at the boundary */
+    fe p, r1, r2;   /* modulus, R mod p, R^2 mod p */
+    u64 pinv;       /* -p^-1 mod 2^64 */
+} field;
+
+/* bls/cpp/bls12_381_fp.hpp:83-98 */
+static const field F_BLS_FP = {6, 48,
+    {{0xB9FEFFFFFFFFAAABULL, 0x1EABFFFEB153FFFFULL, 0x6730D2A0F6B0F624ULL,
+      0x64774B84F38512BFULL, 0x4B1BA7B6434BACD7ULL, 0x1A0111EA397FE69AULL}},
+    {{0x760900000002FFFDULL, 0xEBF4000BC40C0002ULL, 0x5F48985753C758BAULL,
+      0x77CE585370525745ULL, 0x5C071A97A256EC6DULL, 0x15F65EC3FA80E493ULL}},
+    {{0xF4DF1F341C341746ULL, 0x0A76E6A609D104F1ULL, 0x8DE5476C4C95B6D5ULL,
+      0x67EB88A9939D83C0ULL, 0x9A793E85B519952DULL, 0x11988FE592CAE3AAULL}},
+    0x89F3FFFCFFFCFFFDULL};
+/* kzg/cpp/kzg_oracle.hpp:66-90 */
+static const field F_BLS_FR = {4, 32,
+    {{0xFFFFFFFF00000001ULL, 0x53BDA402FFFE5BFEULL, 0x3339D80809A1D805ULL,
+      0x73EDA753299D7D48ULL}},
+    {{0x00000001FFFFFFFEULL, 0x5884B7FA00034802ULL, 0x998C4FEFECBC4FF5ULL,
+      0x1824B159ACC5056FULL}},
+    {{0xC999E990F3F29C6DULL, 0x2B6CEDCB87925C23ULL, 0x05D314967254398FULL,
+      0x0748D9D99F59FF11ULL}},
+    0xFFFFFFFEFFFFFFFFULL};
+/* bn254/cpp/bn254_fp.hpp:75-89 */
+static const field F_BN_FP = {4, 32,
+    {{0x3C208C16D87CFD47ULL, 0x97816A916871CA8DULL, 0xB85045B68181585DULL,
+      0x30644E72E131A029ULL}},
+    {{0xD35D438DC58F0D9DULL, 0x0A78EB28F5C70B3DULL, 0x666EA36F7879462CULL,
+      0x0E0A77C19A07DF2FULL}},
+    {{0xF32CFC5B538AFA89ULL, 0xB5E71911D44501FBULL, 0x47AB1EFF0A417FF6ULL,
+      0x06D89F71CAB8351FULL}},
+    0x87D20782E4866389ULL};
+/* bn254/cpp/bn254_fp.hpp:79-97 */
+static const field F_BN_FR = {4, 32,
+    {{0x43E1F593F0000001ULL, 0x2833E84879B97091ULL, 0xB85045B68181585DULL,
+      0x30644E72E131A029ULL}},
+    {{0xAC96341C4FFFFFFBULL, 0x36FC76959F60CD29ULL, 0x666EA36F7879462EULL,
+      0x0E0A77C19A07DF2FULL}},
+    {{0x1BB8E645AE216DA7ULL, 0x53FE3AB1E35C59E3ULL, 0x8C49833D53BB8085ULL,
+      0x0216D0B17F4E44A5ULL}},
+    0xC2E1F593EFFFFFFFULL};
+
+static const field* field_by_id(int which) {
+    switch (which) {
+        case 0: return &F_BLS_FP;
+        case 1: return &F_BLS_FR;
+        case 2: return &F_BN_FP;
+        case 3: return &F_BN_FR;
+        default: return NULL;
+    }
+}
+
+static int fe_cmp(const field* F, const fe* a, const fe* b) {
+    for (int i = F->n - 1; i >= 0; --i) {
+        if (a->l[i] < b->l[i]) return -1;
+        if (a->l[i] > b->l[i]) return 1;
+    }
+    return 0;
+}
+static int fe_is_zero(const field* F, const fe* a) {
+    u64 acc = 0;
+    for (int i = 0; i < F->n; ++i) acc |= a->l[i];
+    return acc == 0;
+}
+static u64 raw_add(const field* F, fe* r, const fe* a, const fe* b) {
+    u64 c = 0;
+    for (int i = 0; i < F->n; ++i) {
+        u128 t = (u128)a->l[i] + b->l[i] + c;
+        r->l[i] = (u64)t;
+        c = (u64)(t >> 64);
+    }
+    return c;
+}
+static u64 raw_sub(const field* F, fe* r, const fe* a, const fe* b) {
+    u64 bw = 0;
+    for (int i = 0; i < F->n; ++i) {
+        u128 t = (u128)a->l[i] - b->l[i] - bw;
+        r->l[i] = (u64)t;
+        bw = (u64)(t >> 64) & 1;
+    }
+    return bw;
+}
+/* mod_add / mod_sub / neg: bls12_381_fp.hpp:129-147, :204-208 */
+static fe f_add(const field* F, fe a, fe b) {
+    fe t;
+    u64 c = raw_add(F, &t, &a, &b);
+    if (c || fe_cmp(F, &t, &F->p) >= 0) raw_sub(F, &t, &t, &F->p);
+    return t;
+}
+static fe f_sub(const field* F, fe a, fe b) {
+    fe t;
+    if (raw_sub(F, &t, &a, &b)) raw_add(F, &t, &t, &F->p);
+    return t;
+}
+static fe f_neg(const field* F, fe a) {
+    if (fe_is_zero(F, &a)) return a;
+    fe t;
+    raw_sub(F, &t, &F->p, &a);
+    return t;
+}
+/* CIOS Montgomery product a*b*R^-1: bls12_381_fp.hpp:153-189 (n = 6) and
+ * bn254_fp.hpp:155-191 (n = 4) share this shape. */
+static fe f_mul(const field* F, fe a, fe b) {
+    const int n = F->n;
+    u64 t[8] = {0};
+    for (int i = 0; i < n; ++i) {
+        u64 carry = 0;
+        for (int j = 0; j < n; ++j) {
+            u128 prod = (u128)a.l[j] * b.l[i] + t[j] + carry;
+            t[j] = (u64)prod;
+            carry = (u64)(prod >> 64);
+        }
+        u128 sum = (u128)t[n] + carry;
+        t[n] = (u64)sum;
+        t[n + 1] += (u64)(sum >> 64);
+        u64 u = t[0] * F->pinv;
+        carry = 0;
+        for (int j = 0; j < n; ++j) {
+            u128 prod = (u128)u * F->p.l[j] + t[j] + carry;
+            t[j] = (u64)prod;
+            carry = (u64)(prod >> 64);
+        }
+        sum = (u128)t[n] + carry;
+        t[n] = (u64)sum;
+        t[n + 1] += (u64)(sum >> 64);
+        for (int j = 0; j < n + 1; ++j) t[j] = t[j + 1];
+        t[n + 1] = 0;
+    }
+    fe r;
+    memset(&r, 0, sizeof r);
+    for (int i = 0; i < n; ++i) r.l[i] = t[i];
+    if (t[n] != 0 || fe_cmp(F, &r, &F->p) >= 0) raw_sub(F, &r, &r, &F->p);
+    return r;
+}
+static fe f_sqr(const field* F, fe a) { return f_mul(F, a, a); }
+static fe f_to_mont(const field* F, fe a) { return f_mul(F, a, F->r2); }
+static fe f_from_mont(const field* F, fe a) {
+    fe one;
+    memset(&one, 0, sizeof one);
+    one.l[0] = 1;
+    return f_mul(F, a, one);
+}
+static fe f_one(const field* F) { return F->r1; }
+/* square-and-multiply, bls12_381_fp.hpp:220-232 */
+static fe f_pow(const field* F, fe a_mont, const fe* e) {
+    fe result = f_one(F), base = a_mont;
+    for (int limb = 0; limb < F->n; ++limb) {
+        u64 w = e->l[limb];
+        for (int bit = 0; bit < 64; ++bit) {
+            if ((w >> bit) & 1) result = f_mul(F, result, base);
+            base = f_sqr(F, base);
+        }
+    }
+    return result;
+}
+static fe f_inv(const field* F, fe a_mont) {
+    fe e = F->p, two;
+    memset(&two, 0, sizeof two);
+    two.l[0] = 2;
+    raw_sub(F, &e, &e, &two);
+    return f_pow(F, a_mont, &e);
+}
+static fe f_from_small(const field* F, u64 v) {
+    fe a;
+    memset(&a, 0, sizeof a);
+    a.l[0] = v;
+    return f_to_mont(F, a);
+}
+
+static fe fe_from_le(const field* F, const uint8_t* b) {
+    fe r;
+    memset(&r, 0, sizeof r);
+    for (int i = 0; i < F->bytes; ++i) r.l[i / 8] |= (u64)b[i] << (8 * (i % 8));
+    return r;
+}
+static void fe_to_le(const field* F, const fe* a, uint8_t* b) {
+    for (int i = 0; i < F->bytes; ++i) b[i] = (uint8_t)(a->l[i / 8] >> (8 * (i % 8)));
+}
+static fe fe_from_be(const field* F, const uint8_t* b) {
+    fe r;
+    memset(&r, 0, sizeof r);
+    for (int i = 0; i < F->bytes; ++i) {
+        int k = F->bytes - 1 - i;
+        r.l[k / 8] |= (u64)b[i] << (8 * (k % 8));
+    }
+    return r;
+}
+static void fe_to_be(const field* F, const fe* a, uint8_t* b) {
+    for (int i = 0; i < F->bytes; ++i) {
+        int k = F->bytes - 1 - i;
+        b[i] = (uint8_t)(a->l[k / 8] >> (8 * (k % 8)));
+    }
+}
+
+int orc_field_mul(int which, const uint8_t* a, const uint8_t* b, uint8_t* out) {
+    const field* F = field_by_id(which);
+    if (!F) return -1;
+    fe x = f_to_mont(F, fe_from_le(F, a)), y = f_to_mont(F, fe_from_le(F, b));
+    fe z = f_from_mont(F, f_mul(F, x, y));
+    fe_to_le(F, &z, out);
+    return 0;
+}
+int orc_field_inv(int which, const uint8_t* a, uint8_t* out) {
+    const field* F = field_by_id(which);
+    if (!F) return -1;
+    fe z = f_from_mont(F, f_inv(F, f_to_mont(F, fe_from_le(F, a))));
+    fe_to_le(F, &z, out);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* G1, Jacobian coordinates, a = 0.                                        */
+/* ------------------------------------------------------------------------ */
+
+typedef struct { fe X, Y, Z; int inf; } jac;
+
+typedef struct {
+    const field* F;
+    u64 b;             /* curve constant */
+    int pt_bytes;      /* wire bytes per affine point */
+    uint8_t gx[48], gy[48];
+} curve;
+
+static curve C_BLS, C_BN;
+static int curves_ready = 0;
+
+static void init_curves(void) {
+    if (curves_ready) return;
+    /* bls/cpp/bls12_381_g1.hpp:204-224 */
+    static const uint8_t gx[48] = {
+        0x17, 0xF1, 0xD3, 0xA7, 0x31, 0x97, 0xD7, 0x94, 0x26, 0x95, 0x63, 0x8C,
+        0x4F, 0xA9, 0xAC, 0x0F, 0xC3, 0x68, 0x8C, 0x4F, 0x97, 0x74, 0xB9, 0x05,
+        0xA1, 0x4E, 0x3A, 0x3F, 0x17, 0x1B, 0xAC, 0x58, 0x6C, 0x55, 0xE8, 0x3F,
+        0xF9, 0x7A, 0x1A, 0xEF, 0xFB, 0x3A, 0xF0, 0x0A, 0xDB, 0x22, 0xC6, 0xBB};
+    static const uint8_t gy[48] = {
+        0x08, 0xB3, 0xF4, 0x81, 0xE3, 0xAA, 0xA0, 0xF1, 0xA0, 0x9E, 0x30, 0xED,
+        0x74, 0x1D, 0x8A, 0xE4, 0xFC, 0xF5, 0xE0, 0x95, 0xD5, 0xD0, 0x0A, 0xF6,
+        0x00, 0xDB, 0x18, 0xCB, 0x2C, 0x04, 0xB3, 0xED, 0xD0, 0x3C, 0xC7, 0x44,
+        0xA2, 0x88, 0x8A, 0xE4, 0x0C, 0xAA, 0x23, 0x29, 0x46, 0xC5, 0xE7, 0xE1};
+    C_BLS.F = &F_BLS_FP;
+    C_BLS.b = 4;
+    C_BLS.pt_bytes = 96;
+    memcpy(C_BLS.gx, gx, 48);
+    memcpy(C_BLS.gy, gy, 48);
+    /* BN254 G1 generator (1, 2), EIP-196. */
+    C_BN.F = &F_BN_FP;
+    C_BN.b = 3;
+    C_BN.pt_bytes = 64;
+    memset(C_BN.gx, 0, 48);
+    memset(C_BN.gy, 0, 48);
+    C_BN.gx[31] = 1;
+    C_BN.gy[31] = 2;
+    curves_ready = 1;
+}
+
+static const curve* curve_by_id(uint32_t id) {
+    init_curves();
+    if (id == ORC_CURVE_BLS12_381) return &C_BLS;
+    if (id == ORC_CURVE_BN254) return &C_BN;
+    return NULL;
+}
+
+static jac jac_zero(void) {
+    jac r;
+    memset(&r, 0, sizeof r);
+    r.inf = 1;
+    return r;
+}
+
+/* dbl-2009-l: bls12_381_g1.hpp:75-110 */
+static jac jac_double(const curve* C, jac p) {
+    const field* F = C->F;
+    if (p.inf) return p;
+    if (fe_is_zero(F, &p.Y)) return jac_zero();
+    fe A = f_sqr(F, p.X), B = f_sqr(F, p.Y), Cc = f_sqr(F, B);
+    fe D = f_sub(F, f_sqr(F, f_add(F, p.X, B)), A);
+    D = f_sub(F, D, Cc);
+    D = f_add(F, D, D);
+    fe E = f_add(F, f_add(F, A, A), A);
+    fe Fq = f_sqr(F, E);
+    fe X3 = f_sub(F, Fq, f_add(F, D, D));
+    fe C8 = f_add(F, Cc, Cc);
+    C8 = f_add(F, C8, C8);
+    C8 = f_add(F, C8, C8);
+    fe Y3 = f_sub(F, f_mul(F, E, f_sub(F, D, X3)), C8);
+    fe Z3 = f_mul(F, p.Y, p.Z);
+    Z3 = f_add(F, Z3, Z3);
+    jac r = {X3, Y3, Z3, 0};
+    return r;
+}
+
+/* add-2007-bl: bls12_381_g1.hpp:113-151 */
+static jac jac_add(const curve* C, jac a, jac b) {
+    const field* F = C->F;
+    if (a.inf) return b;
+    if (b.inf) return a;
+    fe Z1Z1 = f_sqr(F, a.Z), Z2Z2 = f_sqr(F, b.Z);
+    fe U1 = f_mul(F, a.X, Z2Z2), U2 = f_mul(F, b.X, Z1Z1);
+    fe S1 = f_mul(F, f_mul(F, a.Y, b.Z), Z2Z2);
+    fe S2 = f_mul(F, f_mul(F, b.Y, a.Z), Z1Z1);
+    fe H = f_sub(F, U2, U1);
+    if (fe_is_zero(F, &H)) {
+        if (fe_cmp(F, &S1, &S2) == 0) return jac_double(C, a);
+        return jac_zero();
+    }
+    fe I = f_sqr(F, f_add(F, H, H));
+    fe J = f_mul(F, H, I);
+    fe r_ = f_sub(F, S2, S1);
+    r_ = f_add(F, r_, r_);
+    fe V = f_mul(F, U1, I);
+    fe X3 = f_sub(F, f_sub(F, f_sqr(F, r_), J), f_add(F, V, V));
+    fe Y3 = f_sub(F, f_mul(F, r_, f_sub(F, V, X3)), f_mul(F, f_add(F, S1, S1), J));
+    fe Z3 = f_sub(F, f_sub(F, f_sqr(F, f_add(F, a.Z, b.Z)), Z1Z1), Z2Z2);
+    Z3 = f_mul(F, Z3, H);
+    jac out = {X3, Y3, Z3, 0};
+    return out;
+}
+
+static jac jac_neg(const curve* C, jac p) {
+    if (p.inf) return p;
+    p.Y = f_neg(C->F, p.Y);
+    return p;
+}
+
+/* read_affine: gpukit/curve_traits/bls12_381_g1_first_party_traits.h:58-69 */
+static jac read_point(const curve* C, const uint8_t* xy) {
+    const field* F = C->F;
+    int any = 0;
+    for (int i = 0; i < C->pt_bytes; ++i) any |= xy[i];
+    if (!any) return jac_zero();
+    jac r;
+    r.X = f_to_mont(F, fe_from_be(F, xy));
+    r.Y = f_to_mont(F, fe_from_be(F, xy + F->bytes));
+    r.Z = f_one(F);
+    r.inf = 0;
+    return r;
+}
+
+/* write_affine + g1_to_affine: traits .h:71-83, bls12_381_g1.hpp:57-72 */
+static void write_point(const curve* C, jac p, uint8_t* xy) {
+    const field* F = C->F;
+    if (p.inf || fe_is_zero(F, &p.Z)) {
+        memset(xy, 0, (size_t)C->pt_bytes);
+        return;
+    }
+    fe zi = f_inv(F, p.Z), zi2 = f_sqr(F, zi), zi3 = f_mul(F, zi2, zi);
+    fe x = f_from_mont(F, f_mul(F, p.X, zi2));
+    fe y = f_from_mont(F, f_mul(F, p.Y, zi3));
+    fe_to_be(F, &x, xy);
+    fe_to_be(F, &y, xy + F->bytes);
+}
+
+/* Left-to-right double-and-add over 256 bits (variable time; test use only). */
+static jac jac_mul(const curve* C, jac p, const uint8_t* k_le) {
+    jac acc = jac_zero();
+    for (int i = 255; i >= 0; --i) {
+        acc = jac_double(C, acc);
+        if ((k_le[i >> 3] >> (i & 7)) & 1) acc = jac_add(C, acc, p);
+    }
+    return acc;
+}
+
+static jac generator(const curve* C) {
+    uint8_t g[96];
+    memcpy(g, C->gx, (size_t)C->F->bytes);
+    memcpy(g + C->F->bytes, C->gy, (size_t)C->F->bytes);
+    return read_point(C, g);
+}
+
+int orc_g1_mul_gen(uint32_t curve_id, const uint8_t* k_le, uint8_t* result) {
+    const curve* C = curve_by_id(curve_id);
+    if (!C || !k_le || !result) return -1;
+    write_point(C, jac_mul(C, generator(C), k_le), result);
+    return 0;
+}
+
+int orc_g1_mul(uint32_t curve_id, const uint8_t* point, const uint8_t* k_le,
+               uint8_t* result) {
+    const curve* C = curve_by_id(curve_id);
+    if (!C || !point || !k_le || !result) return -1;
+    write_point(C, jac_mul(C, read_point(C, point), k_le), result);
+    return 0;
+}
+
+int orc_g1_add(uint32_t curve_id, const uint8_t* p, const uint8_t* q, uint8_t* result) {
+    const curve* C = curve_by_id(curve_id);
+    if (!C || !p || !q || !result) return -1;
+    write_point(C, jac_add(C, read_point(C, p), read_point(C, q)), result);
+    return 0;
+}
+
+/* g1_is_on_curve: bls12_381_g1.hpp:195-201 */
+int orc_g1_on_curve(uint32_t curve_id, const uint8_t* p) {
+    const curve* C = curve_by_id(curve_id);
+    if (!C || !p) return -1;
+    const field* F = C->F;
+    int any = 0;
+    for (int i = 0; i < C->pt_bytes; ++i) any |= p[i];
+    if (!any) return 1;
+    fe x = fe_from_be(F, p), y = fe_from_be(F, p + F->bytes);
+    if (fe_cmp(F, &x, &F->p) >= 0 || fe_cmp(F, &y, &F->p) >= 0) return 0;
+    x = f_to_mont(F, x);
+    y = f_to_mont(F, y);
+    fe lhs = f_sqr(F, y);
+    fe rhs = f_add(F, f_mul(F, f_sqr(F, x), x), f_from_small(F, C->b));
+    return fe_cmp(F, &lhs, &rhs) == 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Pippenger: gpukit/cpp/cpu_reference/multi_pippenger.cpp:67-181          */
+/* ------------------------------------------------------------------------ */
+
+enum { K_BITS = 256 };
+
+static u64 cost_model(u64 c, size_t n) {
+    u64 windows = (K_BITS + c - 1) / c;
+    return windows * ((u64)n + ((u64)1 << c));
+}
+
+static u64 best_c(size_t n) {
+    u64 best = 4, best_cost = ~(u64)0;
+    for (u64 c = 4; c <= 12; ++c) {
+        u64 cost = cost_model(c, n);
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = c;
+        }
+    }
+    return best;
+}
+
+static uint32_t window_digit(const uint8_t* s, size_t bit_offset, u64 c) {
+    size_t byte_idx = bit_offset >> 3, bit_in_byte = bit_offset & 7;
+    uint32_t word = 0;
+    for (int i = 0; i < 4; ++i) {
+        size_t bi = byte_idx + (size_t)i;
+        if (bi < 32) word |= (uint32_t)s[bi] << (8 * i);
+    }
+    word >>= bit_in_byte;
+    return word & ((1u << c) - 1u);
+}
+
+static jac pippenger(const curve* C, const jac* pts, const uint8_t* sc, size_t n) {
+    if (n == 0) return jac_zero();
+    u64 c = best_c(n);
+    size_t M = (size_t)1 << (c - 1);
+    size_t chunks = (K_BITS + c - 1) / c;
+    jac* buckets = (jac*)malloc(M * sizeof(jac));
+    int* carries = (int*)calloc(n, sizeof(int));
+    jac* wsum = (jac*)malloc(chunks * sizeof(jac));
+    int32_t max_pos = (int32_t)1 << (c - 1);
+    for (size_t w = 0; w < chunks; ++w) {
+        size_t off = w * c;
+        for (size_t k = 0; k < M; ++k) buckets[k] = jac_zero();
+        for (size_t i = 0; i < n; ++i) {
+            int32_t d = (int32_t)window_digit(sc + 32 * i, off, c) + carries[i];
+            carries[i] = 0;
+            if (d > max_pos) {
+                d -= (int32_t)1 << c;
+                carries[i] = 1;
+            }
+            if (d == 0) continue;
+            if (d > 0)
+                buckets[d - 1] = jac_add(C, buckets[d - 1], pts[i]);
+            else
+                buckets[-d - 1] = jac_add(C, buckets[-d - 1], jac_neg(C, pts[i]));
+        }
+        jac running = jac_zero(), total = jac_zero();
+        for (size_t kk = 0; kk < M; ++kk) {
+            size_t k = M - 1 - kk;
+            running = jac_add(C, running, buckets[k]);
+            total = jac_add(C, total, running);
+        }
+        wsum[w] = total;
+    }
+    jac result = wsum[chunks - 1];
+    for (size_t wi = 1; wi < chunks; ++wi) {
+        for (u64 b = 0; b < c; ++b) result = jac_double(C, result);
+        result = jac_add(C, result, wsum[chunks - 1 - wi]);
+    }
+    free(buckets);
+    free(carries);
+    free(wsum);
+    return result;
+}
+
+int orc_msm(uint32_t curve_id, const uint8_t* scalars, const uint8_t* points,
+            size_t n, uint8_t* result) {
+    if (!result) return -1;                          /* GPUKIT_ERR_NULL_ARG */
+    if (n > 0 && (!scalars || !points)) return -1;
+    const curve* C = curve_by_id(curve_id);
+    if (!C) return -3;                               /* GPUKIT_ERR_BACKEND */
+    jac* pts = (jac*)malloc((n ? n : 1) * sizeof(jac));
+    for (size_t i = 0; i < n; ++i) pts[i] = read_point(C, points + (size_t)C->pt_bytes * i);
+    write_point(C, pippenger(C, pts, scalars, n), result);
+    free(pts);
+    return 0;
+}
+
+int orc_msm_naive(uint32_t curve_id, const uint8_t* scalars, const uint8_t* points,
+                  size_t n, uint8_t* result) {
+    if (!result) return -1;
+    if (n > 0 && (!scalars || !points)) return -1;
+    const curve* C = curve_by_id(curve_id);
+    if (!C) return -3;
+    jac acc = jac_zero();
+    for (size_t i = 0; i < n; ++i) {
+        jac p = read_point(C, points + (size_t)C->pt_bytes * i);
+        acc = jac_add(C, acc, jac_mul(C, p, scalars + 32 * i));
+    }
+    write_point(C, acc, result);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Fr NTT (radix-2 DIT in the order of ntt/cpp/ntt.cpp:128-172).           */
+/* ------------------------------------------------------------------------ */
+
+static const field* fr_of(uint32_t curve_id, u64* gen, int* adicity) {
+    if (curve_id == ORC_CURVE_BLS12_381) {
+        *gen = 7;
+        *adicity = 32;
+        return &F_BLS_FR;
+    }
+    if (curve_id == ORC_CURVE_BN254) {
+        *gen = 5;
+        *adicity = 28;
+        return &F_BN_FR;
+    }
+    return NULL;
+}
+
+/* w_n = g^((r-1)/n) in Montgomery form. */
+static fe root_mont(const field* F, u64 g, int logn) {
+    fe e = F->p;
+    e.l[0] -= 1; /* r - 1; r is odd so no borrow */
+    for (int s = 0; s < logn; ++s) {
+        for (int i = 0; i < F->n; ++i) {
+            u64 hi = (i + 1 < F->n) ? e.l[i + 1] : 0;
+            e.l[i] = (e.l[i] >> 1) | (hi << 63);
+        }
+    }
+    return f_pow(F, f_from_small(F, g), &e);
+}
+
+static int ilog2_exact(size_t n) {
+    if (n == 0 || (n & (n - 1))) return -1;
+    int l = 0;
+    while (((size_t)1 << l) < n) ++l;
+    return l;
+}
+
+static void bit_reverse(fe* a, size_t n, int logn) {
+    for (size_t i = 0; i < n; ++i) {
+        size_t j = 0;
+        for (int b = 0; b < logn; ++b) j |= ((i >> b) & 1) << (logn - 1 - b);
+        if (j > i) {
+            fe t = a[i];
+            a[i] = a[j];
+            a[j] = t;
+        }
+    }
+}
+
+int orc_root_of_unity(uint32_t curve_id, size_t n, uint8_t* out) {
+    u64 g;
+    int adic;
+    const field* F = fr_of(curve_id, &g, &adic);
+    int logn = ilog2_exact(n);
+    if (!F || logn < 0 || logn > adic) return -2;
+    fe w = f_from_mont(F, root_mont(F, g, logn));
+    fe_to_le(F, &w, out);
+    return 0;
+}
+
+int orc_ntt(uint32_t curve_id, uint8_t* data, size_t n, int inverse, int coset) {
+    u64 g;
+    int adic;
+    const field* F = fr_of(curve_id, &g, &adic);
+    int logn = ilog2_exact(n);
+    if (!F || logn < 0 || logn > adic) return -2;
+    fe* a = (fe*)malloc(n * sizeof(fe));
+    for (size_t i = 0; i < n; ++i) a[i] = f_to_mont(F, fe_from_le(F, data + 32 * i));
+    fe gm = f_from_small(F, g);
+    if (coset && !inverse) {
+        fe s = f_one(F);
+        for (size_t i = 0; i < n; ++i) {
+            a[i] = f_mul(F, a[i], s);
+            s = f_mul(F, s, gm);
+        }
+    }
+    bit_reverse(a, n, logn);
+    for (int s = 1; s <= logn; ++s) {
+        size_t m = (size_t)1 << s, half = m >> 1;
+        fe wm = root_mont(F, g, s);
+        if (inverse) wm = f_inv(F, wm);
+        for (size_t k = 0; k < n; k += m) {
+            fe w = f_one(F);
+            for (size_t j = 0; j < half; ++j) {
+                fe u = a[k + j], t = f_mul(F, a[k + j + half], w);
+                a[k + j] = f_add(F, u, t);
+                a[k + j + half] = f_sub(F, u, t);
+                w = f_mul(F, w, wm);
+            }
+        }
+    }
+    if (inverse) {
+        fe ninv = f_inv(F, f_from_small(F, (u64)n));
+        fe gi = f_inv(F, gm), s = ninv;
+        for (size_t i = 0; i < n; ++i) {
+            a[i] = f_mul(F, a[i], s);
+            if (coset) s = f_mul(F, s, gi);
+        }
+    }
+    for (size_t i = 0; i < n; ++i) {
+        fe v = f_from_mont(F, a[i]);
+        fe_to_le(F, &v, data + 32 * i);
+    }
+    free(a);
+    return 0;
+}
+
+int orc_dft(uint32_t curve_id, uint8_t* data, size_t n, int inverse, int coset) {
+    u64 g;
+    int adic;
+    const field* F = fr_of(curve_id, &g, &adic);
+    int logn = ilog2_exact(n);
+    if (!F || logn < 0 || logn > adic) return -2;
+    fe* x = (fe*)malloc(n * sizeof(fe));
+    fe* y = (fe*)malloc(n * sizeof(fe));
+    for (size_t i = 0; i < n; ++i) x[i] = f_to_mont(F, fe_from_le(F, data + 32 * i));
+    fe gm = f_from_small(F, g);
+    fe w = root_mont(F, g, logn);
+    if (inverse) w = f_inv(F, w);
+    if (coset && !inverse) {
+        fe s = f_one(F);
+        for (size_t i = 0; i < n; ++i) {
+            x[i] = f_mul(F, x[i], s);
+            s = f_mul(F, s, gm);
+        }
+    }
+    fe wk = f_one(F);
+    for (size_t k = 0; k < n; ++k) {
+        fe acc, p = f_one(F);
+        memset(&acc, 0, sizeof acc);
+        for (size_t j = 0; j < n; ++j) {
+            acc = f_add(F, acc, f_mul(F, x[j], p));
+            p = f_mul(F, p, wk);
+        }
+        y[k] = acc;
+        wk = f_mul(F, wk, w);
+    }
+    if (inverse) {
+        fe ninv = f_inv(F, f_from_small(F, (u64)n));
+        fe gi = f_inv(F, gm), s = ninv;
+        for (size_t i = 0; i < n; ++i) {
+            y[i] = f_mul(F, y[i], s);
+            if (coset) s = f_mul(F, s, gi);
+        }
+    }
+    for (size_t i = 0; i < n; ++i) {
+        fe v = f_from_mont(F, y[i]);
+        fe_to_le(F, &v, data + 32 * i);
+    }
+    free(x);
+    free(y);
+    return 0;
+}
+
+int orc_fr_powers(uint32_t curve_id, const uint8_t* tau, size_t n, uint8_t* out) {
+    u64 g;
+    int adic;
+    const field* F = fr_of(curve_id, &g, &adic);
+    if (!F) return -2;
+    fe t = f_to_mont(F, fe_from_le(F, tau)), s = f_one(F);
+    for (size_t i = 0; i < n; ++i) {
+        fe v = f_from_mont(F, s);
+        fe_to_le(F, &v, out + 32 * i);
+        s = f_mul(F, s, t);
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Compressed BLS12-381 G1 (ZCash/IETF): bit7 compressed, bit6 infinity,    */
+/* bit5 set iff y is the lexicographically larger root (y > (p-1)/2).      */
+/* Pinned by kzg/test/kzg_test.cpp:38-42 and :64-81.                        */
+/* ------------------------------------------------------------------------ */
+
+int orc_g1_compress(const uint8_t* point96, uint8_t* out48) {
+    const field* F = &F_BLS_FP;
+    int any = 0;
+    for (int i = 0; i < 96; ++i) any |= point96[i];
+    if (!any) {
+        memset(out48, 0, 48);
+        out48[0] = 0xC0;
+        return 0;
+    }
+    fe y = fe_from_be(F, point96 + 48);
+    fe y2;
+    raw_add(F, &y2, &y, &y); /* 2y < 2^384 since y < p < 2^381 */
+    memcpy(out48, point96, 48);
+    out48[0] |= 0x80;
+    if (fe_cmp(F, &y2, &F->p) > 0) out48[0] |= 0x20;
+    return 0;
+}
+
+int orc_kzg_commit(const uint8_t* evals, size_t n, const uint8_t* srs,
+                   uint8_t* commit48) {
+    uint8_t* coeffs = (uint8_t*)malloc(32 * (n ? n : 1));
+    memcpy(coeffs, evals, 32 * n);
+    int rc = orc_ntt(ORC_CURVE_BLS12_381, coeffs, n, 1, 0);
+    if (rc) {
+        free(coeffs);
+        return rc;
+    }
+    uint8_t pt[96];
+    rc = orc_msm(ORC_CURVE_BLS12_381, coeffs, srs, n, pt);
+    free(coeffs);
+    if (rc) return rc;
+    return orc_g1_compress(pt, commit48);
+}

@@ -1,0 +1,156 @@
+"""ctypes wrappers for the CPU checker (oracle/).  Test infrastructure only.
+
+  orc  -> oracle/_build/liboracle.so   (C restatement of the reference path)
+  ref  -> oracle/_ref/libref_msm.so    (the reference's own CPU MSM, built
+                                        unmodified from its sources)
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+ORC_PATH = ROOT / "oracle" / "_build" / "liboracle.so"
+REF_PATH = ROOT / "oracle" / "_ref" / "libref_msm.so"
+
+_orc = None
+_ref = None
+
+
+def orc() -> ctypes.CDLL:
+    global _orc
+    if _orc is None:
+        if not ORC_PATH.exists():
+            subprocess.run(["make", "-C", str(ROOT / "oracle"), "all"], check=True,
+                           capture_output=True)
+        L = ctypes.CDLL(str(ORC_PATH))
+        sz = ctypes.c_size_t
+        for name, args in {
+            "orc_msm": [ctypes.c_uint32, ctypes.c_char_p, ctypes.c_char_p, sz, ctypes.c_void_p],
+            "orc_msm_naive": [ctypes.c_uint32, ctypes.c_char_p, ctypes.c_char_p, sz, ctypes.c_void_p],
+            "orc_g1_mul_gen": [ctypes.c_uint32, ctypes.c_char_p, ctypes.c_void_p],
+            "orc_g1_mul": [ctypes.c_uint32, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_void_p],
+            "orc_g1_add": [ctypes.c_uint32, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_void_p],
+            "orc_g1_on_curve": [ctypes.c_uint32, ctypes.c_char_p],
+            "orc_ntt": [ctypes.c_uint32, ctypes.c_void_p, sz, ctypes.c_int, ctypes.c_int],
+            "orc_dft": [ctypes.c_uint32, ctypes.c_void_p, sz, ctypes.c_int, ctypes.c_int],
+            "orc_root_of_unity": [ctypes.c_uint32, sz, ctypes.c_void_p],
+            "orc_g1_compress": [ctypes.c_char_p, ctypes.c_void_p],
+            "orc_kzg_commit": [ctypes.c_char_p, sz, ctypes.c_char_p, ctypes.c_void_p],
+            "orc_fr_powers": [ctypes.c_uint32, ctypes.c_char_p, sz, ctypes.c_void_p],
+            "orc_field_mul": [ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_void_p],
+            "orc_field_inv": [ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p],
+        }.items():
+            f = getattr(L, name)
+            f.restype = ctypes.c_int
+            f.argtypes = args
+        _orc = L
+    return _orc
+
+
+def ref_available() -> bool:
+    return REF_PATH.exists()
+
+
+def ref() -> ctypes.CDLL:
+    global _ref
+    if _ref is None:
+        L = ctypes.CDLL(str(REF_PATH))
+        sz = ctypes.c_size_t
+        L.ref_msm.restype = ctypes.c_int
+        L.ref_msm.argtypes = [ctypes.c_uint32, ctypes.c_char_p, ctypes.c_char_p, sz, ctypes.c_void_p]
+        L.ref_msm_parallel.restype = ctypes.c_int
+        L.ref_msm_parallel.argtypes = [ctypes.c_uint32, ctypes.c_char_p, ctypes.c_char_p, sz,
+                                       ctypes.c_void_p, ctypes.c_int]
+        L.ref_g1_mul_gen.restype = ctypes.c_int
+        L.ref_g1_mul_gen.argtypes = [ctypes.c_uint32, ctypes.c_char_p, ctypes.c_void_p]
+        _ref = L
+    return _ref
+
+
+PB = {1: 64, 2: 96}
+
+
+def msm(curve: int, scalars: bytes, points: bytes, n: int) -> bytes:
+    out = ctypes.create_string_buffer(PB[curve])
+    rc = orc().orc_msm(curve, scalars, points, n, out)
+    assert rc == 0, rc
+    return out.raw
+
+
+def msm_naive(curve: int, scalars: bytes, points: bytes, n: int) -> bytes:
+    out = ctypes.create_string_buffer(PB[curve])
+    assert orc().orc_msm_naive(curve, scalars, points, n, out) == 0
+    return out.raw
+
+
+def ref_msm(curve: int, scalars: bytes, points: bytes, n: int, threads: int = 1) -> bytes:
+    out = ctypes.create_string_buffer(PB[curve])
+    if threads <= 1:
+        rc = ref().ref_msm(curve, scalars, points, n, out)
+    else:
+        rc = ref().ref_msm_parallel(curve, scalars, points, n, out, threads)
+    assert rc == 0, rc
+    return out.raw
+
+
+def g1_mul_gen(curve: int, k: int) -> bytes:
+    out = ctypes.create_string_buffer(PB[curve])
+    assert orc().orc_g1_mul_gen(curve, k.to_bytes(32, "little"), out) == 0
+    return out.raw
+
+
+def g1_mul(curve: int, point: bytes, k: int) -> bytes:
+    out = ctypes.create_string_buffer(PB[curve])
+    assert orc().orc_g1_mul(curve, point, k.to_bytes(32, "little"), out) == 0
+    return out.raw
+
+
+def g1_add(curve: int, p: bytes, q: bytes) -> bytes:
+    out = ctypes.create_string_buffer(PB[curve])
+    assert orc().orc_g1_add(curve, p, q, out) == 0
+    return out.raw
+
+
+def on_curve(curve: int, p: bytes) -> bool:
+    return orc().orc_g1_on_curve(curve, p) == 1
+
+
+def ntt(curve: int, data: bytes, inverse: bool = False, coset: bool = False) -> bytes:
+    buf = ctypes.create_string_buffer(bytes(data), len(data))
+    rc = orc().orc_ntt(curve, buf, len(data) // 32, int(inverse), int(coset))
+    assert rc == 0, rc
+    return buf.raw
+
+
+def dft(curve: int, data: bytes, inverse: bool = False, coset: bool = False) -> bytes:
+    buf = ctypes.create_string_buffer(bytes(data), len(data))
+    assert orc().orc_dft(curve, buf, len(data) // 32, int(inverse), int(coset)) == 0
+    return buf.raw
+
+
+def compress(point96: bytes) -> bytes:
+    out = ctypes.create_string_buffer(48)
+    assert orc().orc_g1_compress(point96, out) == 0
+    return out.raw
+
+
+def kzg_commit(evals: bytes, srs: bytes) -> bytes:
+    out = ctypes.create_string_buffer(48)
+    rc = orc().orc_kzg_commit(evals, len(evals) // 32, srs, out)
+    assert rc == 0, rc
+    return out.raw
+
+
+def fr_powers(curve: int, tau: bytes, n: int) -> bytes:
+    out = ctypes.create_string_buffer(32 * n)
+    assert orc().orc_fr_powers(curve, tau, n, out) == 0
+    return out.raw
+
+
+# Field moduli for host-side checks (canonical integers).
+FR = {2: 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001,
+      1: 21888242871839275222246405745257275088548364400416034343698204186575808495617}
+FP = {2: 0x1A0111EA397FE69A4B1BA7B6434BACD764774B84F38512BF6730D2A0F6B0F6241EABFFFEB153FFFFB9FEFFFFFFFFAAAB,
+      1: 21888242871839275222246405745257275088696311157297823662689037894645226208583}

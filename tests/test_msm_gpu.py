@@ -1,0 +1,154 @@
+"""GPU MSM parity: gpukit_multi_pippenger (CUDA body, via the C ABI) against
+the reference's CPU MSM and the committed golden vectors, bit-exact."""
+from __future__ import annotations
+
+import ctypes
+import gzip
+import json
+import random
+from pathlib import Path
+
+import pytest
+
+import _oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "golden.json.gz"
+
+
+def kb():
+    import crypto_b200
+    return crypto_b200
+
+
+def rand_points(curve: int, n: int, seed: int) -> bytes:
+    """n distinct points k_i * G from the CUDA fixed-base path, validated on
+    a subsample against the oracle's ladder."""
+    import torch
+    k = kb()
+    sc = k.gen_scalars(curve, seed, n)
+    d_sc = torch.frombuffer(bytearray(sc), dtype=torch.uint8).cuda()
+    d_pts = torch.empty(n * O.PB[curve], dtype=torch.uint8, device="cuda")
+    rc = k.lib().kb200_g1_fixed_base_device(curve, d_sc.data_ptr(), n, d_pts.data_ptr(), None)
+    assert rc == 0, k.last_error()
+    torch.cuda.synchronize()
+    pts = bytes(d_pts.cpu().numpy().tobytes())
+    pb = O.PB[curve]
+    for i in sorted({0, n // 2, n - 1}):
+        kk = int.from_bytes(sc[32 * i:32 * i + 32], "little")
+        assert pts[pb * i:pb * (i + 1)] == O.g1_mul_gen(curve, kk), i
+    return pts
+
+
+def test_golden_vectors(cuda_lib):
+    with gzip.open(GOLDEN, "rt") as f:
+        cases = json.load(f)["msm"]
+    for c in cases:
+        got = kb().gpukit_multi_pippenger(c["curve"], bytes.fromhex(c["scalars"]),
+                                          bytes.fromhex(c["points"]), c["n"])
+        assert got.hex() == c["expected"], (c["curve"], c["n"], c["mode"])
+
+
+@pytest.mark.parametrize("curve", [1, 2])
+def test_reference_harness_sizes(cuda_lib, curve):
+    """Sizes of gpukit/test/multi_pippenger_test.cpp:37 with its scalar mask."""
+    rng = random.Random(100 + curve)
+    pts_all = rand_points(curve, 4096, seed=31 + curve)
+    pb = O.PB[curve]
+    for n in (1, 2, 8, 64, 256, 1024, 4096):
+        pts = pts_all[:pb * n]
+        scs = b"".join((rng.getrandbits(256) & ((1 << 252) - 1)).to_bytes(32, "little")
+                       for _ in range(n))
+        want = O.ref_msm(curve, scs, pts, n, threads=8) if O.ref_available() else O.msm(curve, scs, pts, n)
+        assert kb().gpukit_multi_pippenger(curve, scs, pts, n) == want, n
+
+
+@pytest.mark.parametrize("curve", [1, 2])
+def test_full_range_scalars_reproduce_reference_carry(cuda_lib, curve):
+    """Scalars >= 2^255 at sizes whose reference window is 4 or 8 bits."""
+    rng = random.Random(9)
+    pts_all = rand_points(curve, 1500, seed=77)
+    pb = O.PB[curve]
+    for n in (2, 8, 9, 700, 1500):
+        pts = pts_all[:pb * n]
+        scs = b"".join(rng.getrandbits(256).to_bytes(32, "little") for _ in range(n))
+        assert kb().gpukit_multi_pippenger(curve, scs, pts, n) == O.msm(curve, scs, pts, n), n
+
+
+@pytest.mark.parametrize("curve", [1, 2])
+def test_edge_cases(cuda_lib, curve):
+    pb = O.PB[curve]
+    r = O.FR[curve]
+    g = O.g1_mul_gen(curve, 1)
+    p = O.g1_mul_gen(curve, 123456789)
+    neg_p = O.g1_mul_gen(curve, r - 123456789)
+    zero = bytes(pb)
+    cases = [
+        ([g], [0]),                                   # zero scalar -> identity
+        ([zero], [5]),                                # identity point
+        ([p, p, p, p], [3, 3, 3, 3]),                 # same point in one bucket (doubling)
+        ([p, neg_p], [7, 7]),                         # P + (-P) in one bucket -> infinity
+        ([p, neg_p, g], [7, 7, 1]),
+        ([g] * 64, [1] * 64),                         # every entry in one bucket
+        ([g, p], [r - 1, r]),                         # r - 1 and r itself
+        ([g, p], [(1 << 256) - 1, 1 << 255]),         # top of the 256-bit range
+    ]
+    for pts, scs in cases:
+        P = b"".join(pts)
+        S = b"".join(s.to_bytes(32, "little") for s in scs)
+        assert kb().gpukit_multi_pippenger(curve, S, P, len(pts)) == O.msm(curve, S, P, len(pts))
+
+
+def test_n_zero_and_errors(cuda_lib):
+    k = kb()
+    out = ctypes.create_string_buffer(96)
+    assert k.msm_rc(2, None, None, 0, out) == 0
+    assert out.raw == bytes(96)
+    assert k.msm_rc(2, None, None, 1, out) == -1          # GPUKIT_ERR_NULL_ARG
+    assert k.msm_rc(2, b"\0" * 32, b"\0" * 96, 1, None) == -1
+    assert k.msm_rc(0, b"\0" * 32, b"\0" * 64, 1, out) == -5   # secp256k1: NOTIMPL
+    assert k.msm_rc(3, b"\0" * 32, b"\0" * 64, 1, out) == -5   # banderwagon: NOTIMPL
+    assert k.msm_rc(9, b"\0" * 32, b"\0" * 64, 1, out) == -3   # unknown: BACKEND
+
+
+@pytest.mark.parametrize("curve", [1, 2])
+def test_skewed_scalars(cuda_lib, curve):
+    """50% of scalars in {0,1}, 20% below 2^64, rest uniform (bucket imbalance)."""
+    n = 1 << 14
+    pts = rand_points(curve, n, seed=5)
+    scs = kb().gen_scalars(curve, 1234, n, kind=1)
+    want = O.ref_msm(curve, scs, pts, n, threads=8) if O.ref_available() else O.msm(curve, scs, pts, n)
+    assert kb().gpukit_multi_pippenger(curve, scs, pts, n) == want
+
+
+@pytest.mark.parametrize("curve", [1, 2])
+def test_2_16_against_reference(cuda_lib, curve):
+    n = 1 << 16
+    pts = rand_points(curve, n, seed=8)
+    scs = kb().gen_scalars(curve, 4321, n)
+    want = O.ref_msm(curve, scs, pts, n, threads=8) if O.ref_available() else O.msm(curve, scs, pts, n)
+    assert kb().gpukit_multi_pippenger(curve, scs, pts, n) == want
+
+
+@pytest.mark.parametrize("curve", [1, 2])
+def test_linearity_large(cuda_lib, curve):
+    """Size-independent property at a large size: MSM(s, P) + MSM(t, P) ==
+    MSM(s + t mod r, P), and splitting the input gives the same sum."""
+    n = 1 << 18
+    pts = rand_points(curve, n, seed=21)
+    s = kb().gen_scalars(curve, 1, n)
+    t = kb().gen_scalars(curve, 2, n)
+    r = O.FR[curve]
+    st = b"".join(((int.from_bytes(s[32 * i:32 * i + 32], "little") +
+                    int.from_bytes(t[32 * i:32 * i + 32], "little")) % r).to_bytes(32, "little")
+                  for i in range(n))
+    a = kb().gpukit_multi_pippenger(curve, s, pts, n)
+    b = kb().gpukit_multi_pippenger(curve, t, pts, n)
+    c = kb().gpukit_multi_pippenger(curve, st, pts, n)
+    assert O.g1_add(curve, a, b) == c
+    pb = O.PB[curve]
+    h = n // 2
+    lo = kb().gpukit_multi_pippenger(curve, s[:32 * h], pts[:pb * h], h)
+    hi = kb().gpukit_multi_pippenger(curve, s[32 * h:], pts[pb * h:], n - h)
+    assert O.g1_add(curve, lo, hi) == a
