@@ -66,6 +66,16 @@ def lib() -> ctypes.CDLL:
             "kb200_device_available": (c.c_int, []),
             "kb200_msm_window": (c.c_int, [c.c_uint32, sz]),
             "kb200_launch_count": (c.c_ulonglong, []),
+            "kzg_server_create": (vp, [sz, c.c_int, sz]),
+            "kzg_server_submit": (c.c_int, [vp, u8p, sz, c.POINTER(c.c_uint64)]),
+            "kzg_server_wait": (c.c_int, [vp, c.c_uint64, vp, c.POINTER(c.c_double), c.c_double]),
+            "kzg_server_stats": (c.c_int, [vp, c.POINTER(c.c_double), c.POINTER(c.c_double),
+                                           c.POINTER(c.c_double), c.POINTER(c.c_uint64), c.c_int]),
+            "kzg_server_destroy": (c.c_int, [vp]),
+            "kb200_autotune": (c.c_int, [c.c_uint32, c.c_int, c.c_int, c.c_char_p]),
+            "kb200_autotune_load": (c.c_int, [c.c_char_p]),
+            "kb200_tune_get": (c.c_int, [c.c_int, c.c_uint32, c.c_int]),
+            "kb200_tune_set": (None, [c.c_int, c.c_uint32, c.c_int, c.c_int]),
             "kb200_profile_enable": (None, [c.c_int]),
             "kb200_msm_stage_ms": (c.c_int, [c.c_uint32, c.POINTER(c.c_float), c.c_int]),
         }
@@ -170,10 +180,57 @@ def profile_enable(on: bool) -> None:
     lib().kb200_profile_enable(int(on))
 
 
-MSM_STAGES = ("wire_to_table", "recode", "sort", "accumulate", "fold", "reduce_combine")
+MSM_STAGES = ("wire_to_table", "recode", "sort", "accumulate", "fold", "reduce_blocks",
+              "reduce_windows", "combine")
 
 
 def msm_stage_ms(curve: int) -> dict[str, float]:
-    buf = (ctypes.c_float * 8)()
-    k = lib().kb200_msm_stage_ms(curve, buf, 8)
+    buf = (ctypes.c_float * 16)()
+    k = lib().kb200_msm_stage_ms(curve, buf, 16)
     return {MSM_STAGES[i]: float(buf[i]) for i in range(max(k, 0))}
+
+
+# ---- serving ------------------------------------------------------------------
+
+class KzgServer:
+    """Continuous-batching commit server over the resident SRS (C ABI
+    kzg_server_*).  submit() returns a ticket; wait() returns (commit, ms)."""
+
+    def __init__(self, max_batch: int = 64, slots: int = 2, mem_budget: int = 0):
+        self.h = lib().kzg_server_create(max_batch, slots, mem_budget)
+        if not self.h:
+            raise KinetB200Error("kzg_server_create", -4, last_error())
+
+    def submit(self, evals: bytes) -> int:
+        t = ctypes.c_uint64()
+        _check("kzg_server_submit", lib().kzg_server_submit(self.h, evals, len(evals) // 32,
+                                                            ctypes.byref(t)))
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: float = -1.0):
+        out = ctypes.create_string_buffer(48)
+        lat = ctypes.c_double()
+        rc = lib().kzg_server_wait(self.h, ticket, out, ctypes.byref(lat), timeout_ms)
+        if rc == 1:
+            return None
+        _check("kzg_server_wait", rc)
+        return out.raw, lat.value
+
+    def stats(self, reset: bool = False) -> dict:
+        p50, p99, cps = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        done = ctypes.c_uint64()
+        _check("kzg_server_stats", lib().kzg_server_stats(self.h, ctypes.byref(p50), ctypes.byref(p99),
+                                                          ctypes.byref(cps), ctypes.byref(done), int(reset)))
+        return {"p50_ms": p50.value, "p99_ms": p99.value, "commits_per_s": cps.value,
+                "completed": done.value}
+
+    def close(self) -> None:
+        if self.h:
+            lib().kzg_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

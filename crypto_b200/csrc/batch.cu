@@ -1,0 +1,197 @@
+// Batched KZG commits: see batch.cuh.
+#include "batch.cuh"
+#include "msm.cuh"
+#include "ntt.cuh"
+#include "runtime.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+
+namespace kb200 {
+
+namespace {
+
+struct Signature {
+    std::vector<size_t> sizes;
+    const uint32_t* srs;
+    bool operator<(const Signature& o) const {
+        if (srs != o.srs) return srs < o.srs;
+        return sizes < o.sizes;
+    }
+};
+
+struct Prepared {
+    MsmBatchPlan* plan = nullptr;
+    std::vector<std::pair<size_t, size_t>> classes;  // (n, count) per size class
+    std::vector<size_t> class_off;                   // start in the offsets list
+    DevBuf d_vec_off;                                // element offsets grouped by class
+    size_t total = 0;                                // evaluations
+    cudaGraphExec_t graph = nullptr;
+    ~Prepared() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (plan) msm_batch_plan_destroy(plan);
+        d_vec_off.release();
+    }
+};
+
+}  // namespace
+
+class CommitBatcher {
+   public:
+    NttEngine* ntt = nullptr;
+    MsmEngine* msm = nullptr;
+    DevBuf evals, scratch, out_wire, out_comp;
+    HostBuf h_out;
+    std::map<Signature, std::unique_ptr<Prepared>> cache;
+    Prepared* current = nullptr;
+    unsigned long long graph_launches = 0, graph_captures = 0;
+    ~CommitBatcher() {
+        cache.clear();
+        if (ntt) ntt_engine_destroy(ntt);
+        if (msm) msm_engine_destroy(msm);
+        for (DevBuf* b : {&evals, &scratch, &out_wire, &out_comp}) b->release();
+        h_out.release();
+    }
+};
+
+CommitBatcher* commit_batcher_create() {
+    auto* b = new CommitBatcher();
+    b->ntt = ntt_engine_create(2);
+    b->msm = msm_engine_create(2);
+    return b;
+}
+
+void commit_batcher_destroy(CommitBatcher* b) { delete b; }
+
+static Prepared* prepare(CommitBatcher* B, const size_t* sizes, size_t count,
+                         const uint32_t* srs, size_t srs_n, cudaStream_t st) {
+    Signature sig{std::vector<size_t>(sizes, sizes + count), srs};
+    auto it = B->cache.find(sig);
+    if (it != B->cache.end()) return it->second.get();
+    auto P = std::make_unique<Prepared>();
+    std::vector<MsmItem> items(count);
+    std::map<size_t, std::vector<unsigned long long>> by_size;
+    size_t off = 0;
+    for (size_t i = 0; i < count; ++i) {
+        const size_t n = sizes[i];
+        if (n == 0 || (n & (n - 1))) throw std::invalid_argument("kzg: sizes must be powers of two");
+        if (n > srs_n) throw std::invalid_argument("kzg: SRS shorter than the polynomial");
+        items[i] = MsmItem{off, n, 0};
+        by_size[n].push_back(off);
+        off += n;
+    }
+    P->total = off;
+    std::vector<unsigned long long> offs;
+    for (auto& kv : by_size) {
+        P->class_off.push_back(offs.size());
+        P->classes.emplace_back(kv.first, kv.second.size());
+        offs.insert(offs.end(), kv.second.begin(), kv.second.end());
+        ntt_prepare(B->ntt, kv.first, 0, st);
+    }
+    P->d_vec_off.reserve(std::max<size_t>(1, offs.size()) * 8, st);
+    if (!offs.empty())
+        KB_CUDA(cudaMemcpyAsync(P->d_vec_off.ptr, offs.data(), offs.size() * 8,
+                                cudaMemcpyHostToDevice, st));
+    MsmOptions opt;
+    P->plan = msm_batch_plan_create(2, items.data(), count, opt, st);
+    msm_engine_reserve(B->msm, P->plan, st);
+    B->evals.reserve(std::max<size_t>(1, off) * 32 + 16, st);
+    B->scratch.reserve(std::max<size_t>(1, off) * 32 + 16, st);
+    B->out_wire.reserve(std::max<size_t>(1, count) * 96, st);
+    B->out_comp.reserve(std::max<size_t>(1, count) * 48, st);
+    B->h_out.reserve(std::max<size_t>(1, count) * 48, st);
+    KB_CUDA(cudaStreamSynchronize(st));
+    Prepared* raw = P.get();
+    B->cache[sig] = std::move(P);
+    if (B->cache.size() > 32) {
+        // Bound the cache; keep the current signature.
+        for (auto i2 = B->cache.begin(); i2 != B->cache.end();) {
+            if (i2->second.get() != raw)
+                i2 = B->cache.erase(i2);
+            else
+                ++i2;
+        }
+    }
+    return raw;
+}
+
+// The device work of one batch: grouped inverse NTTs then the batched MSM.
+static void enqueue(CommitBatcher* B, Prepared* P, const uint32_t* srs, cudaStream_t st) {
+    for (size_t k = 0; k < P->classes.size(); ++k) {
+        const size_t n = P->classes[k].first, cnt = P->classes[k].second;
+        ntt_run_list(B->ntt, B->evals.as<uint32_t>(), n, /*inverse=*/1, /*coset=*/0, cnt,
+                     P->d_vec_off.as<unsigned long long>() + P->class_off[k],
+                     B->scratch.as<uint32_t>(), st);
+    }
+    msm_engine_launch(B->msm, P->plan, B->evals.as<uint8_t>(), srs, B->out_wire.as<uint8_t>(),
+                      B->out_comp.as<uint8_t>(), st);
+}
+
+static void run(CommitBatcher* B, Prepared* P, const uint32_t* srs, cudaStream_t st,
+                bool use_graph) {
+    if (!use_graph) {
+        enqueue(B, P, srs, st);
+        return;
+    }
+    if (!P->graph) {
+        cudaGraph_t g = nullptr;
+        KB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        try {
+            enqueue(B, P, srs, st);
+        } catch (...) {
+            cudaStreamEndCapture(st, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        KB_CUDA(cudaStreamEndCapture(st, &g));
+        const cudaError_t err = cudaGraphInstantiate(&P->graph, g, 0);
+        cudaGraphDestroy(g);
+        KB_CUDA(err);
+        ++B->graph_captures;
+    }
+    KB_CUDA(cudaGraphLaunch(P->graph, st));
+    ++B->graph_launches;
+}
+
+void commit_batch_host(CommitBatcher* B, const uint8_t* h_evals, const size_t* sizes,
+                       size_t count, const uint32_t* srs, size_t srs_n, uint8_t* h_out,
+                       cudaStream_t st, bool use_graph) {
+    if (count == 0) return;
+    Prepared* P = prepare(B, sizes, count, srs, srs_n, st);
+    B->current = P;
+    KB_CUDA(cudaMemcpyAsync(B->evals.ptr, h_evals, P->total * 32, cudaMemcpyHostToDevice, st));
+    run(B, P, srs, st, use_graph);
+    KB_CUDA(cudaMemcpyAsync(B->h_out.ptr, B->out_comp.ptr, count * 48, cudaMemcpyDeviceToHost, st));
+    KB_CUDA(cudaStreamSynchronize(st));
+    std::memcpy(h_out, B->h_out.ptr, count * 48);
+}
+
+uint8_t* commit_batch_device_input(CommitBatcher* B, const size_t* sizes, size_t count,
+                                   const uint32_t* srs, size_t srs_n, cudaStream_t st) {
+    Prepared* P = prepare(B, sizes, count, srs, srs_n, st);
+    B->current = P;
+    return B->evals.as<uint8_t>();
+}
+
+void commit_batch_device(CommitBatcher* B, const size_t* sizes, size_t count,
+                         const uint32_t* srs, size_t srs_n, cudaStream_t st, bool use_graph) {
+    if (count == 0) return;
+    Prepared* P = prepare(B, sizes, count, srs, srs_n, st);
+    B->current = P;
+    run(B, P, srs, st, use_graph);
+}
+
+const uint8_t* commit_batch_device_output(CommitBatcher* B) { return B->out_comp.as<uint8_t>(); }
+
+size_t commit_batch_scratch_bytes(const size_t* sizes, size_t count) {
+    size_t total = 0;
+    for (size_t i = 0; i < count; ++i) total += sizes[i];
+    return 2 * total * 32 + count * 144 + msm_scratch_bytes(2, sizes, count);
+}
+
+unsigned long long commit_batcher_graph_launches(CommitBatcher* b) { return b->graph_launches; }
+unsigned long long commit_batcher_graph_captures(CommitBatcher* b) { return b->graph_captures; }
+
+}  // namespace kb200

@@ -2,6 +2,7 @@
 // device engines.  Per device there is one context (stream, engines, I/O
 // staging, resident SRS) guarded by a mutex.
 #include "../../include/kinet_b200/crypto_b200.h"
+#include "batch.cuh"
 #include "curve.cuh"
 #include "kzg.cuh"
 #include "msm.cuh"
@@ -35,6 +36,7 @@ struct DeviceCtx {
     MsmEngine* msm[3] = {nullptr, nullptr, nullptr};
     NttEngine* ntt[3] = {nullptr, nullptr, nullptr};
     FixedBase* fb[3] = {nullptr, nullptr, nullptr};
+    CommitBatcher* batcher = nullptr;
     DevBuf d_a, d_b, d_out, d_srs, d_tmp;
     HostBuf h_a, h_b, h_out;
     size_t srs_n = 0;
@@ -50,6 +52,10 @@ struct DeviceCtx {
     FixedBase* fb_for(int curve) {
         if (!fb[curve]) fb[curve] = fixed_base_create(curve, stream);
         return fb[curve];
+    }
+    CommitBatcher* batcher_get() {
+        if (!batcher) batcher = commit_batcher_create();
+        return batcher;
     }
 };
 
@@ -95,6 +101,13 @@ static int guarded(int backend_err, int size_err, int internal_err, Fn&& fn) {
         set_last_error(e.what());
         return internal_err;
     }
+}
+
+void resident_srs(const uint32_t** table, size_t* n) {
+    DeviceCtx* c = get_ctx();
+    std::lock_guard<std::mutex> lk(c->mu);
+    *table = c->srs_n ? c->d_srs.as<uint32_t>() : nullptr;
+    *n = c->srs_n;
 }
 
 static int wire_bytes(uint32_t curve) { return curve == 2 ? 96 : 64; }
@@ -292,34 +305,18 @@ int kzg_commit_fr(const uint8_t* evals32le, size_t n, uint8_t commit48[48]) {
 int kzg_commit_batch(const uint8_t* evals32le, const size_t* sizes, size_t count,
                      uint8_t* commits48) {
     if (count && (!evals32le || !sizes || !commits48)) return KB200_CRYPTO_ERR_INPUT;
-    size_t total = 0;
-    for (size_t i = 0; i < count; ++i) {
+    for (size_t i = 0; i < count; ++i)
         if (!is_pow2(sizes[i])) return KB200_CRYPTO_ERR_LENGTH;
-        total += sizes[i];
-    }
+    if (count == 0) return KB200_CRYPTO_OK;
     return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_LENGTH, KB200_CRYPTO_ERR_INTERNAL,
                    [&]() -> int {
                        DeviceCtx* c = get_ctx();
                        std::lock_guard<std::mutex> lk(c->mu);
                        for (size_t i = 0; i < count; ++i)
                            if (sizes[i] > c->srs_n) return KB200_CRYPTO_ERR_LENGTH;
-                       cudaStream_t st = c->stream;
-                       c->d_a.reserve(total * 32 + 16, st);
-                       c->d_out.reserve(count * 48 + 256, st);
-                       c->h_out.reserve(count * 48 + 256, st);
-                       if (total)
-                           KB_CUDA(cudaMemcpyAsync(c->d_a.ptr, evals32le, total * 32,
-                                                   cudaMemcpyHostToDevice, st));
-                       size_t off = 0;
-                       for (size_t i = 0; i < count; ++i) {
-                           commit_on_device(c, c->d_a.as<uint32_t>() + off * 8, sizes[i],
-                                            c->d_out.as<uint8_t>() + 48 * i, st);
-                           off += sizes[i];
-                       }
-                       KB_CUDA(cudaMemcpyAsync(c->h_out.ptr, c->d_out.ptr, count * 48,
-                                               cudaMemcpyDeviceToHost, st));
-                       KB_CUDA(cudaStreamSynchronize(st));
-                       std::memcpy(commits48, c->h_out.ptr, count * 48);
+                       commit_batch_host(c->batcher_get(), evals32le, sizes, count,
+                                         c->d_srs.as<uint32_t>(), c->srs_n, commits48, c->stream,
+                                         /*use_graph=*/true);
                        return KB200_CRYPTO_OK;
                    });
 }

@@ -312,11 +312,18 @@ KB_DEV void fe_from_mont(Fe<F>& r, const Fe<F>& a) {
     fe_mul<F>(r, a, one);
 }
 
-// Exponent word i of p - 2 (p is odd and its low word is >= 2 for all four
-// moduli, so only word 0 changes).
+// Exponent word i of p - 2, with the borrow propagated (BLS12-381 r has
+// low word 1, so p - 2 borrows from word 1 there).
 template <class F>
 KB_HD constexpr uint32_t pm2_word(int i) {
-    return i == 0 ? F::P(0) - 2u : F::P(i);
+    uint32_t borrow = 2;
+    uint32_t w = 0;
+    for (int k = 0; k <= i; ++k) {
+        const uint32_t pk = F::P(k);
+        w = pk - borrow;
+        borrow = pk < borrow ? 1u : 0u;
+    }
+    return w;
 }
 
 // a^(p-2) by left-to-right square-and-multiply with 4-bit fixed windows.

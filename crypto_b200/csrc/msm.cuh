@@ -1,19 +1,24 @@
-// G1 multi-scalar multiplication (signed-digit Pippenger) on one GPU.
+// G1 multi-scalar multiplication (signed-digit Pippenger) on one GPU, for a
+// batch of independent MSMs in one pass (a single MSM is a batch of one).
 //
-// Pipeline, all on device, all launched on the caller's stream:
-//   1. wire -> table   : big-endian affine points -> Montgomery affine words
-//   2. recode          : each scalar -> W signed c-bit digits, one
-//                        (bucket, point|sign) entry per non-zero digit
-//   3. histogram/scan  : per-bucket counts -> bucket offsets
-//   4. scatter         : counting sort of the entries by bucket
-//   5. accumulate      : buckets split into segments of <= K entries; one
-//                        thread sums one segment with mixed XYZZ additions
-//   6. segment levels  : partial sums of buckets that span several segments
-//                        are folded K2 at a time until one sum per bucket
-//   7. reduce          : per window, sum_k (k+1) * B_k via grouped running
-//                        sums (groups of S buckets), then a tree per window
-//   8. combine         : Horner over windows (c doublings each), affine
-//                        normalisation and big-endian (and compressed) encode
+// Pipeline, all on device, all queued on the caller's stream:
+//   1. recode          : each scalar -> W signed c-bit digits (c per item);
+//                        one (global bucket, point|sign) entry per non-zero
+//                        digit; buckets of all items share one key space
+//   2. histogram/scan  : per-bucket counts -> bucket offsets
+//   3. scatter         : counting sort of the entries by bucket
+//   4. accumulate      : buckets split into near-equal segments of <= K
+//                        entries, one thread per segment, mixed XYZZ adds;
+//                        a persistent grid pulls segments from a device
+//                        work counter
+//   5. fold            : buckets with more than K2 segments are folded K2
+//                        partial sums at a time (skewed inputs); smaller
+//                        splits are summed inside stage 6
+//   6. reduce          : per window, sum_k (k+1) B_k: running sums per
+//                        thread, shared-memory suffix scan and trees per
+//                        block, then one block per window over its blocks
+//   7. combine         : per item, Horner over windows (c doublings each),
+//                        affine normalisation, big-endian / compressed out
 // The digit recoding follows gpukit/cpp/cpu_reference/multi_pippenger.cpp:90-134
 // (digits in (-2^(c-1), 2^(c-1)], carry into the next window), with enough
 // windows (ceil(257 / c)) that no carry leaves the top window.
@@ -22,6 +27,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 namespace kb200 {
 
@@ -29,13 +35,7 @@ struct MsmPlan {
     int c = 0;          // window bits
     int W = 0;          // windows
     uint32_t M = 0;     // buckets per window (2^(c-1))
-    uint32_t B = 0;     // W * M
-    int K = 32;         // entries per level-1 segment
-    int K2 = 8;         // fan-in of later segment levels
-    int levels = 0;     // segment levels after level 1
-    int S = 8;          // buckets per reduction group
-    uint32_t G = 0;     // reduction groups per window
-    size_t seg_cap = 0; // upper bound on level-1 segments
+    uint32_t M_top = 0; // live buckets in the top window (its digits are small)
 };
 
 struct MsmOptions {
@@ -51,24 +51,45 @@ struct MsmOptions {
 
 // Reference window size for n: multi_pippenger.cpp:69-88.
 int reference_best_c(size_t n);
-
+// Window plan for one MSM of size n (autotuner cache, else cost model).
 MsmPlan make_msm_plan(int curve, size_t n, const MsmOptions& opt);
 
-// Device-side MSM.  scalars: n x 32 B little-endian; points: n x WIRE bytes
-// big-endian affine (all-zero = infinity); out_wire: WIRE bytes; out_comp:
-// 48-byte compressed encoding (BLS12-381 only, may be null).  All pointers
-// are device pointers; work is queued on `stream` and not synchronised.
+// One MSM of a batch: n scalars starting at scalar index `scalar_off` of the
+// batch's scalar array, against table rows point_off .. point_off + n - 1.
+struct MsmItem {
+    size_t scalar_off;
+    size_t n;
+    size_t point_off;
+};
+
+class MsmBatchPlan;
+// Builds the launch plan (descriptors uploaded to the device; synchronous).
+MsmBatchPlan* msm_batch_plan_create(int curve, const MsmItem* items, size_t count,
+                                    const MsmOptions& opt, cudaStream_t stream);
+void msm_batch_plan_destroy(MsmBatchPlan* p);
+size_t msm_batch_plan_count(const MsmBatchPlan* p);
+
 class MsmEngine;
 MsmEngine* msm_engine_create(int curve);
 void msm_engine_destroy(MsmEngine* e);
+// Allocates the engine scratch a plan needs (may synchronise the stream).
+void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t stream);
+// Queues the whole pipeline for a plan; no allocation and no host
+// synchronisation after msm_engine_reserve, so it can be captured in a
+// CUDA graph.  out_wire: count * WIRE bytes; out_comp: count * 48 bytes
+// (BLS12-381 only, may be null).
+void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_scalars,
+                       const uint32_t* d_table, uint8_t* d_out_wire, uint8_t* d_out_comp,
+                       cudaStream_t stream);
+
+// Convenience single-MSM entry points (plan cached per (n, options)).
 void msm_run_wire(MsmEngine* e, const uint8_t* d_scalars, const uint8_t* d_points, size_t n,
                   uint8_t* d_out_wire, uint8_t* d_out_comp, cudaStream_t stream,
                   const MsmOptions& opt);
-// Same with points already in the internal Montgomery table layout
-// (2N words per point) -- used for resident SRS tables.
 void msm_run_table(MsmEngine* e, const uint8_t* d_scalars, const uint32_t* d_table, size_t n,
                    uint8_t* d_out_wire, uint8_t* d_out_comp, cudaStream_t stream,
                    const MsmOptions& opt);
+
 // Convert wire points to the internal table layout (device to device).
 void points_wire_to_table(int curve, const uint8_t* d_wire, uint32_t* d_table, size_t n,
                           cudaStream_t stream);
@@ -79,7 +100,11 @@ void points_table_to_wire(int curve, const uint32_t* d_table, uint8_t* d_wire, s
 int msm_stage_ms(MsmEngine* e, float* out, int max);
 // Words per table entry for a curve.
 int table_words(int curve);
-// Scratch bytes the engine needs for an MSM of size n (admission control).
-size_t msm_scratch_bytes(int curve, size_t n);
+// Device scratch bytes an MSM batch of these sizes needs (admission control).
+size_t msm_scratch_bytes(int curve, const size_t* ns, size_t count);
+
+// Autotuner: record the best window for a size class (log2 n) and curve.
+void msm_tune_set(int curve, int log_n, int c);
+int msm_tune_get(int curve, int log_n);  // 0 if untuned
 
 }  // namespace kb200

@@ -1,0 +1,94 @@
+// Device-side descriptors and launcher table shared by the MSM host driver
+// (msm.cu) and the per-curve kernel units (msm_bls.cu, msm_bn.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace kb200 {
+
+constexpr uint32_t KEY_SENTINEL = 0xffffffffu;
+constexpr int RED_THREADS = 256;
+
+// One MSM of a batch.
+struct ItemDesc {
+    unsigned long long scalar_off;  // first scalar (element index) of the item
+    unsigned long long entry_base;  // first entry slot (W * n slots per item)
+    uint32_t n;
+    uint32_t point_off;             // first table row
+    uint32_t c, W, M;               // window bits, windows, buckets per window
+    uint32_t bucket_base;           // first global bucket of the item
+    uint32_t win_base;              // first WinDesc of the item
+    int32_t quirk_c;                // reference carry emulation (0, 4 or 8)
+};
+
+// One window of one item.
+struct WinDesc {
+    uint32_t bucket_base;  // global id of the window's bucket 0
+    uint32_t Mw;           // live buckets of the window
+    uint32_t log_S;        // buckets per thread in reduction stage 1
+    uint32_t blk_base;     // first stage-1 block of the window
+    uint32_t nb;           // stage-1 blocks (<= RED_THREADS)
+    uint32_t log_blk;      // log2(RED_THREADS << log_S)
+};
+
+struct BlkDesc {
+    uint32_t win;  // WinDesc index
+    uint32_t b;    // block index within the window
+};
+
+struct AccArgs {
+    const uint32_t* sorted;
+    const uint32_t* offsets;
+    const uint32_t* segoff;
+    uint32_t B;
+    const uint32_t* table;
+    uint32_t* partial;
+    uint32_t* bid;
+    uint32_t* buckets;
+    uint32_t* queue;
+};
+
+struct FoldArgs {
+    const uint32_t* bid;
+    const uint32_t* segoff;
+    uint32_t B;
+    int K2;
+    size_t seg_cap;
+    uint32_t* buckets;
+};
+
+struct RedArgs {
+    const uint32_t* segoff;
+    const uint32_t* buckets;
+    const uint32_t* partial;
+    int K2;
+    const WinDesc* wins;
+    const BlkDesc* blks;
+    uint32_t* blk_out;  // 2 XYZZ points per stage-1 block
+    uint32_t* win_out;  // 1 XYZZ point per window
+};
+
+struct MsmLaunchers {
+    void (*wire_to_table)(const uint8_t*, uint32_t*, size_t, cudaStream_t);
+    void (*table_to_wire)(const uint32_t*, uint8_t*, size_t, cudaStream_t);
+    void (*recode)(const ItemDesc*, uint32_t, unsigned long long, const uint32_t*,
+                   const uint32_t*, uint32_t*, uint32_t*, cudaStream_t);
+    void (*accumulate)(const AccArgs&, unsigned, cudaStream_t);
+    void (*fold)(const FoldArgs&, int, const uint32_t*, uint32_t*, cudaStream_t);
+    void (*reduce_blocks)(const RedArgs&, unsigned, cudaStream_t);
+    void (*reduce_windows)(const RedArgs&, unsigned, cudaStream_t);
+    void (*combine)(const ItemDesc*, uint32_t, const uint32_t*, uint8_t*, uint8_t*, cudaStream_t);
+    int (*accumulate_occupancy)();
+    int point_words;  // XYZZ point
+    int table_words;  // affine table row
+    int wire_bytes;
+};
+
+const MsmLaunchers& msm_launchers(int curve);
+
+// Raises a kernel's dynamic shared-memory limit once per device.
+void set_smem_attr(const void* kernel, size_t bytes);
+
+}  // namespace kb200

@@ -1,0 +1,527 @@
+// Curve-templated MSM kernels.  Included by msm_bls.cu and msm_bn.cu, which
+// instantiate one launcher table each (so the two curves compile in
+// parallel); the host driver in msm.cu only sees MsmLaunchers.
+#pragma once
+#include "curve.cuh"
+#include "msm_desc.cuh"
+#include "runtime.cuh"
+
+namespace kb200 {
+
+template <class C>
+__global__ void k_wire_to_table(const uint8_t* __restrict__ wire, uint32_t* __restrict__ table,
+                                size_t n) {
+    using F = typename C::F;
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    wire_to_table<C>(table + i * 2 * F::N, wire + i * C::WIRE);
+}
+
+template <class C>
+__global__ void k_table_to_wire(const uint32_t* __restrict__ table, uint8_t* __restrict__ wire,
+                                size_t n) {
+    using F = typename C::F;
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t* t = table + i * 2 * F::N;
+    uint8_t* o = wire + i * C::WIRE;
+    if (aff_is_inf_words<F>(t)) {
+        for (int k = 0; k < C::WIRE; ++k) o[k] = 0;
+        return;
+    }
+    Affine<F> a;
+    aff_load(a, t);
+    Fe<F> x, y;
+    fe_from_mont(x, a.x);
+    fe_from_mont(y, a.y);
+    fe_to_be_bytes(o, x);
+    fe_to_be_bytes(o + F::BYTES, y);
+}
+
+// Signed-digit recoding, one thread per scalar of the batch.  Entry (w, j)
+// of item i lives at entry_base_i + w * n_i + j.
+// quirk_c: 0, or the reference window size (4 or 8) whose dropped top carry
+// is reproduced by negating (s, P) -> (2^256 - s, -P) for s above the
+// carry threshold 0x8888...88 (c = 4) or 0x8080...80 (c = 8).
+template <class C>
+__global__ void k_recode(const ItemDesc* __restrict__ items, uint32_t n_items,
+                         unsigned long long total, const uint32_t* __restrict__ scalars,
+                         const uint32_t* __restrict__ table, uint32_t* __restrict__ keys,
+                         uint32_t* __restrict__ vals) {
+    using F = typename C::F;
+    const unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    // item: largest i with items[i].scalar_off <= g
+    uint32_t lo = 0, hi = n_items;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (items[mid].scalar_off <= g)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    const ItemDesc it = items[lo];
+    if (g < it.scalar_off || g - it.scalar_off >= it.n) return;  // gap between items
+    const uint32_t j = (uint32_t)(g - it.scalar_off);
+    const uint32_t row = it.point_off + j;
+    const bool inf = aff_is_inf_words<F>(table + (size_t)row * 2 * F::N);
+    uint32_t s[8];
+    const uint4* sp = reinterpret_cast<const uint4*>(scalars + g * 8);
+    const uint4 a = sp[0], b = sp[1];
+    s[0] = a.x; s[1] = a.y; s[2] = a.z; s[3] = a.w;
+    s[4] = b.x; s[5] = b.y; s[6] = b.z; s[7] = b.w;
+    uint32_t neg = 0;
+    if (it.quirk_c == 4 || it.quirk_c == 8) {
+        const uint32_t t = it.quirk_c == 4 ? 0x88888888u : 0x80808080u;
+        int gt = 0;
+#pragma unroll
+        for (int k = 7; k >= 0; --k) {
+            if (gt == 0) {
+                if (s[k] > t) gt = 1;
+                else if (s[k] < t) gt = -1;
+            }
+        }
+        if (gt == 1) {
+            uint32_t carry = 1;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint64_t v = (uint64_t)(~s[k]) + carry;
+                s[k] = (uint32_t)v;
+                carry = (uint32_t)(v >> 32);
+            }
+            neg = 1;
+        }
+    }
+    const int c = (int)it.c;
+    const uint32_t M = it.M;
+    const uint32_t mask = (1u << c) - 1u;
+    uint32_t carry = 0;
+    for (int w = 0; w < (int)it.W; ++w) {
+        const int off = w * c;
+        const int wd = off >> 5, sh = off & 31;
+        uint32_t raw = 0;
+        if (wd < 8) {
+            const uint64_t lo64 = s[wd];
+            const uint64_t hi64 = (wd + 1 < 8) ? s[wd + 1] : 0;
+            raw = (uint32_t)(((hi64 << 32) | lo64) >> sh) & mask;
+        }
+        uint32_t d = raw + carry;
+        uint32_t sign = 0;
+        if (d > M) {
+            d = (1u << c) - d;
+            sign = 1;
+            carry = 1;
+        } else {
+            carry = 0;
+        }
+        const unsigned long long slot = it.entry_base + (unsigned long long)w * it.n + j;
+        if (d == 0 || inf) {
+            keys[slot] = KEY_SENTINEL;
+        } else {
+            keys[slot] = it.bucket_base + (uint32_t)w * M + (d - 1);
+            vals[slot] = row | ((sign ^ neg) << 31);
+        }
+    }
+}
+
+template <class F>
+__device__ __forceinline__ void load_table_point(Affine<F>& a, const uint32_t* table, uint32_t idx) {
+    const uint4* src = reinterpret_cast<const uint4*>(table + (size_t)idx * 2 * F::N);
+    uint32_t w[2 * F::N];
+#pragma unroll
+    for (int k = 0; k < F::N / 2; ++k) {
+        const uint4 v = src[k];
+        w[4 * k] = v.x;
+        w[4 * k + 1] = v.y;
+        w[4 * k + 2] = v.z;
+        w[4 * k + 3] = v.w;
+    }
+    aff_load(a, w);
+}
+
+// Largest b in [0, B) with segoff[b] <= s (segoff non-decreasing, segoff[0] = 0).
+__device__ __forceinline__ uint32_t find_bucket(const uint32_t* segoff, uint32_t B, uint32_t s) {
+    uint32_t lo = 0, hi = B;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (segoff[mid] <= s)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Level 1, persistent: CTAs pull 32-segment work units from *queue until the
+// segment list is exhausted.  Each lane sums one segment with mixed XYZZ
+// additions: a bucket with nseg segments is split into near-equal runs.
+template <class C>
+__global__ void __launch_bounds__(128) k_accumulate(AccArgs a) {
+    using F = typename C::F;
+    __shared__ uint32_t unit;
+    const uint32_t total = a.segoff[a.B];
+    for (;;) {
+        if (threadIdx.x == 0) unit = atomicAdd(a.queue, 1u);
+        __syncthreads();
+        const uint32_t base = unit * blockDim.x;
+        __syncthreads();
+        if (base >= total) return;
+        const uint32_t s = base + threadIdx.x;
+        if (s < total) {
+            const uint32_t b = find_bucket(a.segoff, a.B, s);
+            const uint32_t q = s - a.segoff[b];
+            const uint32_t nseg = a.segoff[b + 1] - a.segoff[b];
+            const uint32_t off = a.offsets[b];
+            const uint32_t cnt = a.offsets[b + 1] - off;
+            const uint32_t start = off + (uint32_t)(((uint64_t)q * cnt) / nseg);
+            const uint32_t end = off + (uint32_t)(((uint64_t)(q + 1) * cnt) / nseg);
+            Xyzz<F> acc;
+            xyzz_set_inf(acc);
+            uint32_t v = start < end ? a.sorted[start] : 0u;
+            for (uint32_t e = start; e < end; ++e) {
+                const uint32_t vn = (e + 1 < end) ? a.sorted[e + 1] : 0u;
+                if (e + 1 < end) {
+                    const uint32_t* nxt = a.table + (size_t)(vn & 0x7fffffffu) * 2 * F::N;
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(nxt));
+                }
+                Affine<F> p;
+                load_table_point<F>(p, a.table, v & 0x7fffffffu);
+                if (v >> 31) fe_neg(p.y, p.y);
+                xyzz_add_affine(acc, p);
+                v = vn;
+            }
+            a.bid[s] = b;
+            if (nseg == 1)
+                xyzz_store(a.buckets + (size_t)b * 4 * F::N, acc);
+            else
+                xyzz_store(a.partial + (size_t)s * 4 * F::N, acc);
+        }
+    }
+}
+
+// Level l >= 2 for buckets with more than K2 segments: fold K2 partial sums
+// at a time; the last level writes the bucket.  Buckets with 2..K2
+// segments are left to the reduction, which sums their partials directly.
+template <class C>
+__global__ void __launch_bounds__(128) k_fold(FoldArgs a, int level, const uint32_t* __restrict__ in,
+                                              uint32_t* __restrict__ out) {
+    using F = typename C::F;
+    const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.seg_cap) return;
+    const uint32_t total = a.segoff[a.B];
+    if (s >= total) return;
+    const uint32_t b = a.bid[s];
+    const uint32_t base = a.segoff[b];
+    const uint32_t nseg = a.segoff[b + 1] - base;
+    if (nseg <= (uint32_t)a.K2) return;
+    const uint32_t q = (uint32_t)s - base;
+    uint32_t n_prev = nseg;
+    for (int l = 2; l < level; ++l) n_prev = (n_prev + a.K2 - 1) / a.K2;
+    if (n_prev <= 1) return;
+    const uint32_t n_cur = (n_prev + a.K2 - 1) / a.K2;
+    if (q >= n_cur) return;
+    const uint32_t lo = q * (uint32_t)a.K2, hi = min(lo + (uint32_t)a.K2, n_prev);
+    Xyzz<F> acc, t;
+    xyzz_load(acc, in + (size_t)(base + lo) * 4 * F::N);
+    for (uint32_t j = lo + 1; j < hi; ++j) {
+        xyzz_load(t, in + (size_t)(base + j) * 4 * F::N);
+        xyzz_add(acc, t);
+    }
+    if (n_cur == 1)
+        xyzz_store(a.buckets + (size_t)b * 4 * F::N, acc);
+    else
+        xyzz_store(out + (size_t)(base + q) * 4 * F::N, acc);
+}
+
+template <class F>
+__device__ __forceinline__ void xyzz_dbl_n(Xyzz<F>& p, int k) {
+    for (int i = 0; i < k; ++i) xyzz_dbl(p, p);
+}
+
+// Sum of global bucket g: its single accumulator, or its 2..K2 partials.
+template <class F>
+__device__ __forceinline__ void bucket_value(Xyzz<F>& r, const RedArgs& a, uint32_t g) {
+    const uint32_t s0 = a.segoff[g], nseg = a.segoff[g + 1] - s0;
+    if (nseg == 0) {
+        xyzz_set_inf(r);
+    } else if (nseg == 1 || nseg > (uint32_t)a.K2) {
+        xyzz_load(r, a.buckets + (size_t)g * 4 * F::N);
+    } else {
+        Xyzz<F> t;
+        xyzz_load(r, a.partial + (size_t)s0 * 4 * F::N);
+        for (uint32_t i = 1; i < nseg; ++i) {
+            xyzz_load(t, a.partial + (size_t)(s0 + i) * 4 * F::N);
+            xyzz_add(r, t);
+        }
+    }
+}
+
+// In-place suffix scan over sm[0..n) (n = blockDim.x) of XYZZ points:
+// afterwards sm[t] = sum_{t' >= t} old sm[t'].
+template <class F>
+__device__ __forceinline__ void smem_suffix_scan(uint32_t* sm) {
+    constexpr int PW = 4 * F::N;
+    const int t = threadIdx.x, n = blockDim.x;
+    for (int d = 1; d < n; d <<= 1) {
+        Xyzz<F> y, o;
+        xyzz_load(y, sm + (size_t)t * PW);
+        if (t + d < n) {
+            xyzz_load(o, sm + (size_t)(t + d) * PW);
+            xyzz_add(y, o);
+        }
+        __syncthreads();
+        xyzz_store(sm + (size_t)t * PW, y);
+        __syncthreads();
+    }
+}
+
+// In-place tree sum over sm[0..n): afterwards sm[0] = sum.
+template <class F>
+__device__ __forceinline__ void smem_tree_sum(uint32_t* sm) {
+    constexpr int PW = 4 * F::N;
+    const int t = threadIdx.x;
+    for (int d = blockDim.x >> 1; d >= 1; d >>= 1) {
+        if (t < d) {
+            Xyzz<F> y, o;
+            xyzz_load(y, sm + (size_t)t * PW);
+            xyzz_load(o, sm + (size_t)(t + d) * PW);
+            xyzz_add(y, o);
+            xyzz_store(sm + (size_t)t * PW, y);
+        }
+        __syncthreads();
+    }
+}
+
+// Reduction stage 1.  Block -> (window, b) via its BlkDesc.  Thread t owns
+// S = 2^log_S consecutive buckets of the block's range; with R_t = sum_j B
+// and T_t = sum_j j B (j relative), the block's
+//   Fb = sum_k k B_k = sum_t T_t + S * sum_{t>=1} Y_t,   Sb = Y_0,
+// where Y_t = sum_{t'>=t} R_t' (suffix scan in shared memory).
+template <class C>
+__global__ void __launch_bounds__(RED_THREADS) k_reduce_blocks(RedArgs a) {
+    using F = typename C::F;
+    constexpr int PW = 4 * F::N;
+    extern __shared__ __align__(16) uint32_t smr[];
+    uint32_t* sA = smr;                       // R_t -> suffix sums -> tree
+    uint32_t* sB = smr + RED_THREADS * PW;    // T_t -> tree
+    const BlkDesc bd = a.blks[blockIdx.x];
+    const WinDesc wd = a.wins[bd.win];
+    const uint32_t S = 1u << wd.log_S;
+    const uint32_t first = bd.b * (RED_THREADS << wd.log_S) + threadIdx.x * S;
+    {
+        Xyzz<F> R, T, Bk;
+        xyzz_set_inf(R);
+        xyzz_set_inf(T);
+        for (int j = (int)S - 1; j >= 0; --j) {
+            if (first + (uint32_t)j < wd.Mw) {
+                bucket_value(Bk, a, wd.bucket_base + first + (uint32_t)j);
+                xyzz_add(R, Bk);
+            }
+            if (j > 0) xyzz_add(T, R);
+        }
+        xyzz_store(sA + (size_t)threadIdx.x * PW, R);
+        xyzz_store(sB + (size_t)threadIdx.x * PW, T);
+    }
+    __syncthreads();
+    smem_suffix_scan<F>(sA);
+    Xyzz<F> Y0;
+    if (threadIdx.x == 0) {
+        xyzz_load(Y0, sA);
+        Xyzz<F> inf;
+        xyzz_set_inf(inf);
+        xyzz_store(sA, inf);  // the tree below sums Y_t for t >= 1
+    }
+    __syncthreads();
+    smem_tree_sum<F>(sA);
+    smem_tree_sum<F>(sB);
+    if (threadIdx.x == 0) {
+        Xyzz<F> Fb, t;
+        xyzz_load(Fb, sA);
+        xyzz_dbl_n(Fb, (int)wd.log_S);
+        xyzz_load(t, sB);
+        xyzz_add(Fb, t);
+        xyzz_store(a.blk_out + ((size_t)blockIdx.x * 2) * PW, Fb);
+        xyzz_store(a.blk_out + ((size_t)blockIdx.x * 2 + 1) * PW, Y0);
+    }
+}
+
+// Reduction stage 2, one block per window over its nb <= RED_THREADS
+// stage-1 results (Fb, Sb):  V = sum_b Fb + BLK * sum_{b>=1} Y_b + Y_0,
+// Y_b = sum_{b'>=b} Sb'.
+template <class C>
+__global__ void __launch_bounds__(RED_THREADS) k_reduce_windows(RedArgs a) {
+    using F = typename C::F;
+    constexpr int PW = 4 * F::N;
+    extern __shared__ __align__(16) uint32_t smr[];
+    uint32_t* sA = smr;
+    uint32_t* sB = smr + RED_THREADS * PW;
+    const WinDesc wd = a.wins[blockIdx.x];
+    const uint32_t t = threadIdx.x;
+    {
+        Xyzz<F> Fb, Sb;
+        xyzz_set_inf(Fb);
+        xyzz_set_inf(Sb);
+        if (t < wd.nb) {
+            xyzz_load(Fb, a.blk_out + ((size_t)(wd.blk_base + t) * 2) * PW);
+            xyzz_load(Sb, a.blk_out + ((size_t)(wd.blk_base + t) * 2 + 1) * PW);
+        }
+        xyzz_store(sA + (size_t)t * PW, Sb);
+        xyzz_store(sB + (size_t)t * PW, Fb);
+    }
+    __syncthreads();
+    smem_suffix_scan<F>(sA);
+    Xyzz<F> Y0;
+    if (t == 0) {
+        xyzz_load(Y0, sA);
+        Xyzz<F> inf;
+        xyzz_set_inf(inf);
+        xyzz_store(sA, inf);
+    }
+    __syncthreads();
+    smem_tree_sum<F>(sA);
+    smem_tree_sum<F>(sB);
+    if (t == 0) {
+        Xyzz<F> V, u;
+        xyzz_load(V, sA);
+        xyzz_dbl_n(V, (int)wd.log_blk);
+        xyzz_load(u, sB);
+        xyzz_add(V, u);
+        xyzz_add(V, Y0);
+        xyzz_store(a.win_out + (size_t)blockIdx.x * PW, V);
+    }
+}
+
+// Horner over each item's windows, then affine + wire (+ compressed for
+// BLS12-381).  One thread per item.
+template <class C>
+__global__ void k_combine(const ItemDesc* __restrict__ items, uint32_t n_items,
+                          const uint32_t* __restrict__ wins, uint8_t* __restrict__ out_wire,
+                          uint8_t* __restrict__ out_comp) {
+    using F = typename C::F;
+    constexpr int PW = 4 * F::N;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_items) return;
+    const ItemDesc it = items[i];
+    uint8_t* ow = out_wire + (size_t)i * C::WIRE;
+    uint8_t* oc = out_comp ? out_comp + (size_t)i * 48 : nullptr;
+    Xyzz<F> acc, t;
+    if (it.n == 0) {
+        xyzz_set_inf(acc);
+    } else {
+        xyzz_load(acc, wins + (size_t)(it.win_base + it.W - 1) * PW);
+        for (int w = (int)it.W - 2; w >= 0; --w) {
+            xyzz_dbl_n(acc, (int)it.c);
+            xyzz_load(t, wins + (size_t)(it.win_base + (uint32_t)w) * PW);
+            xyzz_add(acc, t);
+        }
+    }
+    Affine<F> af;
+    const bool fin = xyzz_to_affine(af, acc);
+    Fe<F> x, y;
+    if (fin) {
+        fe_from_mont(x, af.x);
+        fe_from_mont(y, af.y);
+        fe_to_be_bytes(ow, x);
+        fe_to_be_bytes(ow + F::BYTES, y);
+    } else {
+        for (int k = 0; k < C::WIRE; ++k) ow[k] = 0;
+    }
+    if (oc && C::CURVE_ID == 2) {
+        // ZCash/IETF compressed form: bit7 compressed, bit6 infinity,
+        // bit5 iff y > (p-1)/2, i.e. 2y > p.
+        if (!fin) {
+            oc[0] = 0xC0;
+            for (int k = 1; k < 48; ++k) oc[k] = 0;
+        } else {
+            uint32_t y2[F::N];
+            uint32_t cy = 0;
+            for (int k = 0; k < F::N; ++k) {
+                y2[k] = (y.v[k] << 1) | cy;
+                cy = y.v[k] >> 31;
+            }
+            // 2y > p  <=>  p - 2y borrows (2y != p since p is odd)
+            int64_t bw = 0;
+            for (int k = 0; k < F::N; ++k) {
+                const int64_t v = (int64_t)F::P(k) - (int64_t)y2[k] - bw;
+                bw = v < 0 ? 1 : 0;
+            }
+            for (int k = 0; k < 48; ++k) oc[k] = ow[k];
+            oc[0] |= 0x80;
+            if (bw) oc[0] |= 0x20;
+        }
+    }
+}
+
+template <class C>
+struct MsmLaunchImpl {
+    using F = typename C::F;
+    static void wire_to_table(const uint8_t* w, uint32_t* t, size_t n, cudaStream_t st) {
+        if (!n) return;
+        k_wire_to_table<C><<<ceil_div_u(n, 128), 128, 0, st>>>(w, t, n);
+        KB_LAUNCH_CHECK();
+    }
+    static void table_to_wire(const uint32_t* t, uint8_t* w, size_t n, cudaStream_t st) {
+        if (!n) return;
+        k_table_to_wire<C><<<ceil_div_u(n, 128), 128, 0, st>>>(t, w, n);
+        KB_LAUNCH_CHECK();
+    }
+    static void recode(const ItemDesc* items, uint32_t n_items, unsigned long long total,
+                       const uint32_t* scalars, const uint32_t* table, uint32_t* keys,
+                       uint32_t* vals, cudaStream_t st) {
+        if (!total) return;
+        k_recode<C><<<ceil_div_u(total, 256), 256, 0, st>>>(items, n_items, total, scalars, table,
+                                                           keys, vals);
+        KB_LAUNCH_CHECK();
+    }
+    static void accumulate(const AccArgs& a, unsigned grid, cudaStream_t st) {
+        k_accumulate<C><<<grid, 128, 0, st>>>(a);
+        KB_LAUNCH_CHECK();
+    }
+    static void fold(const FoldArgs& a, int level, const uint32_t* in, uint32_t* out,
+                     cudaStream_t st) {
+        k_fold<C><<<ceil_div_u(a.seg_cap, 128), 128, 0, st>>>(a, level, in, out);
+        KB_LAUNCH_CHECK();
+    }
+    static size_t red_smem() { return (size_t)2 * RED_THREADS * 4 * F::N * 4; }
+    static void reduce_blocks(const RedArgs& a, unsigned nblk, cudaStream_t st) {
+        if (!nblk) return;
+        set_smem_attr((const void*)k_reduce_blocks<C>, red_smem());
+        k_reduce_blocks<C><<<nblk, RED_THREADS, red_smem(), st>>>(a);
+        KB_LAUNCH_CHECK();
+    }
+    static void reduce_windows(const RedArgs& a, unsigned nwin, cudaStream_t st) {
+        if (!nwin) return;
+        set_smem_attr((const void*)k_reduce_windows<C>, red_smem());
+        k_reduce_windows<C><<<nwin, RED_THREADS, red_smem(), st>>>(a);
+        KB_LAUNCH_CHECK();
+    }
+    static void combine(const ItemDesc* items, uint32_t n_items, const uint32_t* wins,
+                        uint8_t* ow, uint8_t* oc, cudaStream_t st) {
+        if (!n_items) return;
+        k_combine<C><<<ceil_div_u(n_items, 32), 32, 0, st>>>(items, n_items, wins, ow, oc);
+        KB_LAUNCH_CHECK();
+    }
+    static int accumulate_occupancy() {
+        int blocks = 0;
+        KB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_accumulate<C>, 128, 0));
+        return blocks;
+    }
+    static MsmLaunchers table() {
+        MsmLaunchers L;
+        L.wire_to_table = &wire_to_table;
+        L.table_to_wire = &table_to_wire;
+        L.recode = &recode;
+        L.accumulate = &accumulate;
+        L.fold = &fold;
+        L.reduce_blocks = &reduce_blocks;
+        L.reduce_windows = &reduce_windows;
+        L.combine = &combine;
+        L.accumulate_occupancy = &accumulate_occupancy;
+        L.point_words = 4 * F::N;
+        L.table_words = 2 * F::N;
+        L.wire_bytes = C::WIRE;
+        return L;
+    }
+};
+
+}  // namespace kb200

@@ -4,7 +4,11 @@
 #include "ntt.cuh"
 #include "runtime.cuh"
 
+#include "msm_desc.cuh"
+
 #include <map>
+#include <mutex>
+#include <vector>
 
 namespace kb200 {
 
@@ -141,6 +145,7 @@ struct PassArgs {
     const uint32_t* post_lo;
     const uint32_t* post_const;  // inverse without coset: n^-1
     size_t batch_stride;         // elements between consecutive vectors
+    const unsigned long long* vec_off;  // if set: element offset of vector y
 };
 
 template <class F>
@@ -170,7 +175,8 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(PassArgs a) {
     uint32_t* sm = smem;                                  // cb * R elements
     uint32_t* stw = smem + ((size_t)8 << (a.log_cb + a.log_R));  // R/2 twiddles
     const int R = 1 << a.log_R, cb = 1 << a.log_cb;
-    const size_t vec = (size_t)blockIdx.y * a.batch_stride;
+    const size_t vec = a.vec_off ? (size_t)a.vec_off[blockIdx.y]
+                                 : (size_t)blockIdx.y * a.batch_stride;
     const uint32_t* in = a.in + vec * 8;
     uint32_t* out = a.out + vec * 8;
     const int tot = R * cb;
@@ -290,13 +296,34 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(PassArgs a) {
 
 struct NttEngine {
     int curve;
-    int log_nt = -1;
-    DevBuf tw, tw_hi, tw_lo, scratch, consts, pre_hi, pre_lo, post_hi, post_lo;
-    int post_log_n = -1;       // n whose n^-1 is folded into post_lo / ninv
+    int log_nt = -1;             // twiddle table covers sizes up to 2^log_nt
+    DevBuf tw, tw_hi, tw_lo, scratch, consts, ninv, pre_hi, pre_lo, post_hi;
+    std::map<int, DevBuf> post_lo;  // per log n: n^-1 * g^-e, e < 2^13
+    bool consts_ready = false;
     bool coset_ready = false;
+    ~NttEngine() {
+        for (DevBuf* b : {&tw, &tw_hi, &tw_lo, &scratch, &consts, &ninv, &pre_hi, &pre_lo, &post_hi})
+            b->release();
+        for (auto& kv : post_lo) kv.second.release();
+    }
 };
 
 int ntt_max_log(int curve) { return curve == 2 ? 28 : 28; }
+
+static std::mutex g_ntt_tune_mu;
+static int g_ntt_tune[3][32];
+
+void ntt_tune_set(int curve, int log_n, int log_r1) {
+    if (curve < 1 || curve > 2 || log_n < 0 || log_n >= 32) return;
+    std::lock_guard<std::mutex> lk(g_ntt_tune_mu);
+    g_ntt_tune[curve][log_n] = log_r1;
+}
+
+int ntt_tune_get(int curve, int log_n) {
+    if (curve < 1 || curve > 2 || log_n < 0 || log_n >= 32) return 0;
+    std::lock_guard<std::mutex> lk(g_ntt_tune_mu);
+    return g_ntt_tune[curve][log_n];
+}
 
 NttEngine* ntt_engine_create(int curve) {
     NttEngine* e = new NttEngine();
@@ -304,13 +331,7 @@ NttEngine* ntt_engine_create(int curve) {
     return e;
 }
 
-void ntt_engine_destroy(NttEngine* e) {
-    if (!e) return;
-    for (DevBuf* b : {&e->tw, &e->tw_hi, &e->tw_lo, &e->scratch, &e->consts, &e->pre_hi,
-                      &e->pre_lo, &e->post_hi, &e->post_lo})
-        b->release();
-    delete e;
-}
+void ntt_engine_destroy(NttEngine* e) { delete e; }
 
 namespace {
 
@@ -323,8 +344,13 @@ void exp_words(uint32_t out[8], int mode, int k) {
         r[0] -= 1;
         for (int s = 0; s < k; ++s)
             for (int i = 0; i < 8; ++i) r[i] = (r[i] >> 1) | (i + 1 < 8 ? (r[i + 1] << 31) : 0u);
-    } else {          // r - 2
-        r[0] -= 2;
+    } else {          // r - 2, borrow propagated (BLS12-381 r ends in ...0001)
+        uint32_t borrow = 2;
+        for (int i = 0; i < 8; ++i) {
+            const uint32_t v = r[i];
+            r[i] = v - borrow;
+            borrow = v < borrow ? 1u : 0u;
+        }
     }
     for (int i = 0; i < 8; ++i) out[i] = r[i];
 }
@@ -337,21 +363,55 @@ void ninv_words(uint32_t out[8], int k) {
     for (int i = 0; i < 8; ++i) r[i] = F::P(i);
     uint64_t bw = 0;
     for (int i = 0; i < 8; ++i) {
-        uint64_t v = (uint64_t)r[i] - q[i] - bw;
+        const uint64_t v = (uint64_t)r[i] - q[i] - bw;
         out[i] = (uint32_t)v;
         bw = (v >> 63) & 1;
     }
 }
 
-// consts layout (8-word slots): 0 = w_NT, 1 = scratch exponent, 2 = g, 3 = g^-1,
-// 4 = n^-1 (Montgomery), 5 = n^-1 (standard), 6 = exponent for g^-1
+// out[i] = to_mont(in[i]) for i < count (standard -> Montgomery form).
+template <class F>
+__global__ void k_to_mont(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    Fe<F> a;
+    ld_elt(a, in + (size_t)i * 8);
+    fe_to_mont(a, a);
+    st_elt(out + (size_t)i * 8, a);
+}
+
+// consts slots (8 words each): 0 = w_NT, 1 = exponent scratch, 2 = g,
+// 3 = g^-1, 4 = exponent scratch.  ninv[k] = Montgomery(2^-k), k <= 28.
+// All set-up work synchronises the stream; once a size (and coset use) has
+// been prepared, ntt_run queues kernels only, so it can be graph-captured.
 template <class F>
 void prepare_impl(NttEngine* e, int log_n, int coset, cudaStream_t st) {
     if (log_n > FrInfo<F>::ADICITY || log_n > ntt_max_log(e->curve))
         throw std::invalid_argument("ntt: size exceeds the field's 2-adicity");
-    e->consts.reserve(16 * 8 * 4, st);
-    uint32_t* C = e->consts.as<uint32_t>();
     const int TB = 256;
+    const int maxlog = ntt_max_log(e->curve);
+    if (!e->consts_ready) {
+        e->consts.reserve(8 * 8 * 4, st);
+        e->ninv.reserve((size_t)(maxlog + 1) * 32 * 2, st);
+        uint32_t* C = e->consts.as<uint32_t>();
+        std::vector<uint32_t> nv((size_t)(maxlog + 1) * 8);
+        for (int k = 0; k <= maxlog; ++k) ninv_words<F>(&nv[(size_t)k * 8], k);
+        uint32_t* stage = e->ninv.as<uint32_t>() + (size_t)(maxlog + 1) * 8;
+        KB_CUDA(cudaMemcpyAsync(stage, nv.data(), nv.size() * 4, cudaMemcpyHostToDevice, st));
+        k_to_mont<F><<<1, 32, 0, st>>>(stage, e->ninv.as<uint32_t>(), maxlog + 1);
+        KB_LAUNCH_CHECK();
+        uint32_t one[8] = {1, 0, 0, 0, 0, 0, 0, 0}, ex[8];
+        KB_CUDA(cudaMemcpyAsync(C + 8, one, 32, cudaMemcpyHostToDevice, st));
+        k_pow_gen<F><<<1, 32, 0, st>>>(C + 8, C + 16);
+        KB_LAUNCH_CHECK();
+        exp_words<F>(ex, 1, 0);
+        KB_CUDA(cudaMemcpyAsync(C + 32, ex, 32, cudaMemcpyHostToDevice, st));
+        k_pow_gen<F><<<1, 32, 0, st>>>(C + 32, C + 24);
+        KB_LAUNCH_CHECK();
+        KB_CUDA(cudaStreamSynchronize(st));
+        e->consts_ready = true;
+    }
+    uint32_t* C = e->consts.as<uint32_t>();
     const int need = log_n < 1 ? 1 : log_n;
     if (need > e->log_nt) {
         const int L = need;
@@ -378,90 +438,72 @@ void prepare_impl(NttEngine* e, int log_n, int coset, cudaStream_t st) {
         KB_CUDA(cudaStreamSynchronize(st));
     }
     if (coset && !e->coset_ready) {
-        // g and g^-1 in Montgomery form, then two-level power tables up to 2^28.
-        uint32_t one[8] = {1, 0, 0, 0, 0, 0, 0, 0}, ex[8];
-        KB_CUDA(cudaMemcpyAsync(C + 8, one, 32, cudaMemcpyHostToDevice, st));
-        k_pow_gen<F><<<1, 32, 0, st>>>(C + 8, C + 16);
-        KB_LAUNCH_CHECK();
-        exp_words<F>(ex, 1, 0);
-        KB_CUDA(cudaMemcpyAsync(C + 48, ex, 32, cudaMemcpyHostToDevice, st));
-        k_pow_gen<F><<<1, 32, 0, st>>>(C + 48, C + 24);
-        KB_LAUNCH_CHECK();
         const size_t nlo = (size_t)1 << TAB_SPLIT;
         const size_t nhi = (size_t)1 << (28 - TAB_SPLIT);
         e->pre_lo.reserve(nlo * 32, st);
         e->pre_hi.reserve(nhi * 32, st);
-        e->post_lo.reserve(nlo * 32, st);
         e->post_hi.reserve(nhi * 32, st);
         k_powers<F><<<ceil_div_u(nlo, TB), TB, 0, st>>>(C + 16, 1, nlo, e->pre_lo.as<uint32_t>());
+        KB_LAUNCH_CHECK();
         k_powers<F><<<ceil_div_u(nhi, TB), TB, 0, st>>>(C + 16, nlo, nhi, e->pre_hi.as<uint32_t>());
+        KB_LAUNCH_CHECK();
         k_powers<F><<<ceil_div_u(nhi, TB), TB, 0, st>>>(C + 24, nlo, nhi, e->post_hi.as<uint32_t>());
         KB_LAUNCH_CHECK();
         e->coset_ready = true;
-        e->post_log_n = -1;
+        KB_CUDA(cudaStreamSynchronize(st));
+    }
+    if (coset && !e->post_lo.count(log_n)) {
+        // post_lo[e] = n^-1 * g^-e
+        const size_t nlo = (size_t)1 << TAB_SPLIT;
+        DevBuf& b = e->post_lo[log_n];
+        b.reserve(nlo * 32, st);
+        k_powers<F><<<ceil_div_u(nlo, TB), TB, 0, st>>>(C + 24, 1, nlo, b.as<uint32_t>());
+        KB_LAUNCH_CHECK();
+        uint32_t* stage = e->ninv.as<uint32_t>() + (size_t)(maxlog + 1) * 8 + (size_t)log_n * 8;
+        k_scale_table<F><<<ceil_div_u(nlo, TB), TB, 0, st>>>(b.as<uint32_t>(), nlo, stage);
+        KB_LAUNCH_CHECK();
         KB_CUDA(cudaStreamSynchronize(st));
     }
 }
 
 template <class F>
-void set_inverse_scale(NttEngine* e, int log_n, int coset, cudaStream_t st) {
-    uint32_t* C = e->consts.as<uint32_t>();
-    const int TB = 256;
-    // n^-1 standard into slot 5, Montgomery into slot 4.
-    uint32_t ni[8];
-    ninv_words<F>(ni, log_n);
-    KB_CUDA(cudaMemcpyAsync(C + 40, ni, 32, cudaMemcpyHostToDevice, st));
-    if (coset && e->post_log_n != log_n) {
-        // post_lo[e] = n^-1 * g^-e
-        const size_t nlo = (size_t)1 << TAB_SPLIT;
-        k_powers<F><<<ceil_div_u(nlo, TB), TB, 0, st>>>(C + 24, 1, nlo, e->post_lo.as<uint32_t>());
-        KB_LAUNCH_CHECK();
-        k_scale_table<F><<<ceil_div_u(nlo, TB), TB, 0, st>>>(e->post_lo.as<uint32_t>(), nlo, C + 40);
-        KB_LAUNCH_CHECK();
-        e->post_log_n = log_n;
-    }
-    // Montgomery n^-1 for the non-coset inverse: slot 4 = to_mont(slot 5).
-    KB_CUDA(cudaMemcpyAsync(C + 32, C + 40, 32, cudaMemcpyDeviceToDevice, st));
-    uint32_t one_m_words[8];
-    for (int i = 0; i < 8; ++i) one_m_words[i] = F::R1(i);
-    KB_CUDA(cudaMemcpyAsync(C + 56, one_m_words, 32, cudaMemcpyHostToDevice, st));
-    // slot 7 holds R (Montgomery one); slot 4 = R * n^-1 -> scale by to_mont.
-    k_scale_table<F><<<1, 32, 0, st>>>(C + 56, 1, C + 40);
-    KB_LAUNCH_CHECK();
-    KB_CUDA(cudaMemcpyAsync(C + 32, C + 56, 32, cudaMemcpyDeviceToDevice, st));
-}
-
-template <class F>
 void run_impl(NttEngine* e, uint32_t* d, size_t n, int inverse, int coset, size_t batch,
-              cudaStream_t st) {
+              const unsigned long long* d_vec_off, uint32_t* d_scratch, cudaStream_t st) {
     if (n == 0 || batch == 0) return;
     if (n & (n - 1)) throw std::invalid_argument("ntt: n must be a power of two");
     int log_n = 0;
     while (((size_t)1 << log_n) < n) ++log_n;
     prepare_impl<F>(e, log_n, coset, st);
-    if (inverse) set_inverse_scale<F>(e, log_n, coset, st);
-    uint32_t* C = e->consts.as<uint32_t>();
 
-    // Radix split: P = 1 up to 2^12, 2 up to 2^20, else 3 (each <= 2^10).
+    // Radix split: P = 1 up to 2^12, 2 up to 2^20, else 3 (each <= 2^10);
+    // the first-pass radix may come from the autotuner.
     int logs[3], P;
+    const int tuned = ntt_tune_get(e->curve, log_n);
     if (log_n <= 12) {
         P = 1;
         logs[0] = log_n;
     } else if (log_n <= 20) {
         P = 2;
         logs[0] = (log_n + 1) / 2;
+        if (tuned >= log_n - 10 && tuned <= 10 && tuned >= 1) logs[0] = tuned;
         logs[1] = log_n - logs[0];
     } else {
         P = 3;
         logs[0] = (log_n + 2) / 3;
+        if (tuned >= log_n - 20 && tuned <= 10 && tuned >= 1) logs[0] = tuned;
         logs[1] = (log_n - logs[0] + 1) / 2;
         logs[2] = log_n - logs[0] - logs[1];
     }
-    e->scratch.reserve(n * batch * 32, st);
-    uint32_t* scr = e->scratch.as<uint32_t>();
+    uint32_t* scr = d_scratch;
+    if (P > 1 && !scr) {
+        if (d_vec_off) throw std::invalid_argument("ntt: listed vectors need caller scratch");
+        e->scratch.reserve(n * batch * 32, st);
+        scr = e->scratch.as<uint32_t>();
+    }
     // P == 1: in place on d (each CUDA block owns whole vectors).  P >= 2: the
     // first pass moves d -> scratch, middle passes run in place on scratch,
-    // and the last pass writes the natural-order result back into d.
+    // and the last pass writes the natural-order result back into d.  With a
+    // vector list the scratch mirrors d's layout (same offsets).
     int log_mprev = log_n;
     for (int p = 0; p < P; ++p) {
         PassArgs a{};
@@ -476,6 +518,7 @@ void run_impl(NttEngine* e, uint32_t* d, size_t n, int inverse, int coset, size_
         a.final = (p == P - 1);
         a.log_R1 = (P == 1) ? 0 : logs[0];
         a.batch_stride = n;
+        a.vec_off = d_vec_off;
         if (a.first && coset && !inverse) {
             a.pre_hi = e->pre_hi.as<uint32_t>();
             a.pre_lo = e->pre_lo.as<uint32_t>();
@@ -483,9 +526,9 @@ void run_impl(NttEngine* e, uint32_t* d, size_t n, int inverse, int coset, size_
         if (a.final && inverse) {
             if (coset) {
                 a.post_hi = e->post_hi.as<uint32_t>();
-                a.post_lo = e->post_lo.as<uint32_t>();
+                a.post_lo = e->post_lo[log_n].as<uint32_t>();
             } else {
-                a.post_const = C + 32;
+                a.post_const = e->ninv.as<uint32_t>() + (size_t)log_n * 8;
             }
         }
         int log_cb = 12 - a.log_R;
@@ -499,12 +542,10 @@ void run_impl(NttEngine* e, uint32_t* d, size_t n, int inverse, int coset, size_
         a.out = (P == 1 || a.final) ? d : scr;
         const size_t nblk = ((size_t)1 << (log_n - a.log_R)) >> log_cb;
         const size_t smem = (((size_t)8 << (log_cb + a.log_R)) + ((size_t)8 << a.log_R) / 2) * 4 + 64;
-        static bool attr_set = false;
-        if (!attr_set) {
-            KB_CUDA(cudaFuncSetAttribute(k_ntt_pass<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(((size_t)8 * NTT_SMEM_ELTS + 8 * 512) * 4 + 64)));
-            attr_set = true;
-        }
+        // Largest pass: 4096 data elements plus 2048 shared twiddles (a
+        // single-pass 2^12 transform) = 192 KiB + 64 B.
+        set_smem_attr((const void*)k_ntt_pass<F>,
+                      ((size_t)8 * NTT_SMEM_ELTS + 8 * 2048) * 4 + 64);
         dim3 grid((unsigned)nblk, (unsigned)batch);
         k_ntt_pass<F><<<grid, NTT_THREADS, smem, st>>>(a);
         KB_LAUNCH_CHECK();
@@ -526,9 +567,17 @@ void ntt_prepare(NttEngine* e, size_t n, int coset, cudaStream_t st) {
 void ntt_run(NttEngine* e, uint32_t* d, size_t n, int inverse, int coset, size_t batch,
              cudaStream_t st) {
     if (e->curve == 2)
-        run_impl<FrBLS>(e, d, n, inverse, coset, batch, st);
+        run_impl<FrBLS>(e, d, n, inverse, coset, batch, nullptr, nullptr, st);
     else
-        run_impl<FrBN>(e, d, n, inverse, coset, batch, st);
+        run_impl<FrBN>(e, d, n, inverse, coset, batch, nullptr, nullptr, st);
+}
+
+void ntt_run_list(NttEngine* e, uint32_t* d, size_t n, int inverse, int coset, size_t count,
+                  const unsigned long long* d_vec_off, uint32_t* d_scratch, cudaStream_t st) {
+    if (e->curve == 2)
+        run_impl<FrBLS>(e, d, n, inverse, coset, count, d_vec_off, d_scratch, st);
+    else
+        run_impl<FrBN>(e, d, n, inverse, coset, count, d_vec_off, d_scratch, st);
 }
 
 }  // namespace kb200

@@ -31,9 +31,21 @@ void ntt_engine_destroy(NttEngine* e);
 void ntt_run(NttEngine* e, uint32_t* d_data, size_t n, int inverse, int coset, size_t batch,
              cudaStream_t stream);
 
+// Transform `count` vectors of n elements whose element offsets (into d)
+// are listed on the device in d_vec_off; d_scratch mirrors d's layout
+// (needed when n > 2^12).  Queues kernels only once ntt_prepare(n, coset)
+// has run, so it can be captured in a CUDA graph.
+void ntt_run_list(NttEngine* e, uint32_t* d, size_t n, int inverse, int coset, size_t count,
+                  const unsigned long long* d_vec_off, uint32_t* d_scratch, cudaStream_t stream);
+
 // Build (or grow) the resident twiddle table so that sizes up to n need no
 // further set-up work.  Synchronises the stream when it builds.
 void ntt_prepare(NttEngine* e, size_t n, int coset, cudaStream_t stream);
+
+// Autotuner table: log2 of the first-pass radix for a size class (0 = the
+// default balanced split).
+void ntt_tune_set(int curve, int log_n, int log_r1);
+int ntt_tune_get(int curve, int log_n);
 
 // Largest supported log2 size for a curve (2-adicity, capped).
 int ntt_max_log(int curve);

@@ -1,0 +1,332 @@
+// Served KZG commits: a request loop over the resident SRS with continuous
+// batching.
+//
+// Requests (evaluations of one polynomial each) are queued by submitters.
+// One worker thread owns `slots` execution slots, each with its own CUDA
+// stream and CommitBatcher.  Whenever a slot is idle and requests are
+// waiting, the worker forms a batch from the head of the queue (up to
+// max_batch requests), admitting requests one by one while the batch's
+// computed device footprint (evaluations, NTT scratch, MSM buckets and
+// entries) fits the memory budget and the device's free memory, and queues
+// it on that slot.  Batches on different slots overlap on the device; a
+// request that arrives while others are running is admitted as soon as a
+// slot frees.  Completion is detected with events, results are copied to
+// pinned memory, and each request records submit-to-completion latency.
+// Every commit is exact, so a request's result is the same bytes alone or
+// in any mix.
+#include "../../include/kinet_b200/crypto_b200.h"
+#include "batch.cuh"
+#include "runtime.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+namespace kb200 {
+
+// Resident SRS of the calling thread's device (owned by the C-ABI context).
+void resident_srs(const uint32_t** table, size_t* n);
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t ticket = 0;
+    std::vector<uint8_t> evals;
+    size_t n = 0;
+    uint8_t commit[48] = {};
+    int status = 1;  // 1 pending, 0 done, < 0 error
+    Clock::time_point t_submit, t_done;
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    CommitBatcher* batcher = nullptr;
+    HostBuf h_in, h_out;
+    std::vector<Request*> reqs;
+    bool busy = false;
+};
+
+}  // namespace
+
+class KzgServer {
+   public:
+    int device = 0;
+    size_t max_batch = 64;
+    size_t mem_budget = 0;
+    const uint32_t* srs = nullptr;
+    size_t srs_n = 0;
+    std::vector<Slot> slots;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request*> queue;
+    std::map<uint64_t, Request*> by_ticket;
+    std::vector<double> latencies_ms;
+    uint64_t next_ticket = 1;
+    uint64_t completed = 0;
+    Clock::time_point first_submit, last_done;
+    bool have_first = false;
+    std::atomic<bool> stop{false};
+    std::string error;
+    std::thread worker;
+
+    void loop();
+    bool launch_batch(Slot& s);
+    void finish(Slot& s);
+};
+
+void KzgServer::finish(Slot& s) {
+    const auto now = Clock::now();
+    std::lock_guard<std::mutex> lk(mu);
+    for (size_t i = 0; i < s.reqs.size(); ++i) {
+        Request* r = s.reqs[i];
+        std::memcpy(r->commit, s.h_out.as<uint8_t>() + 48 * i, 48);
+        r->t_done = now;
+        r->status = 0;
+        latencies_ms.push_back(std::chrono::duration<double, std::milli>(now - r->t_submit).count());
+        ++completed;
+    }
+    last_done = now;
+    s.reqs.clear();
+    s.busy = false;
+    cv_done.notify_all();
+}
+
+bool KzgServer::launch_batch(Slot& s) {
+    std::vector<Request*> take;
+    std::vector<size_t> sizes;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            cudaGetLastError();
+            free_b = 0;
+        }
+        const size_t headroom = (size_t)256 << 20;
+        const size_t avail = free_b > headroom ? free_b - headroom : 0;
+        const size_t cap = mem_budget ? std::min(mem_budget, avail + 0) : avail;
+        while (!queue.empty() && take.size() < max_batch) {
+            Request* r = queue.front();
+            sizes.push_back(r->n);
+            const size_t need = commit_batch_scratch_bytes(sizes.data(), sizes.size());
+            // Admit at least one request when the device is otherwise idle, so
+            // a single oversized request is attempted rather than starved.
+            if (need > cap && !take.empty()) {
+                sizes.pop_back();
+                break;
+            }
+            take.push_back(r);
+            queue.pop_front();
+        }
+    }
+    if (take.empty()) return false;
+    size_t total = 0;
+    for (Request* r : take) total += r->n;
+    s.h_in.reserve(total * 32, s.stream);
+    s.h_out.reserve(take.size() * 48, s.stream);
+    size_t off = 0;
+    for (Request* r : take) {
+        std::memcpy(s.h_in.as<uint8_t>() + off * 32, r->evals.data(), r->n * 32);
+        off += r->n;
+    }
+    uint8_t* d_in = commit_batch_device_input(s.batcher, sizes.data(), sizes.size(), srs, srs_n,
+                                              s.stream);
+    KB_CUDA(cudaMemcpyAsync(d_in, s.h_in.ptr, total * 32, cudaMemcpyHostToDevice, s.stream));
+    commit_batch_device(s.batcher, sizes.data(), sizes.size(), srs, srs_n, s.stream,
+                        /*use_graph=*/false);
+    KB_CUDA(cudaMemcpyAsync(s.h_out.ptr, commit_batch_device_output(s.batcher), take.size() * 48,
+                            cudaMemcpyDeviceToHost, s.stream));
+    KB_CUDA(cudaEventRecord(s.done, s.stream));
+    s.reqs = std::move(take);
+    s.busy = true;
+    return true;
+}
+
+void KzgServer::loop() {
+    try {
+        KB_CUDA(cudaSetDevice(device));
+        while (!stop.load()) {
+            bool progressed = false;
+            for (Slot& s : slots) {
+                if (s.busy) {
+                    const cudaError_t q = cudaEventQuery(s.done);
+                    if (q == cudaSuccess) {
+                        finish(s);
+                        progressed = true;
+                    } else if (q != cudaErrorNotReady) {
+                        KB_CUDA(q);
+                    }
+                }
+            }
+            for (Slot& s : slots) {
+                if (!s.busy && launch_batch(s)) progressed = true;
+            }
+            if (!progressed) {
+                std::unique_lock<std::mutex> lk(mu);
+                bool any_busy = false;
+                for (Slot& s : slots) any_busy |= s.busy;
+                if (any_busy)
+                    cv_work.wait_for(lk, std::chrono::microseconds(50));
+                else
+                    cv_work.wait_for(lk, std::chrono::milliseconds(2),
+                                     [&] { return stop.load() || !queue.empty(); });
+            }
+        }
+    } catch (const std::exception& e) {
+        std::lock_guard<std::mutex> lk(mu);
+        error = e.what();
+        for (auto& kv : by_ticket)
+            if (kv.second->status == 1) kv.second->status = KB200_CRYPTO_ERR_BACKEND;
+        cv_done.notify_all();
+    }
+}
+
+}  // namespace kb200
+
+using namespace kb200;
+
+extern "C" {
+
+void* kzg_server_create(size_t max_batch, int slots, size_t mem_budget_bytes) {
+    try {
+        auto* s = new KzgServer();
+        KB_CUDA(cudaGetDevice(&s->device));
+        resident_srs(&s->srs, &s->srs_n);
+        if (!s->srs || !s->srs_n) {
+            set_last_error("kzg_server_create: no resident SRS (load or generate one first)");
+            delete s;
+            return nullptr;
+        }
+        s->max_batch = max_batch ? max_batch : 64;
+        s->mem_budget = mem_budget_bytes;
+        s->slots.resize(slots > 0 ? (size_t)slots : 2);
+        for (Slot& sl : s->slots) {
+            KB_CUDA(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+            KB_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+            sl.batcher = commit_batcher_create();
+        }
+        s->worker = std::thread([s] { s->loop(); });
+        return s;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return nullptr;
+    }
+}
+
+int kzg_server_submit(void* handle, const uint8_t* evals32le, size_t n, uint64_t* ticket) {
+    auto* s = static_cast<KzgServer*>(handle);
+    if (!s || !evals32le || !ticket) return KB200_CRYPTO_ERR_INPUT;
+    if (n == 0 || (n & (n - 1))) return KB200_CRYPTO_ERR_LENGTH;
+    if (n > s->srs_n) return KB200_CRYPTO_ERR_LENGTH;
+    auto* r = new Request();
+    r->evals.assign(evals32le, evals32le + n * 32);
+    r->n = n;
+    r->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (!s->error.empty()) {
+            delete r;
+            set_last_error(s->error);
+            return KB200_CRYPTO_ERR_BACKEND;
+        }
+        r->ticket = s->next_ticket++;
+        if (!s->have_first) {
+            s->first_submit = r->t_submit;
+            s->have_first = true;
+        }
+        s->by_ticket[r->ticket] = r;
+        s->queue.push_back(r);
+        *ticket = r->ticket;
+    }
+    s->cv_work.notify_one();
+    return KB200_CRYPTO_OK;
+}
+
+// Blocks until the request completes (timeout_ms < 0: no limit).  Returns 0
+// with the commitment, 1 on timeout, or a negative error.  The ticket is
+// released on completion.
+int kzg_server_wait(void* handle, uint64_t ticket, uint8_t commit48[48], double* latency_ms,
+                    double timeout_ms) {
+    auto* s = static_cast<KzgServer*>(handle);
+    if (!s || !commit48) return KB200_CRYPTO_ERR_INPUT;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->by_ticket.find(ticket);
+    if (it == s->by_ticket.end()) return KB200_CRYPTO_ERR_INPUT;
+    Request* r = it->second;
+    auto pred = [&] { return r->status != 1; };
+    if (timeout_ms < 0)
+        s->cv_done.wait(lk, pred);
+    else if (!s->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), pred))
+        return 1;
+    const int st = r->status;
+    if (st == 0) {
+        std::memcpy(commit48, r->commit, 48);
+        if (latency_ms)
+            *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    } else {
+        set_last_error(s->error);
+    }
+    s->by_ticket.erase(it);
+    delete r;
+    return st;
+}
+
+// Latency percentiles over completed requests since creation or the last
+// reset, sustained commits/s from the first submit to the last completion.
+int kzg_server_stats(void* handle, double* p50_ms, double* p99_ms, double* commits_per_s,
+                     uint64_t* completed, int reset) {
+    auto* s = static_cast<KzgServer*>(handle);
+    if (!s) return KB200_CRYPTO_ERR_INPUT;
+    std::lock_guard<std::mutex> lk(s->mu);
+    std::vector<double> v = s->latencies_ms;
+    std::sort(v.begin(), v.end());
+    auto pct = [&](double q) {
+        if (v.empty()) return 0.0;
+        size_t k = (size_t)(q * (double)(v.size() - 1) + 0.5);
+        return v[std::min(k, v.size() - 1)];
+    };
+    if (p50_ms) *p50_ms = pct(0.50);
+    if (p99_ms) *p99_ms = pct(0.99);
+    if (completed) *completed = s->completed;
+    if (commits_per_s) {
+        const double secs =
+            s->have_first ? std::chrono::duration<double>(s->last_done - s->first_submit).count() : 0;
+        *commits_per_s = secs > 0 ? (double)s->completed / secs : 0.0;
+    }
+    if (reset) {
+        s->latencies_ms.clear();
+        s->completed = 0;
+        s->have_first = false;
+    }
+    return KB200_CRYPTO_OK;
+}
+
+int kzg_server_destroy(void* handle) {
+    auto* s = static_cast<KzgServer*>(handle);
+    if (!s) return KB200_CRYPTO_ERR_INPUT;
+    s->stop.store(true);
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    for (Slot& sl : s->slots) {
+        if (sl.stream) cudaStreamSynchronize(sl.stream);
+        commit_batcher_destroy(sl.batcher);
+        sl.h_in.release();
+        sl.h_out.release();
+        if (sl.done) cudaEventDestroy(sl.done);
+        if (sl.stream) cudaStreamDestroy(sl.stream);
+    }
+    for (auto& kv : s->by_ticket) delete kv.second;
+    delete s;
+    return KB200_CRYPTO_OK;
+}
+
+}  // extern "C"

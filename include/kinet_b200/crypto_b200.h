@@ -109,6 +109,25 @@ int kzg_commit_fr(const uint8_t* evals32le, size_t n, uint8_t commit48[48]);
 int kzg_commit_batch(const uint8_t* evals32le, const size_t* sizes, size_t count,
                      uint8_t* commits48);
 
+/* ---- Served commits (continuous batching, new) -------------------------- */
+/* A request server over the resident SRS (which must stay loaded while the
+ * server lives).  Requests are admitted into batches as execution slots and
+ * device memory free up; batches on different slots overlap on the device.
+ * max_batch: requests per batch (0 = 64); slots: concurrent batches
+ * (0 = 2); mem_budget_bytes: cap on a batch's computed device footprint
+ * (0 = free device memory).  Returns NULL on failure (kb200_last_error). */
+void* kzg_server_create(size_t max_batch, int slots, size_t mem_budget_bytes);
+/* Queue one polynomial (n evaluations, 32 B LE); *ticket identifies it. */
+int kzg_server_submit(void* server, const uint8_t* evals32le, size_t n, uint64_t* ticket);
+/* Wait for a ticket (timeout_ms < 0: no limit).  0 = done (commit48 and
+ * latency filled, ticket released), 1 = timed out, < 0 = error. */
+int kzg_server_wait(void* server, uint64_t ticket, uint8_t commit48[48], double* latency_ms,
+                    double timeout_ms);
+/* p50 / p99 submit-to-completion latency and sustained commits/s. */
+int kzg_server_stats(void* server, double* p50_ms, double* p99_ms, double* commits_per_s,
+                     uint64_t* completed, int reset);
+int kzg_server_destroy(void* server);
+
 /* ---- Device-pointer entry points (inputs already resident in HBM) ------ */
 /* Pointers are device pointers (16-byte aligned), `stream` is a
  * cudaStream_t (NULL = legacy default stream); work is queued, not
@@ -132,6 +151,17 @@ int kb200_kzg_commit_device(void* d_evals, size_t n, void* d_commit48, void* str
  * (25% zero, 25% one, 20% uniform below 2^64, 30% uniform in [0, r)). */
 int kb200_gen_scalars(int curve, uint64_t seed, size_t n, int kind, uint8_t* out32le);
 
+/* ---- Autotuner (new) --------------------------------------------------- */
+/* Time MSM window widths and NTT radix splits for log2 sizes in
+ * [log_lo, log_hi] on this GPU, keep the fastest, append them to cache_path
+ * (keyed by GPU name and driver version).  Returns classes tuned or < 0. */
+int kb200_autotune(uint32_t curve, int log_lo, int log_hi, const char* cache_path);
+/* Apply the cached entries that match this GPU; returns entries applied. */
+int kb200_autotune_load(const char* cache_path);
+/* kind 0 = MSM window bits, 1 = NTT first-pass log radix (0 = untuned). */
+int kb200_tune_get(int kind, uint32_t curve, int log_n);
+void kb200_tune_set(int kind, uint32_t curve, int log_n, int value);
+
 /* ---- Introspection ------------------------------------------------------ */
 const char* kb200_last_error(void);
 /* 1 if a CUDA device is usable, else 0. */
@@ -143,7 +173,8 @@ unsigned long long kb200_launch_count(void);
 /* Per-stage CUDA-event timing of MSMs (off by default). */
 void kb200_profile_enable(int on);
 /* Stage times (ms) of the last MSM on this device for the curve, in order:
- * wire->table, recode, sort, accumulate, fold, reduce+combine.  Returns the
+ * wire->table, recode, sort, accumulate, fold, reduce_blocks, reduce_windows,
+ * combine.  Returns the
  * number written (0 if none recorded), or -1. */
 int kb200_msm_stage_ms(uint32_t curve, float* out, int max);
 
