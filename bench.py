@@ -175,6 +175,91 @@ def make_inputs(n: int, seed: int):
     return d_sc, d_pts
 
 
+def _tau(seed: int) -> bytes:
+    import crypto_b200 as kb
+    return kb.gen_scalars(CURVE, seed, 1)
+
+
+def bench_batched_commits(args) -> dict:
+    """512 BLS12-381 commits, sizes log-uniform over 2^8..2^16 (powers of
+    two), uniform Fr evaluations, one resident 2^16 SRS: the batched pass
+    (grouped iNTTs + one batched MSM, CUDA graph) against 512 sequential
+    plain kzg_commit_fr calls on the same GPU, byte-equal."""
+    import random
+    import crypto_b200 as kb
+    rng = random.Random(4096)
+    sizes = [1 << rng.randint(8, 16) for _ in range(args.commits)]
+    kb.kzg_srs_generate(_tau(7), 1 << 16)
+    evs = [kb.gen_scalars(CURVE, 100000 + i, n) for i, n in enumerate(sizes)]
+    blob = b"".join(evs)
+    # per-call: every commit through the plain C ABI, host buffers
+    kb.kzg_commit(evs[0])
+    t0 = time.perf_counter()
+    single = [kb.kzg_commit(e) for e in evs]
+    t_single = time.perf_counter() - t0
+    # batched: one call per 512-commit batch (graph captured on the first)
+    batch = kb.kzg_commit_batch(blob, sizes)
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        batch = kb.kzg_commit_batch(blob, sizes)
+    t_batch = (time.perf_counter() - t0) / reps
+    return {"commits": len(sizes), "sizes": "2^8..2^16 log-uniform", "srs": "2^16 resident",
+            "per_call_commits_per_s": len(sizes) / t_single,
+            "batched_commits_per_s": len(sizes) / t_batch,
+            "batched_over_per_call": t_single / t_batch,
+            "byte_equal": batch == single, "h2d_bytes": len(blob), "d2h_bytes": 48 * len(sizes)}
+
+
+def bench_served_commits(args) -> dict:
+    """Poisson arrivals of commit requests (70% 4096, 25% 2^16, 5% 2^20
+    evaluations) against a resident 2^20 SRS through the continuous-batching
+    server; p50/p99 submit-to-result latency and sustained commits/s per
+    arrival rate, results byte-checked against the plain path."""
+    import random
+    import threading
+    import crypto_b200 as kb
+    kb.kzg_srs_generate(_tau(8), 1 << 20)
+    pool = {}
+    for n in (4096, 1 << 16, 1 << 20):
+        pool[n] = [kb.gen_scalars(CURVE, 200000 + n + j, n) for j in range(3)]
+    want = {(n, j): kb.kzg_commit(e) for n, es in pool.items() for j, e in enumerate(es)}
+    out = []
+    for rate in args.serve_rates:
+        rng = random.Random(int(rate))
+        reqs = []
+        for _ in range(args.serve_requests):
+            u = rng.random()
+            n = 4096 if u < 0.70 else ((1 << 16) if u < 0.95 else (1 << 20))
+            reqs.append((n, rng.randrange(3), rng.expovariate(rate)))
+        ok = True
+        with kb.KzgServer(max_batch=64, slots=2) as srv:
+            tickets = []
+
+            def producer():
+                t_next = time.perf_counter()
+                for n, j, gap in reqs:
+                    t_next += gap
+                    d = t_next - time.perf_counter()
+                    if d > 0:
+                        time.sleep(d)
+                    tickets.append(((n, j), srv.submit(pool[n][j])))
+
+            th = threading.Thread(target=producer)
+            t0 = time.perf_counter()
+            th.start()
+            th.join()
+            for key, t in tickets:
+                c, _ms = srv.wait(t, timeout_ms=120000)
+                ok &= (c == want[key])
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+        out.append({"rate_per_s": rate, "requests": len(reqs), "p50_ms": st["p50_ms"],
+                    "p99_ms": st["p99_ms"], "commits_per_s": st["commits_per_s"],
+                    "wall_s": wall, "byte_equal": ok})
+    return {"mix": "70% 4096 / 25% 2^16 / 5% 2^20", "srs": "2^20 resident", "rates": out}
+
+
 def run_reference(args, ws, rank):
     n_sample = 1 << args.ref_logn
     threads = os.cpu_count() or 1
@@ -288,6 +373,11 @@ def run_ours(args, ws, rank, local):
     msm_roof = {"achieved": msm_w / (ms / 1e3) / 1e12, "peak": peak_imad / 1e12, "unit": "TIMAD/s",
                 "frac": msm_w / (ms / 1e3) / peak_imad, "work": f"W_msm(2^{args.logn}) = {msm_w:.3e} IMAD"}
 
+    kzg_batched = kzg_served = None
+    if rank == 0 and not args.no_kzg:
+        kzg_batched = bench_batched_commits(args)
+        kzg_served = bench_served_commits(args)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         import _oracle as O  # noqa: F401  (tests/ on sys.path inside cpu_reference_msm)
@@ -317,6 +407,8 @@ def run_ours(args, ws, rank, local):
             "stage_ms": stage,
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "kzg_batched": kzg_batched,
+            "kzg_served": kzg_served,
         }
         print(json.dumps(line), flush=True)
 
@@ -330,6 +422,10 @@ def main():
     ap.add_argument("--logn", type=int, default=LOGN)
     ap.add_argument("--ref-logn", type=int, default=17)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-kzg", action="store_true")
+    ap.add_argument("--commits", type=int, default=512)
+    ap.add_argument("--serve-rates", type=float, nargs="*", default=[100.0, 400.0])
+    ap.add_argument("--serve-requests", type=int, default=80)
     args = ap.parse_args()
     sys.path.insert(0, str(ROOT / "tests"))
     ws, rank, local = setup_dist()

@@ -112,18 +112,19 @@ KB_DEV void xyzz_mdbl(Xyzz<F>& r, const Affine<F>& a) {
     r.ZZZ = W;
 }
 
-// madd-2008-s: p += a, with a a finite affine point.
+// madd-2008-s: p += a, with a a finite affine point.  Temporaries are
+// reused so that at most five field elements are live besides p and a.
 template <class F>
 KB_DEV void xyzz_add_affine(Xyzz<F>& p, const Affine<F>& a) {
     if (xyzz_is_inf(p)) {
         xyzz_from_affine(p, a);
         return;
     }
-    Fe<F> U2, S2, P, R;
-    fe_mul(U2, a.x, p.ZZ);
-    fe_mul(S2, a.y, p.ZZZ);
-    fe_sub(P, U2, p.X);
-    fe_sub(R, S2, p.Y);
+    Fe<F> P, R, t;
+    fe_mul(P, a.x, p.ZZ);
+    fe_sub(P, P, p.X);          // P = x2*ZZ1 - X1
+    fe_mul(R, a.y, p.ZZZ);
+    fe_sub(R, R, p.Y);          // R = y2*ZZZ1 - Y1
     if (fe_is_zero(P)) {
         if (fe_is_zero(R))
             xyzz_mdbl(p, a);
@@ -131,24 +132,20 @@ KB_DEV void xyzz_add_affine(Xyzz<F>& p, const Affine<F>& a) {
             xyzz_set_inf(p);
         return;
     }
-    Fe<F> PP, PPP, Q, t;
-    fe_sqr(PP, P);
-    fe_mul(PPP, P, PP);
-    fe_mul(Q, p.X, PP);
-    Fe<F> X3;
-    fe_sqr(X3, R);
-    fe_sub(X3, X3, PPP);
-    fe_sub(X3, X3, Q);
-    fe_sub(X3, X3, Q);
-    fe_sub(t, Q, X3);
-    fe_mul(t, R, t);
-    Fe<F> Y3;
-    fe_mul(Y3, p.Y, PPP);
-    fe_sub(Y3, t, Y3);
-    fe_mul(p.ZZ, p.ZZ, PP);
-    fe_mul(p.ZZZ, p.ZZZ, PPP);
-    p.X = X3;
-    p.Y = Y3;
+    Fe<F> PP, Q;
+    fe_sqr(PP, P);              // PP
+    fe_mul(Q, p.X, PP);         // Q = X1*PP
+    fe_mul(p.ZZ, p.ZZ, PP);     // ZZ3 = ZZ1*PP
+    fe_mul(PP, P, PP);          // PP <- PPP = P*PP
+    fe_mul(p.ZZZ, p.ZZZ, PP);   // ZZZ3 = ZZZ1*PPP
+    fe_mul(t, p.Y, PP);         // Y1*PPP
+    fe_sqr(p.X, R);
+    fe_sub(p.X, p.X, PP);
+    fe_sub(p.X, p.X, Q);
+    fe_sub(p.X, p.X, Q);        // X3 = R^2 - PPP - 2Q
+    fe_sub(Q, Q, p.X);
+    fe_mul(Q, R, Q);
+    fe_sub(p.Y, Q, t);          // Y3 = R(Q - X3) - Y1*PPP
 }
 
 // add-2008-s: p += q, both XYZZ (either may be infinity).
@@ -159,13 +156,13 @@ KB_DEV void xyzz_add(Xyzz<F>& p, const Xyzz<F>& q) {
         p = q;
         return;
     }
-    Fe<F> U1, U2, S1, S2, P, R;
+    Fe<F> U1, S1, P, R;
     fe_mul(U1, p.X, q.ZZ);
-    fe_mul(U2, q.X, p.ZZ);
+    fe_mul(P, q.X, p.ZZ);
+    fe_sub(P, P, U1);           // P = U2 - U1
     fe_mul(S1, p.Y, q.ZZZ);
-    fe_mul(S2, q.Y, p.ZZZ);
-    fe_sub(P, U2, U1);
-    fe_sub(R, S2, S1);
+    fe_mul(R, q.Y, p.ZZZ);
+    fe_sub(R, R, S1);           // R = S2 - S1
     if (fe_is_zero(P)) {
         if (fe_is_zero(R))
             xyzz_dbl(p, p);
@@ -173,26 +170,22 @@ KB_DEV void xyzz_add(Xyzz<F>& p, const Xyzz<F>& q) {
             xyzz_set_inf(p);
         return;
     }
-    Fe<F> PP, PPP, Q, t;
+    Fe<F> PP;
     fe_sqr(PP, P);
-    fe_mul(PPP, P, PP);
-    fe_mul(Q, U1, PP);
-    Fe<F> X3;
-    fe_sqr(X3, R);
-    fe_sub(X3, X3, PPP);
-    fe_sub(X3, X3, Q);
-    fe_sub(X3, X3, Q);
-    fe_sub(t, Q, X3);
-    fe_mul(t, R, t);
-    Fe<F> Y3;
-    fe_mul(Y3, S1, PPP);
-    fe_sub(Y3, t, Y3);
     fe_mul(p.ZZ, p.ZZ, q.ZZ);
-    fe_mul(p.ZZ, p.ZZ, PP);
+    fe_mul(p.ZZ, p.ZZ, PP);     // ZZ3 = ZZ1*ZZ2*PP
+    fe_mul(U1, U1, PP);         // U1 <- Q = U1*PP
+    fe_mul(PP, P, PP);          // PP <- PPP = P*PP
     fe_mul(p.ZZZ, p.ZZZ, q.ZZZ);
-    fe_mul(p.ZZZ, p.ZZZ, PPP);
-    p.X = X3;
-    p.Y = Y3;
+    fe_mul(p.ZZZ, p.ZZZ, PP);   // ZZZ3 = ZZZ1*ZZZ2*PPP
+    fe_mul(S1, S1, PP);         // S1*PPP
+    fe_sqr(p.X, R);
+    fe_sub(p.X, p.X, PP);
+    fe_sub(p.X, p.X, U1);
+    fe_sub(p.X, p.X, U1);       // X3 = R^2 - PPP - 2Q
+    fe_sub(U1, U1, p.X);
+    fe_mul(U1, R, U1);
+    fe_sub(p.Y, U1, S1);        // Y3 = R(Q - X3) - S1*PPP
 }
 
 template <class F>

@@ -64,6 +64,21 @@ __global__ void k_scatter(const uint32_t* __restrict__ keys, const uint32_t* __r
     sorted[base + rank] = vals[t];
 }
 
+// Lists buckets spanning more than K2 + 1 chunks (list = {count, ids});
+// only they go through the fold levels.
+__global__ void k_list_big(const uint32_t* __restrict__ offsets, uint32_t B, uint32_t K, int K2,
+                           uint32_t cap, uint32_t* __restrict__ list) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= B) return;
+    const uint32_t o = offsets[g], c = offsets[g + 1] - o;
+    if (c == 0) return;
+    const uint32_t t0 = o / K, t1 = (o + c - 1) / K;
+    if (t1 - t0 > (uint32_t)K2) {
+        const uint32_t slot = atomicAdd(list, 1u);
+        if (slot < cap) list[1 + slot] = g;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Plans
 // ---------------------------------------------------------------------------
@@ -152,8 +167,8 @@ class MsmBatchPlan {
     std::vector<BlkDesc> blks;
     unsigned long long total_scalars = 0, L = 0;
     uint32_t B = 0;
-    int K = 32, K2 = 8, levels = 0;
-    size_t seg_cap = 0;
+    int K = 64, K2 = 8, FK = 4, levels = 0;
+    size_t nchunks = 0, big_cap = 0;
     DevBuf d_items, d_wins, d_blks;
     ~MsmBatchPlan() {
         d_items.release();
@@ -224,28 +239,29 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
             P.wins.push_back(wd);
         }
     }
+    // Chunk length: long chunks amortise the per-chunk records, but there must
+    // be enough chunks to keep every SM busy (~4 warps x 148 SMs x 32 lanes).
     int K = opt.force_K;
     if (K <= 0) {
-        if (L >= (1u << 24))
-            K = 32;
-        else if (L >= (1u << 22))
-            K = 16;
-        else if (L >= (1u << 20))
-            K = 8;
-        else
-            K = 4;
+        K = 64;
+        while (K > 4 && (unsigned long long)K * 148 * 4 * 32 * 2 > L) K >>= 1;
     }
     P.K = K;
     P.K2 = 8;
-    const size_t max_seg = (max_n + K - 1) / K;
+    P.nchunks = (size_t)((L + (unsigned long long)K - 1) / (unsigned long long)K);
+    // A bucket holds at most max_n entries, so spans at most max_n / K + 1
+    // chunks; its chunk records fold in ceil(log_FK(span)) levels.  A big
+    // bucket spans more than K2 + 1 chunks, so at most nchunks / (K2 + 1)
+    // buckets can be big.
+    const size_t max_span = (max_n + K - 1) / K + 1;
     int lv = 0;
     size_t span = 1;
-    while (span < max_seg) {
-        span *= (size_t)P.K2;
+    while (span < max_span) {
+        span *= (size_t)P.FK;
         ++lv;
     }
-    P.levels = lv;
-    P.seg_cap = (size_t)(L / (unsigned long long)K) + (size_t)B + 1;
+    P.levels = max_span > (size_t)P.K2 + 1 ? lv : 0;
+    P.big_cap = P.nchunks / (size_t)(P.K2 + 1) + 1;
 }
 
 MsmBatchPlan* msm_batch_plan_create(int curve, const MsmItem* items, size_t count,
@@ -285,8 +301,8 @@ constexpr int N_STAGE_EVENTS = 9;
 class MsmEngine {
    public:
     int curve = 0;
-    DevBuf table, keys, vals, counts, offsets, cursor, sorted, segoff, bid, part0, part1, buckets,
-        blk_out, win_out, scan_tmp, queue;
+    DevBuf table, keys, vals, counts, offsets, cursor, sorted, rec_first, rec_last, fold_buf,
+        buckets, blk_out, win_out, scan_tmp, queue;
     std::map<std::tuple<size_t, bool, int, int>, MsmBatchPlan*> single_plans;
     cudaEvent_t ev[N_STAGE_EVENTS] = {};
     bool ev_ready = false, ev_recorded = false;
@@ -303,8 +319,8 @@ class MsmEngine {
         for (auto& kv : single_plans) delete kv.second;
         if (ev_ready)
             for (auto& e : ev) cudaEventDestroy(e);
-        for (DevBuf* b : {&table, &keys, &vals, &counts, &offsets, &cursor, &sorted, &segoff, &bid,
-                          &part0, &part1, &buckets, &blk_out, &win_out, &scan_tmp, &queue})
+        for (DevBuf* b : {&table, &keys, &vals, &counts, &offsets, &cursor, &sorted, &rec_first,
+                          &rec_last, &fold_buf, &buckets, &blk_out, &win_out, &scan_tmp, &queue})
             b->release();
     }
 };
@@ -322,9 +338,9 @@ void msm_engine_destroy(MsmEngine* e) { delete e; }
 static size_t plan_scratch_bytes(const MsmBatchPlan& P) {
     const size_t PW = (size_t)(P.curve == 2 ? 48 : 32);
     size_t bytes = 3 * (size_t)P.L * 4;                      // keys, vals, sorted
-    bytes += 4 * ((size_t)P.B + 1) * 4;                      // counts, offsets, cursor, segoff
-    bytes += P.seg_cap * 4;                                  // bid
-    bytes += (P.levels >= 2 ? 2 : 1) * P.seg_cap * PW * 4;   // partial sums
+    bytes += 3 * ((size_t)P.B + 1) * 4;                      // counts, offsets, cursor
+    bytes += (P.levels >= 1 ? 3 : 2) * P.nchunks * PW * 4;   // chunk records (+ fold buffer)
+    bytes += P.big_cap * 4;
     bytes += (size_t)P.B * PW * 4;                           // bucket accumulators
     bytes += P.blks.size() * 2 * PW * 4 + P.wins.size() * PW * 4;
     return bytes + (1u << 20);
@@ -352,15 +368,15 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
     e->counts.reserve(((size_t)P.B + 1) * 4, st);
     e->offsets.reserve(((size_t)P.B + 1) * 4, st);
     e->cursor.reserve(((size_t)P.B + 1) * 4, st);
-    e->segoff.reserve(((size_t)P.B + 1) * 4, st);
-    e->bid.reserve(P.seg_cap * 4, st);
-    e->part0.reserve(P.seg_cap * PW * 4, st);
-    if (P.levels >= 2) e->part1.reserve(P.seg_cap * PW * 4, st);
+    const size_t nch = std::max<size_t>(1, P.nchunks);
+    e->rec_first.reserve(nch * PW * 4, st);
+    e->rec_last.reserve(nch * PW * 4, st);
+    if (P.levels >= 1) e->fold_buf.reserve(nch * PW * 4, st);
     e->buckets.reserve(std::max<size_t>(1, (size_t)P.B) * PW * 4, st);
     e->blk_out.reserve(std::max<size_t>(1, P.blks.size()) * 2 * PW * 4, st);
     e->win_out.reserve(std::max<size_t>(1, P.wins.size()) * PW * 4, st);
     e->scan_tmp.reserve(scan_tmp_words((size_t)P.B + 1) * 4, st);
-    e->queue.reserve(256, st);
+    e->queue.reserve((P.big_cap + 8) * 4, st);
 }
 
 void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_scalars,
@@ -391,55 +407,66 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
                                                        e->sorted.as<uint32_t>());
         KB_LAUNCH_CHECK();
     }
-    exclusive_scan_u32(e->counts.as<uint32_t>(), e->segoff.as<uint32_t>(), P.B, (uint32_t)P.K,
-                       e->scan_tmp.as<uint32_t>(), st);
+    KB_CUDA(cudaMemsetAsync(e->queue.ptr, 0, 8, st));  // work counter, big-bucket count
+    uint32_t* big_list = e->queue.as<uint32_t>() + 1;
+    if (P.B > 0 && P.levels >= 1) {
+        k_list_big<<<ceil_div_u(P.B, 256), 256, 0, st>>>(e->offsets.as<uint32_t>(), P.B,
+                                                        (uint32_t)P.K, P.K2, (uint32_t)P.big_cap,
+                                                        big_list);
+        KB_LAUNCH_CHECK();
+    }
     e->mark(3, st);
 
     AccArgs acc;
     acc.sorted = e->sorted.as<uint32_t>();
     acc.offsets = e->offsets.as<uint32_t>();
-    acc.segoff = e->segoff.as<uint32_t>();
     acc.B = P.B;
+    acc.K = (uint32_t)P.K;
     acc.table = d_table;
-    acc.partial = e->part0.as<uint32_t>();
-    acc.bid = e->bid.as<uint32_t>();
+    acc.rec_first = e->rec_first.as<uint32_t>();
+    acc.rec_last = e->rec_last.as<uint32_t>();
     acc.buckets = e->buckets.as<uint32_t>();
     acc.queue = e->queue.as<uint32_t>();
-    if (P.L > 0) {
-        KB_CUDA(cudaMemsetAsync(e->queue.ptr, 0, 4, st));
-        static int occ_cache[3] = {0, 0, 0};
-        if (!occ_cache[e->curve]) occ_cache[e->curve] = std::max(1, K.accumulate_occupancy());
-        int sms = 148;
+    int sms = 148;
+    {
         int dev = 0;
         KB_CUDA(cudaGetDevice(&dev));
         KB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        const size_t units = (P.seg_cap + 127) / 128;
+    }
+    if (P.L > 0) {
+        static int occ_cache[3] = {0, 0, 0};
+        if (!occ_cache[e->curve]) occ_cache[e->curve] = std::max(1, K.accumulate_occupancy());
+        const size_t units = (P.nchunks + 127) / 128;
         const unsigned grid = (unsigned)std::min<size_t>(units, (size_t)sms * occ_cache[e->curve]);
         K.accumulate(acc, std::max(1u, grid), st);
     }
     e->mark(4, st);
 
-    FoldArgs fa;
-    fa.bid = e->bid.as<uint32_t>();
-    fa.segoff = e->segoff.as<uint32_t>();
-    fa.B = P.B;
-    fa.K2 = P.K2;
-    fa.seg_cap = P.seg_cap;
-    fa.buckets = e->buckets.as<uint32_t>();
-    {
-        uint32_t* in = e->part0.as<uint32_t>();
-        uint32_t* out = e->part1.as<uint32_t>();
-        for (int l = 2; l <= P.levels + 1 && P.levels >= 2; ++l) {
-            K.fold(fa, l, in, out, st);
+    if (P.levels >= 1 && P.L > 0) {
+        FoldArgs fa;
+        fa.offsets = e->offsets.as<uint32_t>();
+        fa.B = P.B;
+        fa.K = (uint32_t)P.K;
+        fa.K2 = P.K2;
+        fa.FK = P.FK;
+        fa.big_list = big_list;
+        fa.rec_first = e->rec_first.as<uint32_t>();
+        uint32_t* in = e->rec_first.as<uint32_t>();
+        uint32_t* out = e->fold_buf.as<uint32_t>();
+        for (int l = 2; l <= P.levels + 1; ++l) {
+            K.fold(fa, l, in, out, (unsigned)sms * 4, st);
             std::swap(in, out);
         }
     }
     e->mark(5, st);
 
     RedArgs ra;
-    ra.segoff = e->segoff.as<uint32_t>();
+    ra.offsets = e->offsets.as<uint32_t>();
+    ra.B = P.B;
     ra.buckets = e->buckets.as<uint32_t>();
-    ra.partial = e->part0.as<uint32_t>();
+    ra.rec_first = e->rec_first.as<uint32_t>();
+    ra.rec_last = e->rec_last.as<uint32_t>();
+    ra.K = (uint32_t)P.K;
     ra.K2 = P.K2;
     ra.wins = P.d_wins.as<WinDesc>();
     ra.blks = P.d_blks.as<BlkDesc>();

@@ -38,31 +38,43 @@ struct BlkDesc {
     uint32_t b;    // block index within the window
 };
 
+// Level-1 accumulation over fixed chunks of K sorted entries.  Chunk t
+// writes the sum of its first bucket's run to rec_first[t], of its last
+// bucket's run (when different) to rec_last[t], and of every bucket lying
+// strictly inside the chunk directly to buckets[].
 struct AccArgs {
     const uint32_t* sorted;
-    const uint32_t* offsets;
-    const uint32_t* segoff;
+    const uint32_t* offsets;  // B + 1 bucket offsets into sorted; offsets[B] = entries
     uint32_t B;
+    uint32_t K;               // entries per chunk
     const uint32_t* table;
-    uint32_t* partial;
-    uint32_t* bid;
+    uint32_t* rec_first;
+    uint32_t* rec_last;
     uint32_t* buckets;
     uint32_t* queue;
 };
 
+// Buckets spanning more than K2 + 1 chunks ("big": the top window's carry
+// bucket for uniform scalars, the small-digit buckets of skewed inputs) have
+// their records rec_first[t0+1 .. t1] folded FK at a time per level; the
+// total lands in rec_first[t0 + 1].  big_list = {count, bucket ids...}.
 struct FoldArgs {
-    const uint32_t* bid;
-    const uint32_t* segoff;
+    const uint32_t* offsets;
     uint32_t B;
+    uint32_t K;
     int K2;
-    size_t seg_cap;
-    uint32_t* buckets;
+    int FK;
+    const uint32_t* big_list;
+    uint32_t* rec_first;
 };
 
 struct RedArgs {
-    const uint32_t* segoff;
+    const uint32_t* offsets;
+    uint32_t B;
     const uint32_t* buckets;
-    const uint32_t* partial;
+    const uint32_t* rec_first;
+    const uint32_t* rec_last;
+    uint32_t K;
     int K2;
     const WinDesc* wins;
     const BlkDesc* blks;
@@ -76,7 +88,7 @@ struct MsmLaunchers {
     void (*recode)(const ItemDesc*, uint32_t, unsigned long long, const uint32_t*,
                    const uint32_t*, uint32_t*, uint32_t*, cudaStream_t);
     void (*accumulate)(const AccArgs&, unsigned, cudaStream_t);
-    void (*fold)(const FoldArgs&, int, const uint32_t*, uint32_t*, cudaStream_t);
+    void (*fold)(const FoldArgs&, int, const uint32_t*, uint32_t*, unsigned, cudaStream_t);
     void (*reduce_blocks)(const RedArgs&, unsigned, cudaStream_t);
     void (*reduce_windows)(const RedArgs&, unsigned, cudaStream_t);
     void (*combine)(const ItemDesc*, uint32_t, const uint32_t*, uint8_t*, uint8_t*, cudaStream_t);

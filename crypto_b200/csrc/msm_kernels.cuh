@@ -139,12 +139,14 @@ __device__ __forceinline__ void load_table_point(Affine<F>& a, const uint32_t* t
     aff_load(a, w);
 }
 
-// Largest b in [0, B) with segoff[b] <= s (segoff non-decreasing, segoff[0] = 0).
-__device__ __forceinline__ uint32_t find_bucket(const uint32_t* segoff, uint32_t B, uint32_t s) {
+// Bucket holding sorted entry e: the largest b with offsets[b] <= e (empty
+// buckets share their successor's offset, so the largest one is the
+// non-empty bucket that owns e).
+__device__ __forceinline__ uint32_t bucket_of(const uint32_t* offsets, uint32_t B, uint32_t e) {
     uint32_t lo = 0, hi = B;
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (segoff[mid] <= s)
+        if (offsets[mid] <= e)
             lo = mid;
         else
             hi = mid;
@@ -152,35 +154,50 @@ __device__ __forceinline__ uint32_t find_bucket(const uint32_t* segoff, uint32_t
     return lo;
 }
 
-// Level 1, persistent: CTAs pull 32-segment work units from *queue until the
-// segment list is exhausted.  Each lane sums one segment with mixed XYZZ
-// additions: a bucket with nseg segments is split into near-equal runs.
+// Level 1, persistent: CTAs pull units of blockDim.x chunks from *queue.
+// Lane t sums chunk t = entries [tK, tK + K) of the bucket-sorted list
+// with mixed XYZZ additions, flushing at bucket boundaries: the run of the
+// chunk's first bucket goes to rec_first[t], the run of its last bucket (if
+// different) to rec_last[t], runs of buckets strictly inside the chunk
+// straight to buckets[].  Every lane does exactly K additions (the last
+// chunk fewer), whatever the bucket sizes.
 template <class C>
 __global__ void __launch_bounds__(128) k_accumulate(AccArgs a) {
     using F = typename C::F;
+    constexpr int PW = 4 * F::N;
     __shared__ uint32_t unit;
-    const uint32_t total = a.segoff[a.B];
+    // Only non-zero digits were sorted: the list length is offsets[B].
+    const uint32_t L = a.offsets[a.B];
+    const uint32_t nchunks = (L + a.K - 1) / a.K;
     for (;;) {
         if (threadIdx.x == 0) unit = atomicAdd(a.queue, 1u);
         __syncthreads();
         const uint32_t base = unit * blockDim.x;
         __syncthreads();
-        if (base >= total) return;
-        const uint32_t s = base + threadIdx.x;
-        if (s < total) {
-            const uint32_t b = find_bucket(a.segoff, a.B, s);
-            const uint32_t q = s - a.segoff[b];
-            const uint32_t nseg = a.segoff[b + 1] - a.segoff[b];
-            const uint32_t off = a.offsets[b];
-            const uint32_t cnt = a.offsets[b + 1] - off;
-            const uint32_t start = off + (uint32_t)(((uint64_t)q * cnt) / nseg);
-            const uint32_t end = off + (uint32_t)(((uint64_t)(q + 1) * cnt) / nseg);
+        if (base >= nchunks) return;
+        const uint32_t t = base + threadIdx.x;
+        if (t < nchunks) {
+            const uint32_t e0 = t * a.K;
+            const uint32_t e1 = min(e0 + a.K, L);
+            uint32_t b = bucket_of(a.offsets, a.B, e0);
+            uint32_t bend = a.offsets[b + 1];
+            uint32_t run0 = e0;
             Xyzz<F> acc;
             xyzz_set_inf(acc);
-            uint32_t v = start < end ? a.sorted[start] : 0u;
-            for (uint32_t e = start; e < end; ++e) {
-                const uint32_t vn = (e + 1 < end) ? a.sorted[e + 1] : 0u;
-                if (e + 1 < end) {
+            uint32_t v = a.sorted[e0];
+            for (uint32_t e = e0; e < e1; ++e) {
+                if (e == bend) {
+                    // flush the finished run [run0, e) of bucket b
+                    uint32_t* dst = (run0 == e0) ? a.rec_first + (size_t)t * PW
+                                                 : a.buckets + (size_t)b * PW;
+                    xyzz_store(dst, acc);
+                    xyzz_set_inf(acc);
+                    while (a.offsets[b + 1] <= e) ++b;
+                    bend = a.offsets[b + 1];
+                    run0 = e;
+                }
+                const uint32_t vn = (e + 1 < e1) ? a.sorted[e + 1] : 0u;
+                if (e + 1 < e1) {
                     const uint32_t* nxt = a.table + (size_t)(vn & 0x7fffffffu) * 2 * F::N;
                     asm volatile("prefetch.global.L2 [%0];" ::"l"(nxt));
                 }
@@ -190,47 +207,44 @@ __global__ void __launch_bounds__(128) k_accumulate(AccArgs a) {
                 xyzz_add_affine(acc, p);
                 v = vn;
             }
-            a.bid[s] = b;
-            if (nseg == 1)
-                xyzz_store(a.buckets + (size_t)b * 4 * F::N, acc);
-            else
-                xyzz_store(a.partial + (size_t)s * 4 * F::N, acc);
+            uint32_t* dst = (run0 == e0) ? a.rec_first + (size_t)t * PW : a.rec_last + (size_t)t * PW;
+            xyzz_store(dst, acc);
         }
     }
 }
 
-// Level l >= 2 for buckets with more than K2 segments: fold K2 partial sums
-// at a time; the last level writes the bucket.  Buckets with 2..K2
-// segments are left to the reduction, which sums their partials directly.
+// Fold level l >= 2 over the listed big buckets.  Bucket g covers chunks
+// t0..t1; its n_1 = t1 - t0 records rec_first[t0+1 .. t1] are summed FK at
+// a time per level (n_l = ceil(n_{l-1} / FK)); the level that reaches one
+// item writes the total to rec_first[t0 + 1].  The whole grid works on each
+// listed bucket in turn; with no big bucket the kernel exits at once.
 template <class C>
 __global__ void __launch_bounds__(128) k_fold(FoldArgs a, int level, const uint32_t* __restrict__ in,
                                               uint32_t* __restrict__ out) {
     using F = typename C::F;
-    const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= a.seg_cap) return;
-    const uint32_t total = a.segoff[a.B];
-    if (s >= total) return;
-    const uint32_t b = a.bid[s];
-    const uint32_t base = a.segoff[b];
-    const uint32_t nseg = a.segoff[b + 1] - base;
-    if (nseg <= (uint32_t)a.K2) return;
-    const uint32_t q = (uint32_t)s - base;
-    uint32_t n_prev = nseg;
-    for (int l = 2; l < level; ++l) n_prev = (n_prev + a.K2 - 1) / a.K2;
-    if (n_prev <= 1) return;
-    const uint32_t n_cur = (n_prev + a.K2 - 1) / a.K2;
-    if (q >= n_cur) return;
-    const uint32_t lo = q * (uint32_t)a.K2, hi = min(lo + (uint32_t)a.K2, n_prev);
-    Xyzz<F> acc, t;
-    xyzz_load(acc, in + (size_t)(base + lo) * 4 * F::N);
-    for (uint32_t j = lo + 1; j < hi; ++j) {
-        xyzz_load(t, in + (size_t)(base + j) * 4 * F::N);
-        xyzz_add(acc, t);
+    constexpr int PW = 4 * F::N;
+    const uint32_t nbig = a.big_list[0];
+    for (uint32_t k = 0; k < nbig; ++k) {
+        const uint32_t g = a.big_list[1 + k];
+        const uint32_t o = a.offsets[g], c = a.offsets[g + 1] - o;
+        const uint32_t t0 = o / a.K, t1 = (o + c - 1) / a.K;
+        uint32_t n_prev = t1 - t0;
+        for (int l = 2; l < level; ++l) n_prev = (n_prev + a.FK - 1) / a.FK;
+        if (n_prev <= 1) continue;
+        const uint32_t n_cur = (n_prev + a.FK - 1) / a.FK;
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cur;
+             i += gridDim.x * blockDim.x) {
+            const uint32_t lo = i * (uint32_t)a.FK, hi = min(lo + (uint32_t)a.FK, n_prev);
+            Xyzz<F> acc, x;
+            xyzz_load(acc, in + (size_t)(t0 + 1 + lo) * PW);
+            for (uint32_t j = lo + 1; j < hi; ++j) {
+                xyzz_load(x, in + (size_t)(t0 + 1 + j) * PW);
+                xyzz_add(acc, x);
+            }
+            uint32_t* dst = (n_cur == 1) ? a.rec_first : out;
+            xyzz_store(dst + (size_t)(t0 + 1 + i) * PW, acc);
+        }
     }
-    if (n_cur == 1)
-        xyzz_store(a.buckets + (size_t)b * 4 * F::N, acc);
-    else
-        xyzz_store(out + (size_t)(base + q) * 4 * F::N, acc);
 }
 
 template <class F>
@@ -238,55 +252,89 @@ __device__ __forceinline__ void xyzz_dbl_n(Xyzz<F>& p, int k) {
     for (int i = 0; i < k; ++i) xyzz_dbl(p, p);
 }
 
-// Sum of global bucket g: its single accumulator, or its 2..K2 partials.
+// R += B_g, gathering the bucket's pieces from the chunk records (see
+// k_accumulate for where each piece lives).  All pieces go through one
+// addition call site, so lanes whose buckets are split differently stay
+// converged instead of serialising through separate inlined copies.
 template <class F>
-__device__ __forceinline__ void bucket_value(Xyzz<F>& r, const RedArgs& a, uint32_t g) {
-    const uint32_t s0 = a.segoff[g], nseg = a.segoff[g + 1] - s0;
-    if (nseg == 0) {
-        xyzz_set_inf(r);
-    } else if (nseg == 1 || nseg > (uint32_t)a.K2) {
-        xyzz_load(r, a.buckets + (size_t)g * 4 * F::N);
+__device__ __forceinline__ void bucket_add(Xyzz<F>& R, const RedArgs& a, uint32_t g) {
+    constexpr int PW = 4 * F::N;
+    const uint32_t o = a.offsets[g], c = a.offsets[g + 1] - o;
+    if (c == 0) return;
+    const uint32_t t0 = o / a.K, t1 = (o + c - 1) / a.K;
+    const uint32_t* first;
+    uint32_t npieces;
+    if (t0 == t1) {
+        const uint32_t e0 = t0 * a.K, e1 = min(e0 + a.K, a.offsets[a.B]);
+        first = (o == e0) ? a.rec_first + (size_t)t0 * PW
+                : (o + c == e1) ? a.rec_last + (size_t)t0 * PW
+                                : a.buckets + (size_t)g * PW;
+        npieces = 1;
     } else {
-        Xyzz<F> t;
-        xyzz_load(r, a.partial + (size_t)s0 * 4 * F::N);
-        for (uint32_t i = 1; i < nseg; ++i) {
-            xyzz_load(t, a.partial + (size_t)(s0 + i) * 4 * F::N);
-            xyzz_add(r, t);
-        }
+        first = ((o == t0 * a.K) ? a.rec_first : a.rec_last) + (size_t)t0 * PW;
+        // a big bucket's records t0+1..t1 were folded into rec_first[t0+1]
+        npieces = 1 + ((t1 - t0 > (uint32_t)a.K2) ? 1u : (t1 - t0));
+    }
+    for (uint32_t k = 0; k < npieces; ++k) {
+        const uint32_t* src = (k == 0) ? first : a.rec_first + (size_t)(t0 + k) * PW;
+        Xyzz<F> x;
+        xyzz_load(x, src);
+        xyzz_add(R, x);
     }
 }
 
-// In-place suffix scan over sm[0..n) (n = blockDim.x) of XYZZ points:
-// afterwards sm[t] = sum_{t' >= t} old sm[t'].
+// Shared-memory XYZZ arrays are word-major: word i of slot t lives at
+// sm[i * RED_THREADS + t], so a warp touching its 32 slots hits 32 banks.
+template <class F>
+__device__ __forceinline__ void sm_load(Xyzz<F>& p, const uint32_t* sm, int t) {
+#pragma unroll
+    for (int i = 0; i < F::N; ++i) {
+        p.X.v[i] = sm[(i)*RED_THREADS + t];
+        p.Y.v[i] = sm[(F::N + i) * RED_THREADS + t];
+        p.ZZ.v[i] = sm[(2 * F::N + i) * RED_THREADS + t];
+        p.ZZZ.v[i] = sm[(3 * F::N + i) * RED_THREADS + t];
+    }
+}
+template <class F>
+__device__ __forceinline__ void sm_store(uint32_t* sm, int t, const Xyzz<F>& p) {
+#pragma unroll
+    for (int i = 0; i < F::N; ++i) {
+        sm[(i)*RED_THREADS + t] = p.X.v[i];
+        sm[(F::N + i) * RED_THREADS + t] = p.Y.v[i];
+        sm[(2 * F::N + i) * RED_THREADS + t] = p.ZZ.v[i];
+        sm[(3 * F::N + i) * RED_THREADS + t] = p.ZZZ.v[i];
+    }
+}
+
+// In-place suffix scan over the RED_THREADS slots of sm:
+// afterwards slot t = sum_{t' >= t} old slot t'.
 template <class F>
 __device__ __forceinline__ void smem_suffix_scan(uint32_t* sm) {
-    constexpr int PW = 4 * F::N;
-    const int t = threadIdx.x, n = blockDim.x;
-    for (int d = 1; d < n; d <<= 1) {
+    const int t = threadIdx.x;
+    for (int d = 1; d < RED_THREADS; d <<= 1) {
         Xyzz<F> y, o;
-        xyzz_load(y, sm + (size_t)t * PW);
-        if (t + d < n) {
-            xyzz_load(o, sm + (size_t)(t + d) * PW);
+        sm_load(y, sm, t);
+        if (t + d < RED_THREADS) {
+            sm_load(o, sm, t + d);
             xyzz_add(y, o);
         }
         __syncthreads();
-        xyzz_store(sm + (size_t)t * PW, y);
+        sm_store(sm, t, y);
         __syncthreads();
     }
 }
 
-// In-place tree sum over sm[0..n): afterwards sm[0] = sum.
+// In-place tree sum over the RED_THREADS slots of sm: afterwards slot 0 = sum.
 template <class F>
 __device__ __forceinline__ void smem_tree_sum(uint32_t* sm) {
-    constexpr int PW = 4 * F::N;
     const int t = threadIdx.x;
-    for (int d = blockDim.x >> 1; d >= 1; d >>= 1) {
+    for (int d = RED_THREADS >> 1; d >= 1; d >>= 1) {
         if (t < d) {
             Xyzz<F> y, o;
-            xyzz_load(y, sm + (size_t)t * PW);
-            xyzz_load(o, sm + (size_t)(t + d) * PW);
+            sm_load(y, sm, t);
+            sm_load(o, sm, t + d);
             xyzz_add(y, o);
-            xyzz_store(sm + (size_t)t * PW, y);
+            sm_store(sm, t, y);
         }
         __syncthreads();
     }
@@ -303,42 +351,44 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_blocks(RedArgs a) {
     constexpr int PW = 4 * F::N;
     extern __shared__ __align__(16) uint32_t smr[];
     uint32_t* sA = smr;                       // R_t -> suffix sums -> tree
-    uint32_t* sB = smr + RED_THREADS * PW;    // T_t -> tree
+    uint32_t* sB = smr + RED_THREADS * PW;    // T_t (kept here, not in registers)
     const BlkDesc bd = a.blks[blockIdx.x];
     const WinDesc wd = a.wins[bd.win];
     const uint32_t S = 1u << wd.log_S;
     const uint32_t first = bd.b * (RED_THREADS << wd.log_S) + threadIdx.x * S;
+    const int me = threadIdx.x;
     {
-        Xyzz<F> R, T, Bk;
+        Xyzz<F> R;
         xyzz_set_inf(R);
-        xyzz_set_inf(T);
+        sm_store(sB, me, R);
         for (int j = (int)S - 1; j >= 0; --j) {
-            if (first + (uint32_t)j < wd.Mw) {
-                bucket_value(Bk, a, wd.bucket_base + first + (uint32_t)j);
-                xyzz_add(R, Bk);
+            if (first + (uint32_t)j < wd.Mw) bucket_add(R, a, wd.bucket_base + first + (uint32_t)j);
+            if (j > 0) {
+                Xyzz<F> T;
+                sm_load(T, sB, me);
+                xyzz_add(T, R);
+                sm_store(sB, me, T);
             }
-            if (j > 0) xyzz_add(T, R);
         }
-        xyzz_store(sA + (size_t)threadIdx.x * PW, R);
-        xyzz_store(sB + (size_t)threadIdx.x * PW, T);
+        sm_store(sA, me, R);
     }
     __syncthreads();
     smem_suffix_scan<F>(sA);
     Xyzz<F> Y0;
     if (threadIdx.x == 0) {
-        xyzz_load(Y0, sA);
+        sm_load(Y0, sA, 0);
         Xyzz<F> inf;
         xyzz_set_inf(inf);
-        xyzz_store(sA, inf);  // the tree below sums Y_t for t >= 1
+        sm_store(sA, 0, inf);  // the tree below sums Y_t for t >= 1
     }
     __syncthreads();
     smem_tree_sum<F>(sA);
     smem_tree_sum<F>(sB);
     if (threadIdx.x == 0) {
         Xyzz<F> Fb, t;
-        xyzz_load(Fb, sA);
+        sm_load(Fb, sA, 0);
         xyzz_dbl_n(Fb, (int)wd.log_S);
-        xyzz_load(t, sB);
+        sm_load(t, sB, 0);
         xyzz_add(Fb, t);
         xyzz_store(a.blk_out + ((size_t)blockIdx.x * 2) * PW, Fb);
         xyzz_store(a.blk_out + ((size_t)blockIdx.x * 2 + 1) * PW, Y0);
@@ -365,26 +415,26 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_windows(RedArgs a) {
             xyzz_load(Fb, a.blk_out + ((size_t)(wd.blk_base + t) * 2) * PW);
             xyzz_load(Sb, a.blk_out + ((size_t)(wd.blk_base + t) * 2 + 1) * PW);
         }
-        xyzz_store(sA + (size_t)t * PW, Sb);
-        xyzz_store(sB + (size_t)t * PW, Fb);
+        sm_store(sA, (int)t, Sb);
+        sm_store(sB, (int)t, Fb);
     }
     __syncthreads();
     smem_suffix_scan<F>(sA);
     Xyzz<F> Y0;
     if (t == 0) {
-        xyzz_load(Y0, sA);
+        sm_load(Y0, sA, 0);
         Xyzz<F> inf;
         xyzz_set_inf(inf);
-        xyzz_store(sA, inf);
+        sm_store(sA, 0, inf);
     }
     __syncthreads();
     smem_tree_sum<F>(sA);
     smem_tree_sum<F>(sB);
     if (t == 0) {
         Xyzz<F> V, u;
-        xyzz_load(V, sA);
+        sm_load(V, sA, 0);
         xyzz_dbl_n(V, (int)wd.log_blk);
-        xyzz_load(u, sB);
+        sm_load(u, sB, 0);
         xyzz_add(V, u);
         xyzz_add(V, Y0);
         xyzz_store(a.win_out + (size_t)blockIdx.x * PW, V);
@@ -478,8 +528,8 @@ struct MsmLaunchImpl {
         KB_LAUNCH_CHECK();
     }
     static void fold(const FoldArgs& a, int level, const uint32_t* in, uint32_t* out,
-                     cudaStream_t st) {
-        k_fold<C><<<ceil_div_u(a.seg_cap, 128), 128, 0, st>>>(a, level, in, out);
+                     unsigned grid, cudaStream_t st) {
+        k_fold<C><<<grid, 128, 0, st>>>(a, level, in, out);
         KB_LAUNCH_CHECK();
     }
     static size_t red_smem() { return (size_t)2 * RED_THREADS * 4 * F::N * 4; }
