@@ -90,6 +90,29 @@ KB_DEV void xyzz_dbl(Xyzz<F>& r, const Xyzz<F>& p) {
     r.Y = Y3;
 }
 
+// dbl-2008-s-1 with the products inlined: for long serial doubling chains
+// (window combine), where one inlined copy in a loop beats a call per product.
+template <class F>
+KB_DEV void xyzz_dbl_inl(Xyzz<F>& p) {
+    Fe<F> U, V, W, S, M, t;
+    fe_dbl(U, p.Y);
+    fe_sqr_inl(V, U);
+    fe_mul_inl(W, U, V);
+    fe_mul_inl(S, p.X, V);
+    fe_sqr_inl(t, p.X);
+    fe_dbl(M, t);
+    fe_add(M, M, t);
+    fe_mul_inl(p.ZZ, V, p.ZZ);
+    fe_mul_inl(p.ZZZ, W, p.ZZZ);
+    fe_mul_inl(W, W, p.Y);
+    fe_sqr_inl(p.X, M);
+    fe_sub(p.X, p.X, S);
+    fe_sub(p.X, p.X, S);
+    fe_sub(t, S, p.X);
+    fe_mul_inl(p.Y, M, t);
+    fe_sub(p.Y, p.Y, W);
+}
+
 // mdbl-2008-s-1: r = 2 * (affine a).
 template <class F>
 KB_DEV void xyzz_mdbl(Xyzz<F>& r, const Affine<F>& a) {

@@ -233,7 +233,7 @@ KB_DEV void reduce_once(Fe<F>& r, const uint32_t* t) {
 
 // r = a * b * R^-1 mod p, inputs and output in [0, p).
 template <class F>
-KB_DEV void fe_mul(Fe<F>& r, const Fe<F>& a, const Fe<F>& b) {
+KB_DEV void fe_mul_inl(Fe<F>& r, const Fe<F>& a, const Fe<F>& b) {
     constexpr int N = F::N;
     uint32_t p[N];
 #pragma unroll
@@ -253,9 +253,36 @@ KB_DEV void fe_mul(Fe<F>& r, const Fe<F>& a, const Fe<F>& b) {
     reduce_once<F>(r, t);
 }
 
+// Out-of-line copy: one instance of the ~640-instruction product per
+// kernel instead of one per call site, which keeps large kernels (bucket
+// reduction, window combine) inside the instruction cache.
+template <class F>
+__device__ __noinline__ Fe<F> fe_mul_call(Fe<F> a, Fe<F> b) {
+    Fe<F> r;
+    fe_mul_inl<F>(r, a, b);
+    return r;
+}
+
+#ifndef KB_MUL_INLINE
+#define KB_MUL_INLINE 0
+#endif
+
+template <class F>
+KB_DEV void fe_mul(Fe<F>& r, const Fe<F>& a, const Fe<F>& b) {
+#if KB_MUL_INLINE
+    fe_mul_inl<F>(r, a, b);
+#else
+    r = fe_mul_call<F>(a, b);
+#endif
+}
+
 template <class F>
 KB_DEV void fe_sqr(Fe<F>& r, const Fe<F>& a) {
     fe_mul<F>(r, a, a);
+}
+template <class F>
+KB_DEV void fe_sqr_inl(Fe<F>& r, const Fe<F>& a) {
+    fe_mul_inl<F>(r, a, a);
 }
 
 template <class F>

@@ -460,7 +460,7 @@ __global__ void k_combine(const ItemDesc* __restrict__ items, uint32_t n_items,
     } else {
         xyzz_load(acc, wins + (size_t)(it.win_base + it.W - 1) * PW);
         for (int w = (int)it.W - 2; w >= 0; --w) {
-            xyzz_dbl_n(acc, (int)it.c);
+            for (uint32_t k = 0; k < it.c; ++k) xyzz_dbl_inl(acc);
             xyzz_load(t, wins + (size_t)(it.win_base + (uint32_t)w) * PW);
             xyzz_add(acc, t);
         }
