@@ -50,6 +50,7 @@ def lib() -> ctypes.CDLL:
             "gpukit_multi_pippenger_cuda": (c.c_int, [c.c_uint32, u8p, u8p, sz, vp]),
             "ntt_fr_forward": (c.c_int, [c.c_int, vp, sz, c.c_int]),
             "ntt_fr_inverse": (c.c_int, [c.c_int, vp, sz, c.c_int]),
+            "ntt_fr_transform_noalloc": (c.c_int, [c.c_int, vp, sz, c.c_int, c.c_int]),
             "kzg_srs_load_g1": (c.c_int, [u8p, sz]),
             "kzg_srs_generate_g1": (c.c_int, [u8p, sz]),
             "kzg_srs_read_g1": (c.c_int, [vp, sz, sz]),
@@ -122,6 +123,15 @@ def ntt_fr(curve: int, data: bytes, inverse: bool = False, coset: bool = False) 
     buf = ctypes.create_string_buffer(bytes(data), len(data))
     fn = lib().ntt_fr_inverse if inverse else lib().ntt_fr_forward
     _check("ntt_fr_inverse" if inverse else "ntt_fr_forward", fn(curve, buf, n, int(coset)))
+    return buf.raw
+
+
+def ntt_fr_noalloc(curve: int, data: bytes, inverse: bool = False, coset: bool = False) -> bytes:
+    """Allocation-free variant (n <= 2^16), scratch in a static device array."""
+    n = len(data) // 32
+    buf = ctypes.create_string_buffer(bytes(data), len(data))
+    _check("ntt_fr_transform_noalloc",
+           lib().ntt_fr_transform_noalloc(curve, buf, n, int(inverse), int(coset)))
     return buf.raw
 
 

@@ -1,5 +1,6 @@
 // Fr NTT kernels and host driver.  See ntt.cuh for the contract and the
 // pass structure.
+#include "../../include/kinet_b200/crypto_b200.h"
 #include "field.cuh"
 #include "ntt.cuh"
 #include "runtime.cuh"
@@ -580,4 +581,192 @@ void ntt_run_list(NttEngine* e, uint32_t* d, size_t n, int inverse, int coset, s
         run_impl<FrBN>(e, d, n, inverse, coset, count, d_vec_off, d_scratch, st);
 }
 
+
+// ---------------------------------------------------------------------------
+// Allocation-free Fr NTT.
+//
+// Some callers cannot allocate device memory: code that runs while a CUDA
+// graph is being captured, a latency-critical path where cudaMalloc's
+// implicit device-wide synchronisation is unacceptable, or a process whose
+// device memory is entirely owned by another allocator (a framework's
+// caching pool).  For them ntt_fr_transform_noalloc keeps all its scratch --
+// the transform buffer, the pass ping-pong buffer, the twiddle table, the
+// coset tables and the constants -- in one file-scope device array of fixed
+// size, so a call allocates nothing.  The limit is n <= 2^16 elements
+// (6.8 MB of scratch); every GPU that loads this library holds the array
+// until the process exits.
+// ---------------------------------------------------------------------------
+
+constexpr int NOALLOC_MAX_LOG = 16;
+constexpr size_t NOALLOC_MAX_N = (size_t)1 << NOALLOC_MAX_LOG;
+constexpr size_t NOALLOC_TAB = (size_t)1 << TAB_SPLIT;                    // 8192
+constexpr size_t NOALLOC_HI = NOALLOC_MAX_N >> TAB_SPLIT;                  // 8
+// Element (32-byte) offsets of the regions inside the array.
+constexpr size_t NA_DATA = 0;
+constexpr size_t NA_SCR = NA_DATA + NOALLOC_MAX_N;
+constexpr size_t NA_TW = NA_SCR + NOALLOC_MAX_N;
+constexpr size_t NA_PRE_LO = NA_TW + NOALLOC_MAX_N;
+constexpr size_t NA_POST_LO = NA_PRE_LO + NOALLOC_TAB;
+constexpr size_t NA_PRE_HI = NA_POST_LO + NOALLOC_TAB;
+constexpr size_t NA_POST_HI = NA_PRE_HI + NOALLOC_HI;
+constexpr size_t NA_CONST = NA_POST_HI + NOALLOC_HI;  // 8 constant slots
+constexpr size_t NA_ELTS = NA_CONST + 8;
+
+static __device__ __align__(256) uint32_t g_ntt_noalloc_scratch[NA_ELTS * 8];
+
+namespace {
+
+// Device address of the scratch array, resolved once per device (with that
+// device current) by cudaGetSymbolAddress; host code must never use the
+// array's name itself as a device address.
+std::mutex g_na_mu;
+std::map<int, uint32_t*> g_na_ptr;
+
+uint32_t* noalloc_scratch() {
+    int dev = 0;
+    KB_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_na_mu);
+    auto it = g_na_ptr.find(dev);
+    if (it != g_na_ptr.end()) return it->second;
+    void* p = nullptr;
+    KB_CUDA(cudaGetSymbolAddress(&p, g_ntt_noalloc_scratch));
+    g_na_ptr[dev] = static_cast<uint32_t*>(p);
+    return static_cast<uint32_t*>(p);
+}
+
+template <class F>
+void noalloc_impl(uint8_t* h_data, size_t n, int inverse, int coset) {
+    int log_n = 0;
+    while (((size_t)1 << log_n) < n) ++log_n;
+    uint32_t* base = noalloc_scratch();
+    auto at = [&](size_t elt) { return base + elt * 8; };
+    uint32_t* C = at(NA_CONST);  // slots: 0 w_n, 1 exponent, 2 g, 3 g^-1, 4 n^-1 std, 5 n^-1
+    const cudaStream_t st = 0;   // legacy default stream; cudaMemcpy orders with it
+    const int TB = 256;
+    KB_CUDA(cudaMemcpy(at(NA_DATA), h_data, n * 32, cudaMemcpyHostToDevice));
+    // Everything read below is written first in this call, so no region has
+    // to start at zero and the previous call's contents never leak in.
+    uint32_t ex[8];
+    exp_words<F>(ex, 0, log_n);
+    KB_CUDA(cudaMemcpy(C + 8, ex, 32, cudaMemcpyHostToDevice));
+    k_pow_gen<F><<<1, 32, 0, st>>>(C + 8, C + 0);  // w_n
+    KB_LAUNCH_CHECK();
+    k_powers<F><<<ceil_div_u(n, TB), TB, 0, st>>>(C + 0, 1, n, at(NA_TW));
+    KB_LAUNCH_CHECK();
+    uint32_t ni[8];
+    ninv_words<F>(ni, log_n);
+    KB_CUDA(cudaMemcpy(C + 32, ni, 32, cudaMemcpyHostToDevice));
+    k_to_mont<F><<<1, 32, 0, st>>>(C + 32, C + 40, 1);
+    KB_LAUNCH_CHECK();
+    if (coset) {
+        uint32_t one[8] = {1, 0, 0, 0, 0, 0, 0, 0};
+        KB_CUDA(cudaMemcpy(C + 8, one, 32, cudaMemcpyHostToDevice));
+        k_pow_gen<F><<<1, 32, 0, st>>>(C + 8, C + 16);  // g
+        KB_LAUNCH_CHECK();
+        exp_words<F>(ex, 1, 0);
+        KB_CUDA(cudaMemcpy(C + 8, ex, 32, cudaMemcpyHostToDevice));
+        k_pow_gen<F><<<1, 32, 0, st>>>(C + 8, C + 24);  // g^-1
+        KB_LAUNCH_CHECK();
+        k_powers<F><<<ceil_div_u(NOALLOC_TAB, TB), TB, 0, st>>>(C + 16, 1, NOALLOC_TAB, at(NA_PRE_LO));
+        KB_LAUNCH_CHECK();
+        k_powers<F><<<1, 32, 0, st>>>(C + 16, NOALLOC_TAB, NOALLOC_HI, at(NA_PRE_HI));
+        KB_LAUNCH_CHECK();
+        k_powers<F><<<ceil_div_u(NOALLOC_TAB, TB), TB, 0, st>>>(C + 24, 1, NOALLOC_TAB, at(NA_POST_LO));
+        KB_LAUNCH_CHECK();
+        k_scale_table<F><<<ceil_div_u(NOALLOC_TAB, TB), TB, 0, st>>>(at(NA_POST_LO), NOALLOC_TAB, C + 32);
+        KB_LAUNCH_CHECK();
+        k_powers<F><<<1, 32, 0, st>>>(C + 24, NOALLOC_TAB, NOALLOC_HI, at(NA_POST_HI));
+        KB_LAUNCH_CHECK();
+    }
+    // The same passes as the resident path, over the static buffers.
+    int logs[2], P;
+    if (log_n <= 12) {
+        P = 1;
+        logs[0] = log_n;
+    } else {
+        P = 2;
+        logs[0] = (log_n + 1) / 2;
+        logs[1] = log_n - logs[0];
+    }
+    uint32_t* d = at(NA_DATA);
+    uint32_t* scr = at(NA_SCR);
+    int log_mprev = log_n;
+    for (int p = 0; p < P; ++p) {
+        PassArgs a{};
+        a.tw = at(NA_TW);
+        a.log_nt = log_n;
+        a.log_n = log_n;
+        a.log_R = logs[p];
+        a.log_m = log_mprev - logs[p];
+        a.log_mprev = log_mprev;
+        a.inverse = inverse;
+        a.first = (p == 0);
+        a.final = (p == P - 1);
+        a.log_R1 = (P == 1) ? 0 : logs[0];
+        a.batch_stride = n;
+        if (a.first && coset && !inverse) {
+            a.pre_hi = at(NA_PRE_HI);
+            a.pre_lo = at(NA_PRE_LO);
+        }
+        if (a.final && inverse) {
+            if (coset) {
+                a.post_hi = at(NA_POST_HI);
+                a.post_lo = at(NA_POST_LO);
+            } else {
+                a.post_const = C + 40;
+            }
+        }
+        int log_cb = 12 - a.log_R;
+        if (!a.final) {
+            if (log_cb > a.log_m) log_cb = a.log_m;
+        } else {
+            if (log_cb > a.log_R1) log_cb = a.log_R1;
+        }
+        a.log_cb = log_cb;
+        a.in = (P == 1 || p == 0) ? d : scr;
+        a.out = (P == 1 || a.final) ? d : scr;
+        const size_t nblk = ((size_t)1 << (log_n - a.log_R)) >> log_cb;
+        const size_t smem = (((size_t)8 << (log_cb + a.log_R)) + ((size_t)8 << a.log_R) / 2) * 4 + 64;
+        set_smem_attr((const void*)k_ntt_pass<F>, ((size_t)8 * NTT_SMEM_ELTS + 8 * 2048) * 4 + 64);
+        k_ntt_pass<F><<<dim3((unsigned)nblk, 1), NTT_THREADS, smem, st>>>(a);
+        KB_LAUNCH_CHECK();
+        log_mprev = a.log_m;
+    }
+    KB_CUDA(cudaMemcpy(h_data, at(NA_DATA), n * 32, cudaMemcpyDeviceToHost));
+}
+
+}  // namespace
+
+}  // namespace kb200
+
+extern "C" int ntt_fr_transform_noalloc(int curve, uint8_t* coeffs32le, size_t n, int inverse,
+                                        int coset) {
+    using namespace kb200;
+    if (!coeffs32le) return KB200_CRYPTO_ERR_INPUT;
+    if (curve != 1 && curve != 2) return KB200_CRYPTO_ERR_INPUT;
+    if (n == 0 || (n & (n - 1))) return KB200_CRYPTO_ERR_LENGTH;
+    if (n > NOALLOC_MAX_N) {
+        set_last_error("ntt_fr_transform_noalloc: n exceeds the 2^16-element static scratch "
+                       "(use ntt_fr_forward / ntt_fr_inverse for larger transforms)");
+        return KB200_CRYPTO_ERR_LENGTH;
+    }
+    try {
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+            cudaGetLastError();
+            set_last_error("no usable CUDA device (kinet-b200 has no CPU fallback)");
+            return KB200_CRYPTO_ERR_BACKEND;
+        }
+        if (curve == 2)
+            noalloc_impl<FrBLS>(coeffs32le, n, inverse, coset);
+        else
+            noalloc_impl<FrBN>(coeffs32le, n, inverse, coset);
+        return KB200_CRYPTO_OK;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return KB200_CRYPTO_ERR_BACKEND;
+    }
+}
+
+namespace kb200 {
 }  // namespace kb200

@@ -128,6 +128,21 @@ int kzg_server_stats(void* server, double* p50_ms, double* p99_ms, double* commi
                      uint64_t* completed, int reset);
 int kzg_server_destroy(void* server);
 
+/* ---- Allocation-free Fr NTT -------------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory (inside a CUDA graph capture, on a latency-critical path where
+ * cudaMalloc's implicit device synchronisation is unacceptable, or in a
+ * process whose device memory belongs to another allocator): the same
+ * transform as ntt_fr_forward / ntt_fr_inverse (inverse != 0) for
+ * n <= 2^16, with all scratch in a fixed 6.8 MB file-scope device array that
+ * every GPU loading this library holds until exit.  Allocates nothing: no
+ * cudaMalloc/cudaFree or allocating library call.  n > 2^16 returns
+ * CRYPTO_ERR_LENGTH.  The first call on a device resolves the array's
+ * address for that device and should come before any stream capture.  All
+ * calls share the one array, so calls that overlap on the GPU (from several
+ * host threads) race; callers must serialise them. */
+int ntt_fr_transform_noalloc(int curve, uint8_t* coeffs32le, size_t n, int inverse, int coset);
+
 /* ---- Device-pointer entry points (inputs already resident in HBM) ------ */
 /* Pointers are device pointers (16-byte aligned), `stream` is a
  * cudaStream_t (NULL = legacy default stream); work is queued, not
