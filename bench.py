@@ -175,6 +175,86 @@ def make_inputs(n: int, seed: int):
     return d_sc, d_pts
 
 
+def w_ntt(n: int) -> int:
+    """Algorithmic IMAD of one Fr NTT: (n/2) log2 n Montgomery products, M(8) each."""
+    return (n // 2) * (n.bit_length() - 1) * mont_imad(8)
+
+
+def time_device(fn, steps: int, warmup: int) -> float:
+    """Mean ms per call of fn (queued on torch's current stream), CUDA events."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def bench_extra(args, peak_imad: float) -> dict:
+    """The other single-transform configurations: BLS12-381 MSM 2^20, BN254 MSM
+    2^24 (uniform and skewed scalars), BLS12-381 Fr NTT 2^24 forward + inverse,
+    BN254 coset NTT 2^26 forward + inverse.  Device-resident inputs."""
+    import torch
+    import crypto_b200 as kb
+    L = kb.lib()
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = {}
+
+    def msm_case(curve, logn, kind, label):
+        n = 1 << logn
+        pb = 96 if curve == 2 else 64
+        sc = kb.gen_scalars(curve, 31 + logn, n, kind)
+        ks = kb.gen_scalars(curve, 77 + logn, n)
+        d_sc = torch.frombuffer(bytearray(sc), dtype=torch.uint8).cuda()
+        d_ks = torch.frombuffer(bytearray(ks), dtype=torch.uint8).cuda()
+        d_pts = torch.empty(n * pb, dtype=torch.uint8, device="cuda")
+        assert L.kb200_g1_fixed_base_device(curve, d_ks.data_ptr(), n, d_pts.data_ptr(), sp) == 0
+        del d_ks
+        d_out = torch.empty(pb, dtype=torch.uint8, device="cuda")
+        kb.profile_enable(True)
+        ms = time_device(lambda: L.kb200_msm_device(curve, d_sc.data_ptr(), d_pts.data_ptr(), n,
+                                                     d_out.data_ptr(), sp), 3, 2)
+        stage = kb.msm_stage_ms(curve)
+        kb.profile_enable(False)
+        nl = 12 if curve == 2 else 8
+        out[label] = {"n": n, "ms": ms, "mpts_per_s": n / ms / 1e3, "window_bits": kb.msm_window(curve, n),
+                      "imad_frac": w_msm(n, nl) / (ms / 1e3) / peak_imad, "stage_ms": stage}
+        del d_sc, d_pts, d_out
+        torch.cuda.empty_cache()
+
+    def ntt_case(curve, logn, coset, label):
+        n = 1 << logn
+        x = kb.gen_scalars(curve, 5 + logn, n)
+        d = torch.frombuffer(bytearray(x), dtype=torch.uint8).cuda()
+
+        def fwd_inv():
+            assert L.kb200_ntt_device(curve, d.data_ptr(), n, 0, coset, 1, sp) == 0
+            assert L.kb200_ntt_device(curve, d.data_ptr(), n, 1, coset, 1, sp) == 0
+
+        ms = time_device(fwd_inv, 3, 2)
+        assert d.cpu().numpy().tobytes() == x, "NTT round trip changed the data"
+        passes = 1 if logn <= 12 else (2 if logn <= 20 else 3)
+        bytes_moved = 2 * passes * 64 * n + 2 * (passes - 1) * 32 * n
+        out[label] = {"n": n, "coset": bool(coset), "ms_fwd_plus_inv": ms,
+                      "imad_frac": 2 * w_ntt(n) / (ms / 1e3) / peak_imad,
+                      "hbm_gbs": bytes_moved / (ms / 1e3) / 1e9}
+        del d
+        torch.cuda.empty_cache()
+
+    msm_case(2, 20, 0, "msm_bls12_381_2^20")
+    msm_case(1, 24, 0, "msm_bn254_2^24_uniform")
+    msm_case(1, 24, 1, "msm_bn254_2^24_skewed")
+    ntt_case(2, 24, 0, "ntt_bls12_381_2^24")
+    ntt_case(1, 26, 1, "ntt_bn254_2^26_coset")
+    return out
+
+
 def _tau(seed: int) -> bytes:
     import crypto_b200 as kb
     return kb.gen_scalars(CURVE, seed, 1)
@@ -373,6 +453,10 @@ def run_ours(args, ws, rank, local):
     msm_roof = {"achieved": msm_w / (ms / 1e3) / 1e12, "peak": peak_imad / 1e12, "unit": "TIMAD/s",
                 "frac": msm_w / (ms / 1e3) / peak_imad, "work": f"W_msm(2^{args.logn}) = {msm_w:.3e} IMAD"}
 
+    extra = None
+    if rank == 0 and not args.no_extra:
+        extra = bench_extra(args, SM_COUNT * IMAD_PER_CLK_SM * float(load_peaks().get("sm_max_mhz", 1965.0)) * 1e6)
+
     kzg_batched = kzg_served = None
     if rank == 0 and not args.no_kzg:
         kzg_batched = bench_batched_commits(args)
@@ -407,6 +491,7 @@ def run_ours(args, ws, rank, local):
             "stage_ms": stage,
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "configs": extra,
             "kzg_batched": kzg_batched,
             "kzg_served": kzg_served,
         }
@@ -423,6 +508,9 @@ def main():
     ap.add_argument("--ref-logn", type=int, default=17)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-kzg", action="store_true")
+    ap.add_argument("--no-extra", action="store_true")
+    ap.add_argument("--case", default="msm", choices=["msm", "ntt"],
+                    help="msm: the benchmark line; ntt: one Fr NTT size only (profiling)")
     ap.add_argument("--commits", type=int, default=512)
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[100.0, 400.0])
     ap.add_argument("--serve-requests", type=int, default=80)
@@ -430,6 +518,23 @@ def main():
     sys.path.insert(0, str(ROOT / "tests"))
     ws, rank, local = setup_dist()
     try:
+        if args.case == "ntt":
+            # a single Fr NTT size, forward + inverse (for profiling the pass kernel)
+            import torch
+            import crypto_b200 as kb
+            n = 1 << args.logn
+            x = kb.gen_scalars(CURVE, 5, n)
+            d = torch.frombuffer(bytearray(x), dtype=torch.uint8).cuda()
+            sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+            def fwd_inv():
+                assert kb.lib().kb200_ntt_device(CURVE, d.data_ptr(), n, 0, 0, 1, sp) == 0
+                assert kb.lib().kb200_ntt_device(CURVE, d.data_ptr(), n, 1, 0, 1, sp) == 0
+
+            ms = time_device(fwd_inv, args.steps, args.warmup)
+            assert d.cpu().numpy().tobytes() == x
+            print(json.dumps({"case": "ntt", "curve": "BLS12-381", "n": n, "ms_fwd_plus_inv": ms}))
+            return
         if args.impl == "reference":
             run_reference(args, ws, rank)
         else:

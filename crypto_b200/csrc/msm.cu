@@ -79,6 +79,23 @@ __global__ void k_list_big(const uint32_t* __restrict__ offsets, uint32_t B, uin
     }
 }
 
+// Group counts of fold level `level`, one per listed big bucket (zero past
+// the list's end); an exclusive scan of these flattens the level's work.
+__global__ void k_fold_counts(const uint32_t* __restrict__ offsets, uint32_t K, int FK, int level,
+                              const uint32_t* __restrict__ big_list, uint32_t big_cap,
+                              uint32_t* __restrict__ counts) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= big_cap) return;
+    uint32_t n = 0;
+    if (k < min(big_list[0], big_cap)) {
+        const uint32_t g = big_list[1 + k];
+        const uint32_t o = offsets[g], c = offsets[g + 1] - o;
+        uint32_t t0, np;
+        fold_sizes(o, c, K, FK, level, t0, np, n);
+    }
+    counts[k] = n;
+}
+
 // ---------------------------------------------------------------------------
 // Plans
 // ---------------------------------------------------------------------------
@@ -251,8 +268,8 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
     P.nchunks = (size_t)((L + (unsigned long long)K - 1) / (unsigned long long)K);
     // A bucket holds at most max_n entries, so spans at most max_n / K + 1
     // chunks; its chunk records fold in ceil(log_FK(span)) levels.  A big
-    // bucket spans more than K2 + 1 chunks, so at most nchunks / (K2 + 1)
-    // buckets can be big.
+    // bucket spans more than K2 + 1 chunks, so it owns at least K2 interior
+    // chunks outright: at most nchunks / K2 buckets can be big.
     const size_t max_span = (max_n + K - 1) / K + 1;
     int lv = 0;
     size_t span = 1;
@@ -261,7 +278,7 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         ++lv;
     }
     P.levels = max_span > (size_t)P.K2 + 1 ? lv : 0;
-    P.big_cap = P.nchunks / (size_t)(P.K2 + 1) + 1;
+    P.big_cap = P.nchunks / (size_t)P.K2 + 2;
 }
 
 MsmBatchPlan* msm_batch_plan_create(int curve, const MsmItem* items, size_t count,
@@ -302,7 +319,7 @@ class MsmEngine {
    public:
     int curve = 0;
     DevBuf table, keys, vals, counts, offsets, cursor, sorted, rec_first, rec_last, fold_buf,
-        buckets, blk_out, win_out, scan_tmp, queue;
+        buckets, blk_out, win_out, scan_tmp, queue, fold_counts, fold_prefix;
     std::map<std::tuple<size_t, bool, int, int>, MsmBatchPlan*> single_plans;
     cudaEvent_t ev[N_STAGE_EVENTS] = {};
     bool ev_ready = false, ev_recorded = false;
@@ -320,7 +337,8 @@ class MsmEngine {
         if (ev_ready)
             for (auto& e : ev) cudaEventDestroy(e);
         for (DevBuf* b : {&table, &keys, &vals, &counts, &offsets, &cursor, &sorted, &rec_first,
-                          &rec_last, &fold_buf, &buckets, &blk_out, &win_out, &scan_tmp, &queue})
+                          &rec_last, &fold_buf, &buckets, &blk_out, &win_out, &scan_tmp, &queue,
+                          &fold_counts, &fold_prefix})
             b->release();
     }
 };
@@ -375,7 +393,9 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
     e->buckets.reserve(std::max<size_t>(1, (size_t)P.B) * PW * 4, st);
     e->blk_out.reserve(std::max<size_t>(1, P.blks.size()) * 2 * PW * 4, st);
     e->win_out.reserve(std::max<size_t>(1, P.wins.size()) * PW * 4, st);
-    e->scan_tmp.reserve(scan_tmp_words((size_t)P.B + 1) * 4, st);
+    e->scan_tmp.reserve(scan_tmp_words(std::max<size_t>((size_t)P.B, P.big_cap) + 1) * 4, st);
+    e->fold_counts.reserve((P.big_cap + 1) * 4, st);
+    e->fold_prefix.reserve((P.big_cap + 1) * 4, st);
     e->queue.reserve((P.big_cap + 8) * 4, st);
 }
 
@@ -450,11 +470,19 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
         fa.K2 = P.K2;
         fa.FK = P.FK;
         fa.big_list = big_list;
+        fa.big_cap = (uint32_t)P.big_cap;
+        fa.prefix = e->fold_prefix.as<uint32_t>();
         fa.rec_first = e->rec_first.as<uint32_t>();
         uint32_t* in = e->rec_first.as<uint32_t>();
         uint32_t* out = e->fold_buf.as<uint32_t>();
         for (int l = 2; l <= P.levels + 1; ++l) {
-            K.fold(fa, l, in, out, (unsigned)sms * 4, st);
+            k_fold_counts<<<ceil_div_u(P.big_cap, 256), 256, 0, st>>>(
+                e->offsets.as<uint32_t>(), (uint32_t)P.K, P.FK, l, big_list, (uint32_t)P.big_cap,
+                e->fold_counts.as<uint32_t>());
+            KB_LAUNCH_CHECK();
+            exclusive_scan_u32(e->fold_counts.as<uint32_t>(), e->fold_prefix.as<uint32_t>(),
+                               P.big_cap, 0, e->scan_tmp.as<uint32_t>(), st);
+            K.fold(fa, l, in, out, (unsigned)sms * 8, st);
             std::swap(in, out);
         }
     }

@@ -65,6 +65,8 @@ struct FoldArgs {
     int K2;
     int FK;
     const uint32_t* big_list;
+    uint32_t big_cap;
+    const uint32_t* prefix;  // per level: exclusive prefix of group counts (big_cap + 1)
     uint32_t* rec_first;
 };
 
@@ -97,6 +99,17 @@ struct MsmLaunchers {
     int table_words;  // affine table row
     int wire_bytes;
 };
+
+// Items of fold level l for big bucket g: n_1 = t1 - t0 records, n_l =
+// ceil(n_{l-1} / FK); a level has n_l groups when n_{l-1} > 1, else none.
+__device__ __forceinline__ void fold_sizes(uint32_t o, uint32_t c, uint32_t K, int FK, int level,
+                                           uint32_t& t0, uint32_t& n_prev, uint32_t& n_cur) {
+    t0 = o / K;
+    const uint32_t t1 = (o + c - 1) / K;
+    n_prev = t1 - t0;
+    for (int l = 2; l < level; ++l) n_prev = (n_prev + FK - 1) / FK;
+    n_cur = n_prev <= 1 ? 0u : (n_prev + FK - 1) / FK;
+}
 
 const MsmLaunchers& msm_launchers(int curve);
 

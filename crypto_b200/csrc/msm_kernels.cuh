@@ -161,8 +161,11 @@ __device__ __forceinline__ uint32_t bucket_of(const uint32_t* offsets, uint32_t 
 // different) to rec_last[t], runs of buckets strictly inside the chunk
 // straight to buckets[].  Every lane does exactly K additions (the last
 // chunk fewer), whatever the bucket sizes.
+#ifndef KB_ACC_MIN_BLOCKS
+#define KB_ACC_MIN_BLOCKS 3
+#endif
 template <class C>
-__global__ void __launch_bounds__(128) k_accumulate(AccArgs a) {
+__global__ void __launch_bounds__(128, KB_ACC_MIN_BLOCKS) k_accumulate(AccArgs a) {
     using F = typename C::F;
     constexpr int PW = 4 * F::N;
     __shared__ uint32_t unit;
@@ -213,37 +216,41 @@ __global__ void __launch_bounds__(128) k_accumulate(AccArgs a) {
     }
 }
 
-// Fold level l >= 2 over the listed big buckets.  Bucket g covers chunks
-// t0..t1; its n_1 = t1 - t0 records rec_first[t0+1 .. t1] are summed FK at
-// a time per level (n_l = ceil(n_{l-1} / FK)); the level that reaches one
-// item writes the total to rec_first[t0 + 1].  The whole grid works on each
-// listed bucket in turn; with no big bucket the kernel exits at once.
+// Fold level l >= 2: the level's (big bucket, group) items are flattened by
+// the prefix of group counts and spread over the whole grid.  Group q of
+// bucket g sums FK consecutive items of its previous level (records
+// rec_first[t0+1 ..] at level 2); the level that reaches one group writes the
+// bucket's total to rec_first[t0 + 1].
 template <class C>
 __global__ void __launch_bounds__(128) k_fold(FoldArgs a, int level, const uint32_t* __restrict__ in,
                                               uint32_t* __restrict__ out) {
     using F = typename C::F;
     constexpr int PW = 4 * F::N;
-    const uint32_t nbig = a.big_list[0];
-    for (uint32_t k = 0; k < nbig; ++k) {
-        const uint32_t g = a.big_list[1 + k];
-        const uint32_t o = a.offsets[g], c = a.offsets[g + 1] - o;
-        const uint32_t t0 = o / a.K, t1 = (o + c - 1) / a.K;
-        uint32_t n_prev = t1 - t0;
-        for (int l = 2; l < level; ++l) n_prev = (n_prev + a.FK - 1) / a.FK;
-        if (n_prev <= 1) continue;
-        const uint32_t n_cur = (n_prev + a.FK - 1) / a.FK;
-        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cur;
-             i += gridDim.x * blockDim.x) {
-            const uint32_t lo = i * (uint32_t)a.FK, hi = min(lo + (uint32_t)a.FK, n_prev);
-            Xyzz<F> acc, x;
-            xyzz_load(acc, in + (size_t)(t0 + 1 + lo) * PW);
-            for (uint32_t j = lo + 1; j < hi; ++j) {
-                xyzz_load(x, in + (size_t)(t0 + 1 + j) * PW);
-                xyzz_add(acc, x);
-            }
-            uint32_t* dst = (n_cur == 1) ? a.rec_first : out;
-            xyzz_store(dst + (size_t)(t0 + 1 + i) * PW, acc);
+    const uint32_t total = a.prefix[a.big_cap];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += gridDim.x * blockDim.x) {
+        uint32_t lo_k = 0, hi_k = a.big_cap;  // largest k with prefix[k] <= i
+        while (hi_k - lo_k > 1) {
+            const uint32_t mid = (lo_k + hi_k) >> 1;
+            if (a.prefix[mid] <= i)
+                lo_k = mid;
+            else
+                hi_k = mid;
         }
+        const uint32_t g = a.big_list[1 + lo_k];
+        const uint32_t q = i - a.prefix[lo_k];
+        const uint32_t o = a.offsets[g], c = a.offsets[g + 1] - o;
+        uint32_t t0, n_prev, n_cur;
+        fold_sizes(o, c, a.K, a.FK, level, t0, n_prev, n_cur);
+        const uint32_t lo = q * (uint32_t)a.FK, hi = min(lo + (uint32_t)a.FK, n_prev);
+        Xyzz<F> acc, x;
+        xyzz_load(acc, in + (size_t)(t0 + 1 + lo) * PW);
+        for (uint32_t j = lo + 1; j < hi; ++j) {
+            xyzz_load(x, in + (size_t)(t0 + 1 + j) * PW);
+            xyzz_add(acc, x);
+        }
+        uint32_t* dst = (n_cur == 1) ? a.rec_first : out;
+        xyzz_store(dst + (size_t)(t0 + 1 + q) * PW, acc);
     }
 }
 

@@ -15,7 +15,7 @@ namespace kb200 {
 
 namespace {
 
-constexpr int NTT_THREADS = 256;
+constexpr int NTT_THREADS = 1024;
 constexpr int NTT_SMEM_ELTS = 4096;  // 128 KiB of 32-byte elements per block
 constexpr int TAB_SPLIT = 13;        // two-level tables: e = hi * 2^13 + lo
 

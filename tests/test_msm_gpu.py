@@ -152,3 +152,15 @@ def test_linearity_large(cuda_lib, curve):
     lo = kb().gpukit_multi_pippenger(curve, s[:32 * h], pts[:pb * h], h)
     hi = kb().gpukit_multi_pippenger(curve, s[32 * h:], pts[pb * h:], n - h)
     assert O.g1_add(curve, lo, hi) == a
+
+
+@pytest.mark.parametrize("curve,logn,bits", [(1, 20, 10), (2, 18, 8)])
+def test_many_big_buckets(cuda_lib, curve, logn, bits):
+    """Small scalars over many points: every bucket of window 0 holds
+    thousands of entries, so thousands of buckets take the fold path."""
+    n = 1 << logn
+    pts = rand_points(curve, n, seed=40 + logn)
+    rng = random.Random(logn)
+    scs = b"".join(rng.getrandbits(bits).to_bytes(32, "little") for _ in range(n))
+    want = O.ref_msm(curve, scs, pts, n, threads=16) if O.ref_available() else O.msm(curve, scs, pts, n)
+    assert kb().gpukit_multi_pippenger(curve, scs, pts, n) == want
