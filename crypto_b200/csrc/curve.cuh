@@ -14,17 +14,28 @@
 
 namespace kb200 {
 
+// Resident 128-thread blocks per SM requested for the bucket-accumulation
+// kernel (sets its register budget: 5 -> 96 registers, 6 -> 80).
+#ifndef KB_ACC_MIN_BLOCKS_BLS
+#define KB_ACC_MIN_BLOCKS_BLS 5
+#endif
+#ifndef KB_ACC_MIN_BLOCKS_BN
+#define KB_ACC_MIN_BLOCKS_BN 6
+#endif
+
 struct G1BLS {
     using F = FpBLS;
     static constexpr uint32_t B = 4;
     static constexpr int WIRE = 96;  // x || y, 48-byte big-endian each
     static constexpr int CURVE_ID = 2;
+    static constexpr int ACC_MIN_BLOCKS = KB_ACC_MIN_BLOCKS_BLS;
 };
 struct G1BN {
     using F = FpBN;
     static constexpr uint32_t B = 3;
     static constexpr int WIRE = 64;  // x || y, 32-byte big-endian each
     static constexpr int CURVE_ID = 1;
+    static constexpr int ACC_MIN_BLOCKS = KB_ACC_MIN_BLOCKS_BN;
 };
 
 template <class F>
@@ -245,6 +256,230 @@ KB_DEV void xyzz_store(uint32_t* w, const Xyzz<F>& p) {
     fe_store(w + F::N, p.Y);
     fe_store(w + 2 * F::N, p.ZZ);
     fe_store(w + 3 * F::N, p.ZZZ);
+}
+
+// An XYZZ point held in shared memory, word-major over a block of STRIDE
+// threads: coordinate f (0 = X, 1 = Y, 2 = ZZ, 3 = ZZZ), word k of this
+// thread at base[(f * N + k) * STRIDE].  Consecutive threads hit consecutive
+// banks.  An accumulator kept here rather than in registers leaves only the
+// temporaries of the formula in registers, which raises the resident warps
+// per SM of the latency-bound addition kernels.
+template <class F, int STRIDE>
+struct SmXyzz {
+    uint32_t* base;  // shared array + threadIdx.x
+    KB_DEV void get(int f, Fe<F>& r) const {
+#pragma unroll
+        for (int k = 0; k < F::N; ++k) r.v[k] = base[(f * F::N + k) * STRIDE];
+    }
+    KB_DEV void put(int f, const Fe<F>& r) const {
+#pragma unroll
+        for (int k = 0; k < F::N; ++k) base[(f * F::N + k) * STRIDE] = r.v[k];
+    }
+    KB_DEV bool is_inf() const {
+        uint32_t o = 0;
+#pragma unroll
+        for (int k = 0; k < F::N; ++k) o |= base[(2 * F::N + k) * STRIDE];
+        return o == 0;
+    }
+    KB_DEV void set_inf() const {
+#pragma unroll
+        for (int k = 0; k < 4 * F::N; ++k) base[k * STRIDE] = 0;
+    }
+    KB_DEV void to_global(uint32_t* w) const {
+#pragma unroll
+        for (int k = 0; k < 4 * F::N; ++k) w[k] = base[k * STRIDE];
+    }
+};
+
+// Read-only view of an XYZZ point stored as 4N consecutive words in global
+// memory, with the accessors of SmXyzz.
+template <class F>
+struct GXyzz {
+    const uint32_t* w;
+    KB_DEV void get(int f, Fe<F>& r) const { fe_load(r, w + f * F::N); }
+    KB_DEV bool is_inf() const {
+        uint32_t o = 0;
+#pragma unroll
+        for (int k = 0; k < F::N; ++k) o |= w[2 * F::N + k];
+        return o == 0;
+    }
+};
+
+template <class F, int S, class Q>
+KB_DEV void xyzz_copy(const SmXyzz<F, S>& p, const Q& q) {
+    Fe<F> t;
+#pragma unroll 1
+    for (int f = 0; f < 4; ++f) {
+        q.get(f, t);
+        p.put(f, t);
+    }
+}
+
+// dbl-2008-s-1 in place on a shared-memory point.
+template <class F, int S>
+KB_DEV void xyzz_dbl(const SmXyzz<F, S>& p) {
+    Fe<F> U, V, W, t;
+    p.get(1, t);
+    fe_dbl(U, t);
+    fe_sqr(V, U);
+    fe_mul(W, U, V);
+    p.get(2, t);
+    fe_mul(t, V, t);
+    p.put(2, t);                // ZZ3 = V*ZZ1
+    p.get(0, t);
+    fe_mul(U, t, V);            // U <- S = X1*V
+    p.get(3, t);
+    fe_mul(t, W, t);
+    p.put(3, t);                // ZZZ3 = W*ZZZ1
+    p.get(1, t);
+    fe_mul(W, W, t);            // W <- W*Y1
+    p.get(0, t);
+    fe_sqr(V, t);
+    fe_dbl(t, V);
+    fe_add(V, V, t);            // V <- M = 3 X1^2
+    fe_sqr(t, V);
+    fe_sub(t, t, U);
+    fe_sub(t, t, U);            // X3 = M^2 - 2S
+    p.put(0, t);
+    fe_sub(U, U, t);
+    fe_mul(U, V, U);
+    fe_sub(U, U, W);            // Y3 = M(S - X3) - W*Y1
+    p.put(1, U);
+}
+
+// add-2008-s on a shared-memory accumulator: p += q, q an SmXyzz or GXyzz
+// (either may be infinity; q must not alias p).
+template <class F, int S, class Q>
+KB_DEV void xyzz_add(const SmXyzz<F, S>& p, const Q& q) {
+    if (q.is_inf()) return;
+    if (p.is_inf()) {
+        xyzz_copy(p, q);
+        return;
+    }
+    Fe<F> U1, S1, P, R, t;
+    q.get(2, t);
+    p.get(0, U1);
+    fe_mul(U1, U1, t);          // U1 = X1*ZZ2
+    p.get(2, t);
+    q.get(0, P);
+    fe_mul(P, P, t);
+    fe_sub(P, P, U1);           // P = X2*ZZ1 - U1
+    q.get(3, t);
+    p.get(1, S1);
+    fe_mul(S1, S1, t);          // S1 = Y1*ZZZ2
+    p.get(3, t);
+    q.get(1, R);
+    fe_mul(R, R, t);
+    fe_sub(R, R, S1);           // R = Y2*ZZZ1 - S1
+    if (fe_is_zero(P)) {
+        if (fe_is_zero(R))
+            xyzz_dbl(p);
+        else
+            p.set_inf();
+        return;
+    }
+    fe_sqr(t, P);               // t = PP
+    fe_mul(U1, U1, t);          // U1 <- Q = U1*PP
+    fe_mul(P, P, t);            // P <- PPP
+    {
+        Fe<F> z;
+        p.get(2, z);
+        fe_mul(t, t, z);
+        q.get(2, z);
+        fe_mul(t, t, z);
+        p.put(2, t);            // ZZ3 = ZZ1*ZZ2*PP
+        p.get(3, t);
+        q.get(3, z);
+        fe_mul(t, t, z);
+        fe_mul(t, t, P);
+        p.put(3, t);            // ZZZ3 = ZZZ1*ZZZ2*PPP
+    }
+    fe_mul(S1, S1, P);          // S1*PPP
+    fe_sqr(t, R);
+    fe_sub(t, t, P);
+    fe_sub(t, t, U1);
+    fe_sub(t, t, U1);           // X3 = R^2 - PPP - 2Q
+    p.put(0, t);
+    fe_sub(U1, U1, t);
+    fe_mul(U1, R, U1);
+    fe_sub(U1, U1, S1);         // Y3 = R(Q - X3) - S1*PPP
+    p.put(1, U1);
+}
+
+// mdbl-2008-s-1 into a shared-memory point: p = 2 * (affine a).
+template <class F, int S>
+KB_DEV void xyzz_mdbl_sm(const SmXyzz<F, S>& p, const Affine<F>& a) {
+    Fe<F> U, V, W, t;
+    fe_dbl(U, a.y);
+    fe_sqr(V, U);
+    fe_mul(W, U, V);
+    p.put(3, W);                // ZZZ3 = W
+    fe_mul(U, a.x, V);          // U <- S = x*V
+    p.put(2, V);                // ZZ3 = V
+    fe_sqr(t, a.x);
+    fe_dbl(V, t);
+    fe_add(V, V, t);            // V <- M = 3x^2
+    fe_sqr(t, V);
+    fe_sub(t, t, U);
+    fe_sub(t, t, U);            // X3 = M^2 - 2S
+    p.put(0, t);
+    fe_sub(U, U, t);
+    fe_mul(U, V, U);            // M(S - X3)
+    fe_mul(W, W, a.y);
+    fe_sub(U, U, W);            // Y3 = M(S - X3) - W*y
+    p.put(1, U);
+}
+
+// madd-2008-s on a shared-memory accumulator: p += a, a finite affine
+// point.  At most five field elements are live in registers besides a.
+template <class F, int S>
+KB_DEV void xyzz_add_affine(const SmXyzz<F, S>& p, const Affine<F>& a) {
+    Fe<F> P, R, t;
+    p.get(2, t);
+    if (fe_is_zero(t)) {
+        p.put(0, a.x);
+        p.put(1, a.y);
+        fe_one(t);
+        p.put(2, t);
+        p.put(3, t);
+        return;
+    }
+    fe_mul(P, a.x, t);
+    p.get(0, t);
+    fe_sub(P, P, t);            // P = x2*ZZ1 - X1
+    p.get(3, t);
+    fe_mul(R, a.y, t);
+    p.get(1, t);
+    fe_sub(R, R, t);            // R = y2*ZZZ1 - Y1
+    if (fe_is_zero(P)) {
+        if (fe_is_zero(R))
+            xyzz_mdbl_sm(p, a);
+        else
+            p.set_inf();
+        return;
+    }
+    Fe<F> PP, Q;
+    fe_sqr(PP, P);              // PP
+    p.get(0, t);
+    fe_mul(Q, t, PP);           // Q = X1*PP
+    p.get(2, t);
+    fe_mul(t, t, PP);
+    p.put(2, t);                // ZZ3 = ZZ1*PP
+    fe_mul(PP, P, PP);          // PP <- PPP
+    p.get(3, t);
+    fe_mul(t, t, PP);
+    p.put(3, t);                // ZZZ3 = ZZZ1*PPP
+    p.get(1, t);
+    fe_mul(P, t, PP);           // P <- Y1*PPP
+    fe_sqr(t, R);
+    fe_sub(t, t, PP);
+    fe_sub(t, t, Q);
+    fe_sub(t, t, Q);            // X3 = R^2 - PPP - 2Q
+    p.put(0, t);
+    fe_sub(Q, Q, t);
+    fe_mul(Q, R, Q);
+    fe_sub(Q, Q, P);            // Y3 = R(Q - X3) - Y1*PPP
+    p.put(1, Q);
 }
 
 // Affine table entry (2N words) -> Affine<F>; the infinity flag is masked.

@@ -194,6 +194,25 @@ class MsmBatchPlan {
     }
 };
 
+// SM count of the current device and resident 128-thread accumulation blocks
+// per SM for a curve, both cached per device.
+static int device_sms() {
+    static int cache[64] = {0};
+    int dev = 0;
+    KB_CUDA(cudaGetDevice(&dev));
+    int& v = cache[dev & 63];
+    if (!v) KB_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+    return v;
+}
+static int acc_occupancy(int curve) {
+    static int cache[64][3] = {{0}};
+    int dev = 0;
+    KB_CUDA(cudaGetDevice(&dev));
+    int& v = cache[dev & 63][curve == 2 ? 2 : 1];
+    if (!v) v = std::max(1, msm_launchers(curve).accumulate_occupancy());
+    return v;
+}
+
 static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, size_t count,
                             const MsmOptions& opt) {
     P.curve = curve;
@@ -233,9 +252,9 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
     P.B = (uint32_t)B;
     P.total_scalars = tot_sc;
     // Reduction granularity: buckets per thread S (power of two) so that
-    // stage 1 fills about one wave of 148 SMs x 256 threads, and every window
-    // has at most RED_THREADS stage-1 blocks.
-    const size_t per_wave = (size_t)148 * RED_THREADS;
+    // stage 1 fills about one wave (two resident 256-thread blocks per SM),
+    // and every window has at most RED_THREADS stage-1 blocks.
+    const size_t per_wave = (size_t)2 * device_sms() * RED_THREADS;
     int log_S = 0;
     while (((size_t)1 << log_S) * per_wave < total_live && log_S < 6) ++log_S;
     for (size_t i = 0; i < count; ++i) {
@@ -250,6 +269,7 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
             wd.log_S = ls;
             wd.log_blk = 8 + ls;
             wd.nb = (wd.Mw + (1u << wd.log_blk) - 1) >> wd.log_blk;
+            wd.shift = d.c * w;
             wd.blk_base = (uint32_t)P.blks.size();
             for (uint32_t b = 0; b < wd.nb; ++b)
                 P.blks.push_back(BlkDesc{(uint32_t)P.wins.size(), b});
@@ -257,11 +277,13 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         }
     }
     // Chunk length: long chunks amortise the per-chunk records, but there must
-    // be enough chunks to keep every SM busy (~4 warps x 148 SMs x 32 lanes).
+    // be at least two chunks per resident accumulation thread.
     int K = opt.force_K;
     if (K <= 0) {
+        const unsigned long long resident =
+            (unsigned long long)device_sms() * acc_occupancy(curve) * 128;
         K = 64;
-        while (K > 4 && (unsigned long long)K * 148 * 4 * 32 * 2 > L) K >>= 1;
+        while (K > 4 && (unsigned long long)K * resident * 2 > L) K >>= 1;
     }
     P.K = K;
     P.K2 = 8;
@@ -447,17 +469,10 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
     acc.rec_last = e->rec_last.as<uint32_t>();
     acc.buckets = e->buckets.as<uint32_t>();
     acc.queue = e->queue.as<uint32_t>();
-    int sms = 148;
-    {
-        int dev = 0;
-        KB_CUDA(cudaGetDevice(&dev));
-        KB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    }
     if (P.L > 0) {
-        static int occ_cache[3] = {0, 0, 0};
-        if (!occ_cache[e->curve]) occ_cache[e->curve] = std::max(1, K.accumulate_occupancy());
         const size_t units = (P.nchunks + 127) / 128;
-        const unsigned grid = (unsigned)std::min<size_t>(units, (size_t)sms * occ_cache[e->curve]);
+        const unsigned grid =
+            (unsigned)std::min<size_t>(units, (size_t)device_sms() * acc_occupancy(e->curve));
         K.accumulate(acc, std::max(1u, grid), st);
     }
     e->mark(4, st);
@@ -482,7 +497,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
             KB_LAUNCH_CHECK();
             exclusive_scan_u32(e->fold_counts.as<uint32_t>(), e->fold_prefix.as<uint32_t>(),
                                P.big_cap, 0, e->scan_tmp.as<uint32_t>(), st);
-            K.fold(fa, l, in, out, (unsigned)sms * 8, st);
+            K.fold(fa, l, in, out, (unsigned)device_sms() * 8, st);
             std::swap(in, out);
         }
     }

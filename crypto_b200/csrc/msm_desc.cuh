@@ -31,6 +31,7 @@ struct WinDesc {
     uint32_t blk_base;     // first stage-1 block of the window
     uint32_t nb;           // stage-1 blocks (<= RED_THREADS)
     uint32_t log_blk;      // log2(RED_THREADS << log_S)
+    uint32_t shift;        // c * w: the window's weight is 2^shift
 };
 
 struct BlkDesc {

@@ -161,14 +161,16 @@ __device__ __forceinline__ uint32_t bucket_of(const uint32_t* offsets, uint32_t 
 // different) to rec_last[t], runs of buckets strictly inside the chunk
 // straight to buckets[].  Every lane does exactly K additions (the last
 // chunk fewer), whatever the bucket sizes.
-#ifndef KB_ACC_MIN_BLOCKS
-#define KB_ACC_MIN_BLOCKS 3
-#endif
+// The running sum lives in shared memory (SmXyzz), so registers hold only
+// the formula's temporaries and more warps stay resident to hide the
+// latency of the dependent multiply chains.
 template <class C>
-__global__ void __launch_bounds__(128, KB_ACC_MIN_BLOCKS) k_accumulate(AccArgs a) {
+__global__ void __launch_bounds__(128, C::ACC_MIN_BLOCKS) k_accumulate(AccArgs a) {
     using F = typename C::F;
     constexpr int PW = 4 * F::N;
     __shared__ uint32_t unit;
+    __shared__ uint32_t s_acc[4 * F::N * 128];
+    const SmXyzz<F, 128> acc{s_acc + threadIdx.x};
     // Only non-zero digits were sorted: the list length is offsets[B].
     const uint32_t L = a.offsets[a.B];
     const uint32_t nchunks = (L + a.K - 1) / a.K;
@@ -185,16 +187,15 @@ __global__ void __launch_bounds__(128, KB_ACC_MIN_BLOCKS) k_accumulate(AccArgs a
             uint32_t b = bucket_of(a.offsets, a.B, e0);
             uint32_t bend = a.offsets[b + 1];
             uint32_t run0 = e0;
-            Xyzz<F> acc;
-            xyzz_set_inf(acc);
+            acc.set_inf();
             uint32_t v = a.sorted[e0];
             for (uint32_t e = e0; e < e1; ++e) {
                 if (e == bend) {
                     // flush the finished run [run0, e) of bucket b
                     uint32_t* dst = (run0 == e0) ? a.rec_first + (size_t)t * PW
                                                  : a.buckets + (size_t)b * PW;
-                    xyzz_store(dst, acc);
-                    xyzz_set_inf(acc);
+                    acc.to_global(dst);
+                    acc.set_inf();
                     while (a.offsets[b + 1] <= e) ++b;
                     bend = a.offsets[b + 1];
                     run0 = e;
@@ -211,7 +212,7 @@ __global__ void __launch_bounds__(128, KB_ACC_MIN_BLOCKS) k_accumulate(AccArgs a
                 v = vn;
             }
             uint32_t* dst = (run0 == e0) ? a.rec_first + (size_t)t * PW : a.rec_last + (size_t)t * PW;
-            xyzz_store(dst, acc);
+            acc.to_global(dst);
         }
     }
 }
@@ -264,7 +265,7 @@ __device__ __forceinline__ void xyzz_dbl_n(Xyzz<F>& p, int k) {
 // addition call site, so lanes whose buckets are split differently stay
 // converged instead of serialising through separate inlined copies.
 template <class F>
-__device__ __forceinline__ void bucket_add(Xyzz<F>& R, const RedArgs& a, uint32_t g) {
+__device__ __forceinline__ void bucket_add(const SmXyzz<F, RED_THREADS>& R, const RedArgs& a, uint32_t g) {
     constexpr int PW = 4 * F::N;
     const uint32_t o = a.offsets[g], c = a.offsets[g + 1] - o;
     if (c == 0) return;
@@ -284,9 +285,7 @@ __device__ __forceinline__ void bucket_add(Xyzz<F>& R, const RedArgs& a, uint32_
     }
     for (uint32_t k = 0; k < npieces; ++k) {
         const uint32_t* src = (k == 0) ? first : a.rec_first + (size_t)(t0 + k) * PW;
-        Xyzz<F> x;
-        xyzz_load(x, src);
-        xyzz_add(R, x);
+        xyzz_add(R, GXyzz<F>{src});
     }
 }
 
@@ -352,53 +351,68 @@ __device__ __forceinline__ void smem_tree_sum(uint32_t* sm) {
 // and T_t = sum_j j B (j relative), the block's
 //   Fb = sum_k k B_k = sum_t T_t + S * sum_{t>=1} Y_t,   Sb = Y_0,
 // where Y_t = sum_{t'>=t} R_t' (suffix scan in shared memory).
+// Every point lives in shared memory (SmXyzz): sA holds R_t, sB holds T_t,
+// and the two double as the ping-pong buffers of the scan once T is summed;
+// sX holds two stashed points (sum of T, Y_0).  Registers carry only the
+// addition formula's temporaries, so two 256-thread blocks fit per SM.
 template <class C>
-__global__ void __launch_bounds__(RED_THREADS) k_reduce_blocks(RedArgs a) {
+__global__ void __launch_bounds__(RED_THREADS, 2) k_reduce_blocks(RedArgs a) {
     using F = typename C::F;
     constexpr int PW = 4 * F::N;
+    using SP = SmXyzz<F, RED_THREADS>;
+    using S1 = SmXyzz<F, 1>;
     extern __shared__ __align__(16) uint32_t smr[];
-    uint32_t* sA = smr;                       // R_t -> suffix sums -> tree
-    uint32_t* sB = smr + RED_THREADS * PW;    // T_t (kept here, not in registers)
+    uint32_t* sA = smr;
+    uint32_t* sB = smr + RED_THREADS * PW;
+    uint32_t* sX = smr + 2 * RED_THREADS * PW;
     const BlkDesc bd = a.blks[blockIdx.x];
     const WinDesc wd = a.wins[bd.win];
     const uint32_t S = 1u << wd.log_S;
     const uint32_t first = bd.b * (RED_THREADS << wd.log_S) + threadIdx.x * S;
     const int me = threadIdx.x;
     {
-        Xyzz<F> R;
-        xyzz_set_inf(R);
-        sm_store(sB, me, R);
+        const SP R{sA + me}, T{sB + me};
+        R.set_inf();
+        T.set_inf();
         for (int j = (int)S - 1; j >= 0; --j) {
             if (first + (uint32_t)j < wd.Mw) bucket_add(R, a, wd.bucket_base + first + (uint32_t)j);
-            if (j > 0) {
-                Xyzz<F> T;
-                sm_load(T, sB, me);
-                xyzz_add(T, R);
-                sm_store(sB, me, T);
-            }
+            if (j > 0) xyzz_add(T, R);
         }
-        sm_store(sA, me, R);
     }
     __syncthreads();
-    smem_suffix_scan<F>(sA);
-    Xyzz<F> Y0;
-    if (threadIdx.x == 0) {
-        sm_load(Y0, sA, 0);
-        Xyzz<F> inf;
-        xyzz_set_inf(inf);
-        sm_store(sA, 0, inf);  // the tree below sums Y_t for t >= 1
+    // sum of T_t -> stash 0
+    for (int d = RED_THREADS >> 1; d >= 1; d >>= 1) {
+        if (me < d) xyzz_add(SP{sB + me}, SP{sB + me + d});
+        __syncthreads();
+    }
+    if (me == 0) xyzz_copy(S1{sX}, SP{sB});
+    // suffix scan of R_t, ping-pong between sA and sB (8 steps: ends in sA)
+    uint32_t* src = sA;
+    uint32_t* dst = sB;
+    for (int d = 1; d < RED_THREADS; d <<= 1) {
+        const SP o{dst + me};
+        xyzz_copy(o, SP{src + me});
+        if (me + d < RED_THREADS) xyzz_add(o, SP{src + me + d});
+        __syncthreads();
+        uint32_t* tmp = src;
+        src = dst;
+        dst = tmp;
+    }
+    if (me == 0) {
+        xyzz_copy(S1{sX + PW}, SP{src});  // Y_0
+        SP{src}.set_inf();                // the tree below sums Y_t for t >= 1
     }
     __syncthreads();
-    smem_tree_sum<F>(sA);
-    smem_tree_sum<F>(sB);
-    if (threadIdx.x == 0) {
-        Xyzz<F> Fb, t;
-        sm_load(Fb, sA, 0);
-        xyzz_dbl_n(Fb, (int)wd.log_S);
-        sm_load(t, sB, 0);
-        xyzz_add(Fb, t);
-        xyzz_store(a.blk_out + ((size_t)blockIdx.x * 2) * PW, Fb);
-        xyzz_store(a.blk_out + ((size_t)blockIdx.x * 2 + 1) * PW, Y0);
+    for (int d = RED_THREADS >> 1; d >= 1; d >>= 1) {
+        if (me < d) xyzz_add(SP{src + me}, SP{src + me + d});
+        __syncthreads();
+    }
+    if (me == 0) {
+        const SP Fb{src};
+        for (uint32_t k = 0; k < wd.log_S; ++k) xyzz_dbl(Fb);
+        xyzz_add(Fb, S1{sX});
+        Fb.to_global(a.blk_out + ((size_t)blockIdx.x * 2) * PW);
+        S1{sX + PW}.to_global(a.blk_out + ((size_t)blockIdx.x * 2 + 1) * PW);
     }
 }
 
@@ -444,12 +458,16 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_windows(RedArgs a) {
         sm_load(u, sB, 0);
         xyzz_add(V, u);
         xyzz_add(V, Y0);
+        // Weight the window by 2^(c*w) here, one doubling chain per window
+        // running in parallel, instead of a Horner chain over all windows
+        // (c*(W-1) sequential doublings) in the combine.
+        for (uint32_t k = 0; k < wd.shift; ++k) xyzz_dbl_inl(V);
         xyzz_store(a.win_out + (size_t)blockIdx.x * PW, V);
     }
 }
 
-// Horner over each item's windows, then affine + wire (+ compressed for
-// BLS12-381).  One thread per item.
+// Sum of each item's (already weighted) windows, then affine + wire
+// (+ compressed for BLS12-381).  One thread per item.
 template <class C>
 __global__ void k_combine(const ItemDesc* __restrict__ items, uint32_t n_items,
                           const uint32_t* __restrict__ wins, uint8_t* __restrict__ out_wire,
@@ -465,9 +483,9 @@ __global__ void k_combine(const ItemDesc* __restrict__ items, uint32_t n_items,
     if (it.n == 0) {
         xyzz_set_inf(acc);
     } else {
+        // windows arrive already weighted by 2^(c*w): a plain sum
         xyzz_load(acc, wins + (size_t)(it.win_base + it.W - 1) * PW);
         for (int w = (int)it.W - 2; w >= 0; --w) {
-            for (uint32_t k = 0; k < it.c; ++k) xyzz_dbl_inl(acc);
             xyzz_load(t, wins + (size_t)(it.win_base + (uint32_t)w) * PW);
             xyzz_add(acc, t);
         }
@@ -540,10 +558,11 @@ struct MsmLaunchImpl {
         KB_LAUNCH_CHECK();
     }
     static size_t red_smem() { return (size_t)2 * RED_THREADS * 4 * F::N * 4; }
+    static size_t red_blocks_smem() { return red_smem() + (size_t)2 * 4 * F::N * 4; }
     static void reduce_blocks(const RedArgs& a, unsigned nblk, cudaStream_t st) {
         if (!nblk) return;
-        set_smem_attr((const void*)k_reduce_blocks<C>, red_smem());
-        k_reduce_blocks<C><<<nblk, RED_THREADS, red_smem(), st>>>(a);
+        set_smem_attr((const void*)k_reduce_blocks<C>, red_blocks_smem());
+        k_reduce_blocks<C><<<nblk, RED_THREADS, red_blocks_smem(), st>>>(a);
         KB_LAUNCH_CHECK();
     }
     static void reduce_windows(const RedArgs& a, unsigned nwin, cudaStream_t st) {
