@@ -445,7 +445,7 @@ def run_ours(args, ws, rank, local):
         ach = acc_imad / (acc_ms / 1e3)
         roofline = {"bound": "int", "kernel": "k_accumulate", "achieved": ach / 1e12,
                     "peak": peak_imad / 1e12, "unit": "TIMAD/s", "frac": ach / peak_imad,
-                    "traffic": None,
+                    "traffic": accumulate_traffic(entries),
                     "peak_source": f"derived: {SM_COUNT} SMs x {IMAD_PER_CLK_SM} IMAD/clk x "
                                    f"{sm_mhz:.0f} MHz (MEASURED_PEAKS sm_max_mhz)",
                     "work_per_launch": f"{entries:.3e} bucket additions x 6 x {mont_imad(N_LIMBS)} IMAD"}
@@ -496,6 +496,17 @@ def run_ours(args, ws, rank, local):
             "kzg_served": kzg_served,
         }
         print(json.dumps(line), flush=True)
+
+
+def accumulate_traffic(entries):
+    """DRAM bytes of one k_accumulate launch: the ncu capture committed under
+    profiles/ (dram__bytes_read.sum + dram__bytes_write.sum at a size whose
+    affine table exceeds L2), scaled by the number of sorted entries."""
+    p = ROOT / "profiles" / "k_accumulate_dram.json"
+    if CURVE != 2 or not p.exists():
+        return None
+    d = json.loads(p.read_text())["bls12_381"]
+    return (d["dram_read"] + d["dram_write"]) * entries / d["entries"]
 
 
 def main():
