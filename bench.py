@@ -199,7 +199,8 @@ def time_device(fn, steps: int, warmup: int) -> float:
 def bench_extra(args, peak_imad: float) -> dict:
     """The other single-transform configurations: BLS12-381 MSM 2^20, BN254 MSM
     2^24 (uniform and skewed scalars), BLS12-381 Fr NTT 2^24 forward + inverse,
-    BN254 coset NTT 2^26 forward + inverse.  Device-resident inputs."""
+    BN254 coset NTT 2^26 forward + inverse, word-prime NTT 2^20 (Goldilocks and
+    Cyclone-FFT primes).  Device-resident inputs."""
     import torch
     import crypto_b200 as kb
     L = kb.lib()
@@ -247,11 +248,56 @@ def bench_extra(args, peak_imad: float) -> dict:
         del d
         torch.cuda.empty_cache()
 
+    def word_ntt_case(q, g, logn, label):
+        """ntt_forward on the six-step path (2^16 < n <= 2^20): device time
+        of forward + inverse on resident words, the host-buffer C-ABI call,
+        and the reference's own CPU body on the same input."""
+        import numpy as np
+        n = 1 << logn
+        root = pow(g, (q - 1) // (2 * n), q)
+        root_inv = pow(root, q - 2, q)
+        x = np.random.Generator(np.random.PCG64(logn)).bit_generator.random_raw(n).astype(np.uint64) % np.uint64(q)
+        d = torch.from_numpy(x.view(np.int64).copy()).cuda()
+
+        def fwd_inv():
+            assert L.kb200_word_ntt_device(d.data_ptr(), None, n, q, root, 0, sp) == 0
+            assert L.kb200_word_ntt_device(d.data_ptr(), None, n, q, root_inv, 1, sp) == 0
+
+        ms = time_device(fwd_inv, 3, 5)
+        assert np.array_equal(d.cpu().numpy().view(np.uint64), x), "word NTT round trip changed the data"
+        h = x.copy()
+        assert L.ntt_forward(h.ctypes.data, n, q, root) == 0
+        reps = 5
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            h[:] = x
+            assert L.ntt_forward(h.ctypes.data, n, q, root) == 0
+        e2e_ms = (time.perf_counter() - t0) * 1e3 / reps
+        rec = {"n": n, "q": q, "ms_fwd_plus_inv_device": ms, "e2e_ms_forward": e2e_ms,
+               "api": "ntt_forward (host words, copies included)"}
+        ref = ROOT / "oracle" / "_ref" / "libref_ntt.so"
+        if ref.exists():
+            R = ctypes.CDLL(str(ref))
+            R.ntt_forward.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint64]
+            g_ = x.copy()
+            R.ntt_forward(g_.ctypes.data, n, q, root)  # builds its cached context
+            g_[:] = x
+            t0 = time.perf_counter()
+            R.ntt_forward(g_.ctypes.data, n, q, root)
+            rec["reference_cpu_ms_forward"] = (time.perf_counter() - t0) * 1e3
+            rec["reference_cpu"] = "ntt_forward of the reference (ntt_large.cpp), 1 core"
+            assert np.array_equal(g_, h), "GPU and reference outputs differ"
+        out[label] = rec
+        del d
+        torch.cuda.empty_cache()
+
     msm_case(2, 20, 0, "msm_bls12_381_2^20")
     msm_case(1, 24, 0, "msm_bn254_2^24_uniform")
     msm_case(1, 24, 1, "msm_bn254_2^24_skewed")
     ntt_case(2, 24, 0, "ntt_bls12_381_2^24")
     ntt_case(1, 26, 1, "ntt_bn254_2^26_coset")
+    word_ntt_case(0xFFFFFFFF00000001, 7, 20, "word_ntt_goldilocks_2^20")
+    word_ntt_case(998244353, 3, 20, "word_ntt_cyclone_2^20")
     return out
 
 

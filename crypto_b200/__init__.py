@@ -48,6 +48,9 @@ def lib() -> ctypes.CDLL:
         sigs = {
             "gpukit_multi_pippenger": (c.c_int, [c.c_uint32, u8p, u8p, sz, vp]),
             "gpukit_multi_pippenger_cuda": (c.c_int, [c.c_uint32, u8p, u8p, sz, vp]),
+            "ntt_forward": (c.c_int, [vp, sz, c.c_uint64, c.c_uint64]),
+            "ntt_inverse": (c.c_int, [vp, sz, c.c_uint64, c.c_uint64]),
+            "kb200_word_ntt_device": (c.c_int, [vp, vp, sz, c.c_uint64, c.c_uint64, c.c_int, vp]),
             "ntt_fr_forward": (c.c_int, [c.c_int, vp, sz, c.c_int]),
             "ntt_fr_inverse": (c.c_int, [c.c_int, vp, sz, c.c_int]),
             "ntt_fr_transform_noalloc": (c.c_int, [c.c_int, vp, sz, c.c_int, c.c_int]),
@@ -117,6 +120,23 @@ def msm_rc(curve: int, scalars, points, n: int, out) -> int:
 
 
 # ---- NTT --------------------------------------------------------------------
+
+def word_ntt_rc(words, n: int, modulus: int, root: int, inverse: bool = False) -> int:
+    """ntt_forward / ntt_inverse in place on a writable buffer of uint64
+    words (a numpy array or ctypes buffer); returns the status code."""
+    ptr = words.ctypes.data if hasattr(words, "ctypes") else ctypes.addressof(words)
+    fn = lib().ntt_inverse if inverse else lib().ntt_forward
+    return fn(ptr, n, modulus, root)
+
+
+def word_ntt(words, modulus: int, root: int, inverse: bool = False):
+    """Word-prime NTT of a uint64 numpy array (returns a transformed copy)."""
+    import numpy as np
+    a = np.ascontiguousarray(np.array(words, dtype=np.uint64))
+    _check("ntt_inverse" if inverse else "ntt_forward",
+           word_ntt_rc(a, len(a), modulus, root, inverse))
+    return a
+
 
 def ntt_fr(curve: int, data: bytes, inverse: bool = False, coset: bool = False) -> bytes:
     n = len(data) // 32

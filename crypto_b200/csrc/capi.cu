@@ -8,6 +8,7 @@
 #include "msm.cuh"
 #include "ntt.cuh"
 #include "runtime.cuh"
+#include "wntt.cuh"
 
 #include <atomic>
 #include <cstring>
@@ -37,7 +38,8 @@ struct DeviceCtx {
     NttEngine* ntt[3] = {nullptr, nullptr, nullptr};
     FixedBase* fb[3] = {nullptr, nullptr, nullptr};
     CommitBatcher* batcher = nullptr;
-    DevBuf d_a, d_b, d_out, d_srs, d_tmp;
+    WordNttCache* wntt = nullptr;
+    DevBuf d_a, d_b, d_out, d_srs, d_tmp, d_w, d_ws;
     HostBuf h_a, h_b, h_out;
     size_t srs_n = 0;
 
@@ -52,6 +54,10 @@ struct DeviceCtx {
     FixedBase* fb_for(int curve) {
         if (!fb[curve]) fb[curve] = fixed_base_create(curve, stream);
         return fb[curve];
+    }
+    WordNttCache* wntt_get() {
+        if (!wntt) wntt = word_ntt_cache_create();
+        return wntt;
     }
     CommitBatcher* batcher_get() {
         if (!batcher) batcher = commit_batcher_create();
@@ -169,6 +175,38 @@ static int ntt_host(int curve, uint8_t* data, size_t n, int inverse, int coset) 
                        KB_CUDA(cudaMemcpyAsync(c->d_a.ptr, data, n * 32, cudaMemcpyHostToDevice, st));
                        ntt_run(c->ntt_for(curve), c->d_a.as<uint32_t>(), n, inverse, coset, 1, st);
                        KB_CUDA(cudaMemcpyAsync(data, c->d_a.ptr, n * 32, cudaMemcpyDeviceToHost, st));
+                       KB_CUDA(cudaStreamSynchronize(st));
+                       return KB200_CRYPTO_OK;
+                   });
+}
+
+// ---- word-prime NTT -----------------------------------------------------------
+
+// ntt_forward / ntt_inverse (ntt/c-abi/c_ntt.cpp:81-179): argument checks in
+// the reference's order, then the transform on the device.  Invalid
+// arguments return CRYPTO_ERR_INPUT before any data moves.
+static bool word_ntt_args_ok(const uint64_t* coeffs, size_t n, uint64_t modulus) {
+    if (!coeffs || !is_pow2(n)) return false;
+    if (n <= ((size_t)1 << 16)) return modulus != 0;
+    return n <= ((size_t)1 << 20) && modulus != 0;
+}
+
+static int word_ntt_host(uint64_t* coeffs, size_t n, uint64_t modulus, uint64_t root, bool inverse) {
+    if (!word_ntt_args_ok(coeffs, n, modulus)) return KB200_CRYPTO_ERR_INPUT;
+    if (n == 1) return KB200_CRYPTO_OK;
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_INPUT, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       cudaStream_t st = c->stream;
+                       c->d_w.reserve(n * 8, st);
+                       c->d_ws.reserve(n * 8, st);
+                       KB_CUDA(cudaMemcpyAsync(c->d_w.ptr, coeffs, n * 8, cudaMemcpyHostToDevice, st));
+                       const int rc = word_ntt_device(c->wntt_get(), c->d_w.as<uint64_t>(),
+                                                      c->d_ws.as<uint64_t>(), n, modulus, root,
+                                                      inverse, st);
+                       if (rc != 0) return KB200_CRYPTO_ERR_INPUT;
+                       KB_CUDA(cudaMemcpyAsync(coeffs, c->d_w.ptr, n * 8, cudaMemcpyDeviceToHost, st));
                        KB_CUDA(cudaStreamSynchronize(st));
                        return KB200_CRYPTO_OK;
                    });
@@ -335,6 +373,30 @@ int kb200_msm_device(uint32_t curve, const void* d_scalars, const void* d_points
                                     (const uint8_t*)d_points, n, (uint8_t*)d_result, nullptr,
                                     (cudaStream_t)stream, opt);
                        return KB200_GPUKIT_OK;
+                   });
+}
+
+int ntt_forward(uint64_t* coeffs, size_t n, uint64_t modulus, uint64_t root) {
+    return word_ntt_host(coeffs, n, modulus, root, false);
+}
+
+int ntt_inverse(uint64_t* coeffs, size_t n, uint64_t modulus, uint64_t root_inv) {
+    return word_ntt_host(coeffs, n, modulus, root_inv, true);
+}
+
+int kb200_word_ntt_device(void* d_coeffs, void* d_scratch, size_t n, uint64_t modulus,
+                          uint64_t root, int inverse, void* stream) {
+    if (!word_ntt_args_ok((const uint64_t*)d_coeffs, n, modulus)) return KB200_CRYPTO_ERR_INPUT;
+    if (n > ((size_t)1 << 11) && n <= ((size_t)1 << 16) && !d_scratch) return KB200_CRYPTO_ERR_INPUT;
+    if (n == 1) return KB200_CRYPTO_OK;
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_INPUT, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       const int rc = word_ntt_device(c->wntt_get(), (uint64_t*)d_coeffs,
+                                                      (uint64_t*)d_scratch, n, modulus, root,
+                                                      inverse != 0, (cudaStream_t)stream);
+                       return rc == 0 ? KB200_CRYPTO_OK : KB200_CRYPTO_ERR_INPUT;
                    });
 }
 

@@ -69,6 +69,30 @@ int gpukit_multi_pippenger(uint32_t curve, const uint8_t* scalars, const uint8_t
 int gpukit_multi_pippenger_cuda(uint32_t curve, const uint8_t* scalars,
                                 const uint8_t* points, size_t n, uint8_t* result);
 
+/* ---- Word-prime NTT (replaces ntt_forward/ntt_inverse, crypto.h:368-369,
+ * bodies ntt/c-abi/c_ntt.cpp:81-179) --------------------------------------- */
+
+/* In-place transform of n 64-bit words mod `modulus`, with the reference's
+ * dispatch and results:
+ *   n <= 2^16   : natural order in and out.  modulus 998244353 with root
+ *                 629671588 (its 2^16-th root; for the inverse also its
+ *                 inverse) selects the reference's Montgomery path with
+ *                 w = root^(2^16/n); any other pair the generic path with
+ *                 `root` as the n-th root (`root_inv` used as given).
+ *   2^16 < n <= 2^20 : six-step; `root` is a 2n-th root, the transform root
+ *                 is root^2, and the forward output (= inverse input) is in
+ *                 the transposed N2 x N1 layout: word k1*N2 + k2 holds
+ *                 X[k1 + N1*k2], N1 = 2^floor(log2(n)/2), N2 = n/N1.
+ * The inverse includes the 1/n scaling.  Results match the reference for
+ * every input word, reduced or not (so, like the reference, the n <= 2^16
+ * generic path does not round-trip for moduli above 2^63: its addition has
+ * no overflow check).  Returns CRYPTO_OK, or CRYPTO_ERR_INPUT for a null
+ * pointer, n not a power of two, n > 2^20 or modulus 0 (the reference's
+ * 2^64 sentinel, which it rejects for every n > 1); CRYPTO_ERR_BACKEND
+ * without a usable GPU. */
+int ntt_forward(uint64_t* coeffs, size_t n, uint64_t modulus, uint64_t root);
+int ntt_inverse(uint64_t* coeffs, size_t n, uint64_t modulus, uint64_t root_inv);
+
 /* ---- Fr NTT (new; same style as ntt_forward/ntt_inverse, crypto.h:368-369) */
 
 /* In-place transform of n canonical Fr elements (32 B LE each), natural
@@ -149,6 +173,10 @@ int ntt_fr_transform_noalloc(int curve, uint8_t* coeffs32le, size_t n, int inver
  * synchronised.  Calls sharing a device must not overlap across streams. */
 int kb200_msm_device(uint32_t curve, const void* d_scalars, const void* d_points, size_t n,
                      void* d_result, void* stream);
+/* ntt_forward (inverse = 0) / ntt_inverse (inverse = 1) on device words;
+ * d_scratch (n words) is needed for 2^11 < n <= 2^16. */
+int kb200_word_ntt_device(void* d_coeffs, void* d_scratch, size_t n, uint64_t modulus,
+                          uint64_t root, int inverse, void* stream);
 int kb200_ntt_device(int curve, void* d_data, size_t n, int inverse, int coset, size_t batch,
                      void* stream);
 /* d_out_points[i] = d_scalars[i] * G1 (wire encoding), fixed-base windows. */

@@ -90,6 +90,15 @@ int orc_kzg_commit(const uint8_t* evals, size_t n, const uint8_t* srs,
 /* Fr helpers: powers tau^0..tau^(n-1) (canonical 32 B LE), and a*b mod r. */
 int orc_fr_powers(uint32_t curve, const uint8_t* tau, size_t n, uint8_t* out);
 
+/* Word-prime NTT with the contract of the reference's ntt_forward /
+ * ntt_inverse (ntt/c-abi/c_ntt.cpp:81-179): in place on n uint64 words;
+ * n <= 2^16 natural order (Cyclone prime 998244353 with its pinned root on
+ * the Montgomery path, anything else on the generic path, root = n-th root);
+ * 2^16 < n <= 2^20 six-step with output in the transposed N2 x N1 layout,
+ * root = 2n-th root.  Returns 0 or -1 (CRYPTO_ERR_INPUT).  word_ntt.c. */
+int orc_word_ntt_forward(uint64_t* a, size_t n, uint64_t q, uint64_t root);
+int orc_word_ntt_inverse(uint64_t* a, size_t n, uint64_t q, uint64_t root_inv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -3,6 +3,8 @@
   orc  -> oracle/_build/liboracle.so   (C restatement of the reference path)
   ref  -> oracle/_ref/libref_msm.so    (the reference's own CPU MSM, built
                                         unmodified from its sources)
+  ref_ntt -> oracle/_ref/libref_ntt.so (the reference's word-prime NTT and its
+                                        C-ABI shim, built unmodified)
 """
 from __future__ import annotations
 
@@ -13,9 +15,11 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parents[1]
 ORC_PATH = ROOT / "oracle" / "_build" / "liboracle.so"
 REF_PATH = ROOT / "oracle" / "_ref" / "libref_msm.so"
+REF_NTT_PATH = ROOT / "oracle" / "_ref" / "libref_ntt.so"
 
 _orc = None
 _ref = None
+_ref_ntt = None
 
 
 def orc() -> ctypes.CDLL:
@@ -41,6 +45,8 @@ def orc() -> ctypes.CDLL:
             "orc_fr_powers": [ctypes.c_uint32, ctypes.c_char_p, sz, ctypes.c_void_p],
             "orc_field_mul": [ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_void_p],
             "orc_field_inv": [ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p],
+            "orc_word_ntt_forward": [ctypes.c_void_p, sz, ctypes.c_uint64, ctypes.c_uint64],
+            "orc_word_ntt_inverse": [ctypes.c_void_p, sz, ctypes.c_uint64, ctypes.c_uint64],
         }.items():
             f = getattr(L, name)
             f.restype = ctypes.c_int
@@ -147,6 +153,34 @@ def fr_powers(curve: int, tau: bytes, n: int) -> bytes:
     out = ctypes.create_string_buffer(32 * n)
     assert orc().orc_fr_powers(curve, tau, n, out) == 0
     return out.raw
+
+
+def word_ntt(words, q: int, root: int, inverse: bool = False):
+    """Oracle word-prime NTT (ntt_forward / ntt_inverse contract) of a uint64
+    numpy array; returns (status, transformed copy)."""
+    import numpy as np
+    a = np.array(words, dtype=np.uint64)
+    f = orc().orc_word_ntt_inverse if inverse else orc().orc_word_ntt_forward
+    return f(a.ctypes.data, len(a), q, root), a
+
+
+def ref_ntt_available() -> bool:
+    return REF_NTT_PATH.exists()
+
+
+def ref_word_ntt(a, n: int, q: int, root: int, inverse: bool = False) -> int:
+    """The reference's own ntt_forward / ntt_inverse, in place on a uint64
+    numpy array."""
+    global _ref_ntt
+    if _ref_ntt is None:
+        L = ctypes.CDLL(str(REF_NTT_PATH))
+        for name in ("ntt_forward", "ntt_inverse"):
+            f = getattr(L, name)
+            f.restype = ctypes.c_int
+            f.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint64]
+        _ref_ntt = L
+    f = _ref_ntt.ntt_inverse if inverse else _ref_ntt.ntt_forward
+    return f(a.ctypes.data, n, q, root)
 
 
 # Field moduli for host-side checks (canonical integers).

@@ -15,6 +15,12 @@ The reference has no Fr NTT, so NTT vectors come from the C restatement in
 oracle/ and are cross-checked here against an O(n^2) DFT before writing.
 KZG vectors: SRS [tau^i]G1 from the reference ladder, commit = restated iNTT
 -> reference MSM -> compressed encoding.
+
+Word-prime NTT vectors (word_ntt.json.gz; `--word-ntt` regenerates only
+these): the reference's own known-answer vectors (ntt/test/vectors/
+ntt_kat.json, re-checked against the reference build), listed small-size
+outputs of the reference build (oracle/_ref/libref_ntt.so) across its
+dispatch, and SHA-256 digests of its six-step outputs on seeded inputs.
 """
 from __future__ import annotations
 
@@ -98,12 +104,88 @@ def kzg_cases(rng: random.Random) -> list[dict]:
     return cases
 
 
+# ---- word-prime NTT (ntt_forward / ntt_inverse) -----------------------------
+
+CYC_Q, CYC_ROOT = 998244353, 629671588
+GOLD_Q = 0xFFFFFFFF00000001
+KAT = Path("/root/reference/ntt/test/vectors/ntt_kat.json")
+
+
+def word_ntt_inputs(seed: int, n: int, q: int, canonical: bool):
+    """Seeded input words (PCG64 raw 64-bit draws, reduced mod q if
+    canonical); the tests regenerate them with this same function."""
+    import numpy as np
+    raw = np.random.Generator(np.random.PCG64(seed)).bit_generator.random_raw(n).astype(np.uint64)
+    return raw % np.uint64(q) if canonical else raw
+
+
+def ref_word_ntt(words, q: int, root: int, inverse: bool):
+    import numpy as np
+    a = np.array(words, dtype=np.uint64)
+    rc = O.ref_word_ntt(a, len(a), q, root, inverse)
+    return rc, a
+
+
+def word_ntt_cases() -> dict:
+    import hashlib
+    import numpy as np
+    # 1. the reference's own known-answer vectors (Cyclone path), checked
+    #    against the reference build before they are copied into the fixture
+    kat = []
+    for v in json.loads(KAT.read_text()):
+        rc, fwd = ref_word_ntt(v["input"], CYC_Q, CYC_ROOT, False)
+        assert rc == 0 and [int(x) for x in fwd] == v["forward"], v["name"]
+        kat.append({"name": v["name"], "n": v["n"], "input": v["input"], "forward": v["forward"]})
+    # 2. listed small-path vectors across the dispatch (reference outputs)
+    small = []
+    specs = [("cyc_noncanonical", CYC_Q, CYC_ROOT, 256, False),
+             ("gold_generic", GOLD_Q, pow(7, (GOLD_Q - 1) // 1024, GOLD_Q), 1024, True),
+             ("gold_noncanonical", GOLD_Q, pow(7, (GOLD_Q - 1) // 64, GOLD_Q), 64, False),
+             ("cyc_other_root", CYC_Q, pow(3, (CYC_Q - 1) // 512, CYC_Q), 512, True),
+             ("mersenne61_any_root", (1 << 61) - 1, 37, 128, False),
+             ("even_modulus", 1 << 40, 12345, 32, False)]
+    for i, (name, q, root, n, canon) in enumerate(specs):
+        x = word_ntt_inputs(100 + i, n, q, canon)
+        rc, f = ref_word_ntt(x, q, root, False)
+        rc2, b = ref_word_ntt(x, q, root, True)
+        assert rc == 0 and rc2 == 0
+        small.append({"name": name, "n": n, "q": q, "root": root,
+                      "input": [int(v) for v in x], "forward": [int(v) for v in f],
+                      "inverse": [int(v) for v in b]})
+    # 3. six-step path: hashes of the reference outputs on seeded inputs
+    large = []
+    for i, (name, q, g, logn, canon) in enumerate([("cyc_2^17", CYC_Q, 3, 17, True),
+                                                   ("gold_2^17", GOLD_Q, 7, 17, False),
+                                                   ("gold_2^20", GOLD_Q, 7, 20, True),
+                                                   ("cyc_2^20", CYC_Q, 3, 20, True)]):
+        n = 1 << logn
+        root = pow(g, (q - 1) // (2 * n), q)
+        x = word_ntt_inputs(200 + i, n, q, canon)
+        rc, f = ref_word_ntt(x, q, root, False)
+        root_inv = pow(root, q - 2, q)
+        rc2, b = ref_word_ntt(x, q, root_inv, True)
+        rc3, rt = ref_word_ntt(f, q, root_inv, True)
+        assert rc == rc2 == rc3 == 0
+        if canon:
+            assert np.array_equal(rt, x), name
+        large.append({"name": name, "n": n, "q": q, "root": root, "root_inv": root_inv,
+                      "seed": 200 + i, "canonical": canon,
+                      "forward_sha256": hashlib.sha256(f.tobytes()).hexdigest(),
+                      "inverse_sha256": hashlib.sha256(b.tobytes()).hexdigest()})
+    return {"kat": kat, "small": small, "large": large}
+
+
 def main() -> None:
-    rng = random.Random(SEED)
-    data = {"msm": msm_cases(rng), "ntt": ntt_cases(rng), "kzg": kzg_cases(rng)}
-    with gzip.open(HERE / "golden.json.gz", "wt") as f:
-        json.dump(data, f)
-    print({k: len(v) for k, v in data.items()})
+    if "--word-ntt" not in sys.argv[1:]:
+        rng = random.Random(SEED)
+        data = {"msm": msm_cases(rng), "ntt": ntt_cases(rng), "kzg": kzg_cases(rng)}
+        with gzip.open(HERE / "golden.json.gz", "wt") as f:
+            json.dump(data, f)
+        print({k: len(v) for k, v in data.items()})
+    w = word_ntt_cases()
+    with gzip.open(HERE / "word_ntt.json.gz", "wt") as f:
+        json.dump(w, f)
+    print({k: len(v) for k, v in w.items()})
 
 
 if __name__ == "__main__":
