@@ -48,6 +48,8 @@ def lib() -> ctypes.CDLL:
         sigs = {
             "gpukit_multi_pippenger": (c.c_int, [c.c_uint32, u8p, u8p, sz, vp]),
             "gpukit_multi_pippenger_cuda": (c.c_int, [c.c_uint32, u8p, u8p, sz, vp]),
+            "bls12_381_g1_msm": (c.c_int, [vp, vp, u8p, sz]),
+            "kb200_bls12_381_g1_msm_device": (c.c_int, [vp, sz, vp, vp, vp]),
             "ntt_forward": (c.c_int, [vp, sz, c.c_uint64, c.c_uint64]),
             "ntt_inverse": (c.c_int, [vp, sz, c.c_uint64, c.c_uint64]),
             "kb200_word_ntt_device": (c.c_int, [vp, vp, sz, c.c_uint64, c.c_uint64, c.c_int, vp]),
@@ -112,6 +114,15 @@ def gpukit_multi_pippenger(curve: int, scalars: bytes, points: bytes, n: int) ->
     _check("gpukit_multi_pippenger",
            lib().gpukit_multi_pippenger(curve, scalars, points, n, out))
     return out.raw
+
+
+def bls12_381_g1_msm(xycs: bytes):
+    """EIP-2537 BLS12_G1MSM: returns (status, rx || ry) with status 1 = ok,
+    0 = invalid input, < 0 = backend error."""
+    rx = ctypes.create_string_buffer(64)
+    ry = ctypes.create_string_buffer(64)
+    rc = lib().bls12_381_g1_msm(rx, ry, xycs, len(xycs))
+    return rc, rx.raw + ry.raw
 
 
 def msm_rc(curve: int, scalars, points, n: int, out) -> int:

@@ -3,6 +3,7 @@
 // staging, resident SRS) guarded by a mutex.
 #include "../../include/kinet_b200/crypto_b200.h"
 #include "batch.cuh"
+#include "eip2537.cuh"
 #include "curve.cuh"
 #include "kzg.cuh"
 #include "msm.cuh"
@@ -39,7 +40,7 @@ struct DeviceCtx {
     FixedBase* fb[3] = {nullptr, nullptr, nullptr};
     CommitBatcher* batcher = nullptr;
     WordNttCache* wntt = nullptr;
-    DevBuf d_a, d_b, d_out, d_srs, d_tmp, d_w, d_ws;
+    DevBuf d_a, d_b, d_out, d_srs, d_tmp, d_w, d_ws, d_e_in, d_e_tab, d_e_sc, d_e_out;
     HostBuf h_a, h_b, h_out;
     size_t srs_n = 0;
 
@@ -212,6 +213,46 @@ static int word_ntt_host(uint64_t* coeffs, size_t n, uint64_t modulus, uint64_t 
                    });
 }
 
+// ---- EIP-2537 G1 MSM -------------------------------------------------------
+
+// bls12_381_g1_msm (bls/c-abi/c_bls_pairing.cpp:106-110): 1 = result
+// written, 0 = invalid input.  Reference behaviour kept: (0,0) entries are
+// infinity and skipped, an input of no finite points gives (0,0).
+static int g1_msm_eip2537_host(uint8_t* rx, uint8_t* ry, const uint8_t* xycs, size_t size) {
+    if (!rx || !ry || (size && !xycs) || size % 160) return 0;
+    const size_t n = size / 160;
+    return guarded(KB200_CRYPTO_ERR_BACKEND, 0, KB200_CRYPTO_ERR_INTERNAL, [&]() -> int {
+        DeviceCtx* c = get_ctx();
+        std::lock_guard<std::mutex> lk(c->mu);
+        cudaStream_t st = c->stream;
+        c->d_e_in.reserve(size + 16, st);
+        c->d_e_tab.reserve(n * (size_t)table_words(2) * 4 + 16, st);
+        c->d_e_sc.reserve(n * 32 + 16, st);
+        c->d_e_out.reserve(256, st);
+        c->h_out.reserve(256, st);
+        if (size)
+            KB_CUDA(cudaMemcpyAsync(c->d_e_in.ptr, xycs, size, cudaMemcpyHostToDevice, st));
+        uint8_t* d_out = c->d_e_out.as<uint8_t>();
+        uint32_t* d_flag = reinterpret_cast<uint32_t*>(d_out + 128);
+        g1_msm_eip2537_device(c->msm_for(2), c->d_e_in.as<uint8_t>(), n, c->d_e_tab.as<uint32_t>(),
+                              c->d_e_sc.as<uint8_t>(), d_flag, d_out, st);
+        KB_CUDA(cudaMemcpyAsync(c->h_out.ptr, d_out, 132, cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaStreamSynchronize(st));
+        const uint8_t* h = static_cast<const uint8_t*>(c->h_out.ptr);
+        uint32_t flag;
+        std::memcpy(&flag, h + 128, 4);
+        if (flag) {
+            set_last_error("bls12_381_g1_msm: a point is out of range, off the curve or not in G1");
+            return 0;
+        }
+        std::memset(rx, 0, 16);
+        std::memset(ry, 0, 16);
+        std::memcpy(rx + 16, h, 48);
+        std::memcpy(ry + 16, h + 48, 48);
+        return 1;
+    });
+}
+
 // ---- KZG -------------------------------------------------------------------
 
 static void commit_on_device(DeviceCtx* c, uint32_t* d_evals, size_t n, uint8_t* d_out48,
@@ -373,6 +414,28 @@ int kb200_msm_device(uint32_t curve, const void* d_scalars, const void* d_points
                                     (const uint8_t*)d_points, n, (uint8_t*)d_result, nullptr,
                                     (cudaStream_t)stream, opt);
                        return KB200_GPUKIT_OK;
+                   });
+}
+
+int bls12_381_g1_msm(uint8_t rx[64], uint8_t ry[64], const uint8_t* xycs, size_t size) {
+    return g1_msm_eip2537_host(rx, ry, xycs, size);
+}
+
+int kb200_bls12_381_g1_msm_device(const void* d_xycs, size_t size, void* d_out_wire96,
+                                  void* d_status, void* stream) {
+    if (!d_out_wire96 || !d_status || (size && !d_xycs) || size % 160) return KB200_CRYPTO_ERR_INPUT;
+    const size_t n = size / 160;
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_LENGTH, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       cudaStream_t st = (cudaStream_t)stream;
+                       c->d_e_tab.reserve(n * (size_t)table_words(2) * 4 + 16, st);
+                       c->d_e_sc.reserve(n * 32 + 16, st);
+                       g1_msm_eip2537_device(c->msm_for(2), (const uint8_t*)d_xycs, n,
+                                             c->d_e_tab.as<uint32_t>(), c->d_e_sc.as<uint8_t>(),
+                                             (uint32_t*)d_status, (uint8_t*)d_out_wire96, st);
+                       return KB200_CRYPTO_OK;
                    });
 }
 

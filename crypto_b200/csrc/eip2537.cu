@@ -1,0 +1,150 @@
+// EIP-2537 BLS12_G1MSM on the GPU, behind the reference's bls12_381_g1_msm
+// (bls/c-abi/c_bls_pairing.cpp:106-110; body bls/cpp/bls.cpp:194-254, which
+// hands the work to blst).  One thread per entry checks, as the reference
+// does before its Pippenger call:
+//   * each coordinate, a 64-byte big-endian integer, is below p
+//     (bls.cpp:33-41; so its top 16 bytes are zero);
+//   * the point is on y^2 = x^3 + 4, or is (0,0), the EIP-2537 infinity
+//     (bls.cpp:44-58);
+//   * the point is in G1 (bls.cpp:217-218), by the endomorphism test:
+//     P in G1 iff sigma(P) = -[u^2]P, with sigma(x, y) = (beta x, y), beta a
+//     cube root of unity in Fp and u = -0xd201000000010000 the curve
+//     parameter (M. Scott, "A note on group membership tests for G1, G2 and
+//     GT on BLS pairing-friendly curves", 2021);
+// then drops infinity entries (bls.cpp:220-222), reduces the big-endian
+// scalar mod r (the sum over points of order r is unchanged), and runs the
+// G1 MSM of msm.cu on the resulting table.
+#include "curve.cuh"
+#include "eip2537.cuh"
+#include "runtime.cuh"
+
+namespace kb200 {
+namespace {
+
+using F = FpBLS;
+using FR = FrBLS;
+
+// |u| for the BLS12-381 parameter u = -0xd201000000010000.
+constexpr uint64_t BLS_U_ABS = 0xd201000000010000ull;
+
+// beta: the primitive cube root of unity of Fp for which sigma acts on G1
+// as multiplication by -u^2 (canonical, little-endian 32-bit words).
+__constant__ uint32_t kBeta[12] = {0xfffefffe, 0x2e01ffff, 0x620a0002, 0xde17d813,
+                                   0xe6f89688, 0xddb3a93b, 0x6a0f77ea, 0xba69c607,
+                                   0xdf76ce51, 0x5f19672f, 0x00000000, 0x00000000};
+
+template <class Fx>
+__device__ __forceinline__ bool below_modulus(const Fe<Fx>& a) {
+    for (int i = Fx::N - 1; i >= 0; --i) {
+        if (a.v[i] != Fx::P(i)) return a.v[i] < Fx::P(i);
+    }
+    return false;
+}
+
+// A 64-byte big-endian coordinate below p (its top 16 bytes zero).
+__device__ bool coord_ok(const uint8_t* c, Fe<F>& v) {
+    uint32_t hi = 0;
+    for (int i = 0; i < 16; ++i) hi |= c[i];
+    fe_from_be_bytes(v, c + 16);
+    return hi == 0 && below_modulus(v);
+}
+
+// [|u|] base, double-and-add from the top bit (bit 63 is set).
+__device__ void mul_abs_u(Xyzz<F>& acc, const Xyzz<F>& base) {
+    acc = base;
+    for (int b = 62; b >= 0; --b) {
+        xyzz_dbl(acc, acc);
+        if ((BLS_U_ABS >> b) & 1ull) xyzz_add(acc, base);
+    }
+}
+
+// a finite affine point on the curve (Montgomery form): in G1?
+__device__ bool in_g1(const Affine<F>& a) {
+    Xyzz<F> p, q1, q2;
+    xyzz_from_affine(p, a);
+    mul_abs_u(q1, p);
+    mul_abs_u(q2, q1);  // [u^2] P
+    if (xyzz_is_inf(q2)) return false;
+    Fe<F> beta, t;
+    fe_load(beta, kBeta);
+    fe_to_mont(beta, beta);
+    fe_mul(t, beta, a.x);
+    fe_mul(t, t, q2.ZZ);
+    if (!fe_eq(t, q2.X)) return false;  // beta x == X / ZZ
+    fe_neg(t, a.y);
+    fe_mul(t, t, q2.ZZZ);
+    return fe_eq(t, q2.Y);              // -y == Y / ZZZ
+}
+
+__device__ bool on_curve(const Affine<F>& a) {
+    Fe<F> l, r, b;
+    fe_sqr(l, a.y);
+    fe_sqr(r, a.x);
+    fe_mul(r, r, a.x);
+    fe_one(b);
+    fe_add(b, b, b);
+    fe_add(b, b, b);  // 4 in Montgomery form
+    fe_add(r, r, b);
+    return fe_eq(l, r);
+}
+
+__global__ void __launch_bounds__(128) k_g1msm_unpack(const uint8_t* __restrict__ xycs, uint32_t n,
+                                                      uint32_t* __restrict__ table,
+                                                      uint8_t* __restrict__ scalars,
+                                                      uint32_t* __restrict__ flag) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint8_t* e = xycs + (size_t)160 * i;
+    uint32_t* row = table + (size_t)i * 2 * F::N;
+    uint32_t* sc = reinterpret_cast<uint32_t*>(scalars + (size_t)32 * i);
+    Fe<F> x, y;
+    bool ok = coord_ok(e, x);
+    ok = coord_ok(e + 64, y) && ok;
+    bool inf = false;
+    if (ok) {
+        inf = fe_is_zero(x) && fe_is_zero(y);
+        if (!inf) {
+            Affine<F> a;
+            fe_to_mont(a.x, x);
+            fe_to_mont(a.y, y);
+            ok = on_curve(a) && in_g1(a);
+            fe_store(row, a.x);
+            fe_store(row + F::N, a.y);
+        }
+    }
+    if (!ok) atomicOr(flag, 1u);
+    if (!ok || inf) {
+        for (int k = 0; k < 2 * F::N; ++k) row[k] = 0;
+        row[F::N - 1] = INF_FLAG;
+        for (int k = 0; k < 8; ++k) sc[k] = 0;
+        return;
+    }
+    Fe<FR> s;
+    fe_from_be_bytes(s, e + 128);
+    while (!below_modulus(s)) {  // at most twice: 2^256 < 3r
+        uint32_t b = 0;
+        for (int k = 0; k < FR::N; ++k) {
+            const uint64_t d = (uint64_t)s.v[k] - FR::P(k) - b;
+            s.v[k] = (uint32_t)d;
+            b = (uint32_t)(d >> 63);
+        }
+    }
+    for (int k = 0; k < 8; ++k) sc[k] = s.v[k];
+}
+
+}  // namespace
+
+void g1_msm_eip2537_device(MsmEngine* eng, const uint8_t* d_xycs, size_t n, uint32_t* d_table,
+                           uint8_t* d_scalars, uint32_t* d_flag, uint8_t* d_out_wire,
+                           cudaStream_t st) {
+    KB_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(uint32_t), st));
+    if (n) {
+        k_g1msm_unpack<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(d_xycs, (uint32_t)n, d_table,
+                                                                     d_scalars, d_flag);
+        KB_LAUNCH_CHECK();
+    }
+    MsmOptions opt;
+    msm_run_table(eng, d_scalars, d_table, n, d_out_wire, nullptr, st, opt);
+}
+
+}  // namespace kb200

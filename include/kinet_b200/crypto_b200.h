@@ -69,6 +69,20 @@ int gpukit_multi_pippenger(uint32_t curve, const uint8_t* scalars, const uint8_t
 int gpukit_multi_pippenger_cuda(uint32_t curve, const uint8_t* scalars,
                                 const uint8_t* points, size_t n, uint8_t* result);
 
+/* ---- EIP-2537 G1 MSM (replaces bls12_381_g1_msm, bls/c-abi/c_bls_pairing.h:
+ * 153-156, body bls/cpp/bls.cpp:194-254) ----------------------------------- */
+
+/* BLS12_G1MSM: xycs holds N entries of x[64] || y[64] || c[32], all big
+ * endian, size = 160 N.  Each coordinate must be below p (so its top 16
+ * bytes are zero), each point on the curve and in G1; (0,0) is the point at
+ * infinity and is skipped.  The scalar is any 256-bit value.  Writes the sum
+ * as rx, ry (16 zero bytes then the 48-byte big-endian coordinate; (0,0) for
+ * infinity) and returns 1; returns 0 for invalid input (also for size not a
+ * multiple of 160, which the reference only asserts, and for null
+ * pointers), and CRYPTO_ERR_BACKEND (< 0) when no GPU is usable -- a value
+ * the reference's CPU body never returns. */
+int bls12_381_g1_msm(uint8_t rx[64], uint8_t ry[64], const uint8_t* xycs, size_t size);
+
 /* ---- Word-prime NTT (replaces ntt_forward/ntt_inverse, crypto.h:368-369,
  * bodies ntt/c-abi/c_ntt.cpp:81-179) --------------------------------------- */
 
@@ -173,6 +187,10 @@ int ntt_fr_transform_noalloc(int curve, uint8_t* coeffs32le, size_t n, int inver
  * synchronised.  Calls sharing a device must not overlap across streams. */
 int kb200_msm_device(uint32_t curve, const void* d_scalars, const void* d_points, size_t n,
                      void* d_result, void* stream);
+/* bls12_381_g1_msm on device memory: d_out_wire96 receives x || y (48 B BE
+ * each, zeros for infinity), d_status one 32-bit word: 0 valid, 1 invalid. */
+int kb200_bls12_381_g1_msm_device(const void* d_xycs, size_t size, void* d_out_wire96,
+                                  void* d_status, void* stream);
 /* ntt_forward (inverse = 0) / ntt_inverse (inverse = 1) on device words;
  * d_scratch (n words) is needed for 2^11 < n <= 2^16. */
 int kb200_word_ntt_device(void* d_coeffs, void* d_scratch, size_t n, uint64_t modulus,

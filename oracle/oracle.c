@@ -749,3 +749,66 @@ int orc_kzg_commit(const uint8_t* evals, size_t n, const uint8_t* srs,
     if (rc) return rc;
     return orc_g1_compress(pt, commit48);
 }
+
+/* ---- EIP-2537 G1 MSM (bls/cpp/bls.cpp:194-254, bls/c-abi/c_bls_pairing.cpp:106-110).
+ * The reference delegates to blst (absent here); this restates the published
+ * EIP-2537 semantics with the definitional checks: each 64-byte coordinate is
+ * a big-endian integer below p (so its top 16 bytes are zero), the point is
+ * on the curve or is (0,0) = infinity, and the subgroup check is [r]P = O.
+ * Infinity entries are dropped, scalars (32 B big-endian) are reduced mod r
+ * (exact for points of order r), and the sum comes from orc_msm. */
+static int be64_coord_ok(const uint8_t* c) {
+    for (int i = 0; i < 16; ++i)
+        if (c[i]) return 0;
+    fe v = fe_from_be(&F_BLS_FP, c + 16);
+    return fe_cmp(&F_BLS_FP, &v, &F_BLS_FP.p) < 0;
+}
+
+int orc_bls12_381_g1_msm(uint8_t rx[64], uint8_t ry[64], const uint8_t* xycs, size_t size) {
+    if (!rx || !ry || (size && !xycs) || size % 160) return 0;
+    const size_t n = size / 160;
+    uint8_t* pts = (uint8_t*)malloc(96 * (n ? n : 1));
+    uint8_t* scs = (uint8_t*)malloc(32 * (n ? n : 1));
+    size_t m = 0;
+    uint8_t r_le[32];
+    fe_to_le(&F_BLS_FR, &F_BLS_FR.p, r_le);
+    for (size_t i = 0; i < n; ++i) {
+        const uint8_t* e = xycs + 160 * i;
+        if (!be64_coord_ok(e) || !be64_coord_ok(e + 64)) goto invalid;
+        uint8_t pt[96];
+        memcpy(pt, e + 16, 48);
+        memcpy(pt + 48, e + 80, 48);
+        if (!orc_g1_on_curve(ORC_CURVE_BLS12_381, pt)) goto invalid;
+        int inf = 1;
+        for (int k = 0; k < 96; ++k) inf &= pt[k] == 0;
+        if (inf) continue;
+        uint8_t rp[96];
+        orc_g1_mul(ORC_CURVE_BLS12_381, pt, r_le, rp);
+        for (int k = 0; k < 96; ++k)
+            if (rp[k]) goto invalid;
+        /* scalar: big-endian 256-bit -> little-endian, reduced mod r */
+        fe s;
+        memset(&s, 0, sizeof s);
+        for (int k = 0; k < 32; ++k) s.l[k / 8] |= (u64)e[128 + 31 - k] << (8 * (k % 8));
+        while (fe_cmp(&F_BLS_FR, &s, &F_BLS_FR.p) >= 0) raw_sub(&F_BLS_FR, &s, &s, &F_BLS_FR.p);
+        memcpy(pts + 96 * m, pt, 96);
+        fe_to_le(&F_BLS_FR, &s, scs + 32 * m);
+        ++m;
+    }
+    {
+        uint8_t out[96];
+        memset(out, 0, 96);
+        if (m) orc_msm(ORC_CURVE_BLS12_381, scs, pts, m, out);
+        memset(rx, 0, 64);
+        memset(ry, 0, 64);
+        memcpy(rx + 16, out, 48);
+        memcpy(ry + 16, out + 48, 48);
+    }
+    free(pts);
+    free(scs);
+    return 1;
+invalid:
+    free(pts);
+    free(scs);
+    return 0;
+}

@@ -90,6 +90,14 @@ int orc_kzg_commit(const uint8_t* evals, size_t n, const uint8_t* srs,
 /* Fr helpers: powers tau^0..tau^(n-1) (canonical 32 B LE), and a*b mod r. */
 int orc_fr_powers(uint32_t curve, const uint8_t* tau, size_t n, uint8_t* out);
 
+/* EIP-2537 BLS12_G1MSM with the contract of the reference's
+ * bls12_381_g1_msm (bls/c-abi/c_bls_pairing.h:155, bls/cpp/bls.cpp:194-254):
+ * xycs = N x (x[64] || y[64] || c[32]) big-endian, size = 160 N; returns 1
+ * with rx, ry (64 B each, 16 zero bytes then 48 B BE) or 0 if any point is
+ * out of range, off the curve or outside G1.  (0,0) is infinity and is
+ * skipped. */
+int orc_bls12_381_g1_msm(uint8_t rx[64], uint8_t ry[64], const uint8_t* xycs, size_t size);
+
 /* Word-prime NTT with the contract of the reference's ntt_forward /
  * ntt_inverse (ntt/c-abi/c_ntt.cpp:81-179): in place on n uint64 words;
  * n <= 2^16 natural order (Cyclone prime 998244353 with its pinned root on

@@ -45,6 +45,7 @@ def orc() -> ctypes.CDLL:
             "orc_fr_powers": [ctypes.c_uint32, ctypes.c_char_p, sz, ctypes.c_void_p],
             "orc_field_mul": [ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_void_p],
             "orc_field_inv": [ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p],
+            "orc_bls12_381_g1_msm": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p, sz],
             "orc_word_ntt_forward": [ctypes.c_void_p, sz, ctypes.c_uint64, ctypes.c_uint64],
             "orc_word_ntt_inverse": [ctypes.c_void_p, sz, ctypes.c_uint64, ctypes.c_uint64],
         }.items():
@@ -153,6 +154,14 @@ def fr_powers(curve: int, tau: bytes, n: int) -> bytes:
     out = ctypes.create_string_buffer(32 * n)
     assert orc().orc_fr_powers(curve, tau, n, out) == 0
     return out.raw
+
+
+def bls12_381_g1_msm(xycs: bytes):
+    """Oracle EIP-2537 G1 MSM: (status 1/0, rx || ry)."""
+    rx = ctypes.create_string_buffer(64)
+    ry = ctypes.create_string_buffer(64)
+    rc = orc().orc_bls12_381_g1_msm(rx, ry, xycs, len(xycs))
+    return rc, rx.raw + ry.raw
 
 
 def word_ntt(words, q: int, root: int, inverse: bool = False):
