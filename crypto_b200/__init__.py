@@ -49,6 +49,10 @@ def lib() -> ctypes.CDLL:
             "gpukit_multi_pippenger": (c.c_int, [c.c_uint32, u8p, u8p, sz, vp]),
             "gpukit_multi_pippenger_cuda": (c.c_int, [c.c_uint32, u8p, u8p, sz, vp]),
             "bls12_381_g1_msm": (c.c_int, [vp, vp, u8p, sz]),
+            "kzg_blob_setup_load_g1_lagrange": (c.c_int, [u8p, sz]),
+            "kzg_blob_setup_generate": (c.c_int, [u8p]),
+            "kzg_blob_to_commit": (c.c_int, [u8p, vp]),
+            "kzg_commit_to_proof": (c.c_int, [u8p, u8p, vp, vp]),
             "kb200_bls12_381_g1_msm_device": (c.c_int, [vp, sz, vp, vp, vp]),
             "ntt_forward": (c.c_int, [vp, sz, c.c_uint64, c.c_uint64]),
             "ntt_inverse": (c.c_int, [vp, sz, c.c_uint64, c.c_uint64]),
@@ -123,6 +127,21 @@ def bls12_381_g1_msm(xycs: bytes):
     ry = ctypes.create_string_buffer(64)
     rc = lib().bls12_381_g1_msm(rx, ry, xycs, len(xycs))
     return rc, rx.raw + ry.raw
+
+
+def kzg_blob_to_commit(blob: bytes):
+    """(status, 48-byte commitment) for a 131072-byte blob."""
+    out = ctypes.create_string_buffer(48)
+    rc = lib().kzg_blob_to_commit(blob, out)
+    return rc, out.raw
+
+
+def kzg_commit_to_proof(blob: bytes, z: bytes):
+    """(status, 48-byte proof, 32-byte big-endian y)."""
+    proof = ctypes.create_string_buffer(48)
+    y = ctypes.create_string_buffer(32)
+    rc = lib().kzg_commit_to_proof(blob, z, proof, y)
+    return rc, proof.raw, y.raw
 
 
 def msm_rc(curve: int, scalars, points, n: int, out) -> int:

@@ -6,11 +6,13 @@
 #include "eip2537.cuh"
 #include "curve.cuh"
 #include "kzg.cuh"
+#include "kzg_blob.cuh"
 #include "msm.cuh"
 #include "ntt.cuh"
 #include "runtime.cuh"
 #include "wntt.cuh"
 
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <map>
@@ -40,6 +42,12 @@ struct DeviceCtx {
     FixedBase* fb[3] = {nullptr, nullptr, nullptr};
     CommitBatcher* batcher = nullptr;
     WordNttCache* wntt = nullptr;
+    BlobSetup* blob = nullptr;
+    DevBuf d_bl;  // blob ops: input, z, outputs, flag
+    BlobSetup* blob_get() {
+        if (!blob) blob = blob_setup_create();
+        return blob;
+    }
     DevBuf d_a, d_b, d_out, d_srs, d_tmp, d_w, d_ws, d_e_in, d_e_tab, d_e_sc, d_e_out;
     HostBuf h_a, h_b, h_out;
     size_t srs_n = 0;
@@ -253,6 +261,86 @@ static int g1_msm_eip2537_host(uint8_t* rx, uint8_t* ry, const uint8_t* xycs, si
     });
 }
 
+// ---- EIP-4844 blobs ----------------------------------------------------------
+
+// Layout of the blob-op staging buffer d_bl.
+constexpr size_t BL_BLOB = 0, BL_Z = BLOB_BYTES, BL_OUT = BLOB_BYTES + 64, BL_Y = BL_OUT + 64,
+                 BL_FLAG = BL_Y + 64, BL_SIZE = BL_FLAG + 64;
+
+static void blob_stage(DeviceCtx* c, cudaStream_t st) {
+    c->d_bl.reserve(BL_SIZE + (size_t)BLOB_N * 48, st);  // + setup points after BL_SIZE
+    c->h_out.reserve(256, st);
+}
+
+static int blob_setup_host(const uint8_t* points48, size_t n) {
+    if (!points48) return KB200_CRYPTO_ERR_INPUT;
+    if (n != BLOB_N) return KB200_CRYPTO_ERR_LENGTH;
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_LENGTH, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       cudaStream_t st = c->stream;
+                       blob_stage(c, st);
+                       uint8_t* base = c->d_bl.as<uint8_t>();
+                       KB_CUDA(cudaMemcpyAsync(base + BL_SIZE, points48, n * 48, cudaMemcpyHostToDevice,
+                                               st));
+                       uint32_t* d_flag = reinterpret_cast<uint32_t*>(base + BL_FLAG);
+                       blob_setup_load_lagrange(c->blob_get(), base + BL_SIZE, d_flag, st);
+                       KB_CUDA(cudaMemcpyAsync(c->h_out.ptr, d_flag, 4, cudaMemcpyDeviceToHost, st));
+                       KB_CUDA(cudaStreamSynchronize(st));
+                       uint32_t flag;
+                       std::memcpy(&flag, c->h_out.ptr, 4);
+                       if (flag) {
+                           blob_setup_mark(c->blob, false);
+                           set_last_error("kzg blob setup: a point is not a valid compressed G1 point");
+                           return KB200_CRYPTO_ERR_INPUT;
+                       }
+                       return KB200_CRYPTO_OK;
+                   });
+}
+
+// kzg_blob_to_commit (kzg/c-abi/c_kzg_blob.cpp:26-30) and kzg_commit_to_proof
+// (:32-43).  CRYPTO_ERR_INPUT for null pointers, a blob element or z not
+// below r, or no resident setup (the reference's setup-load failure).
+static int blob_op_host(const uint8_t* blob, const uint8_t* z, uint8_t* out48, uint8_t* y32) {
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_INPUT, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       if (!blob_setup_ready(c->blob)) {
+                           set_last_error("kzg blob ops: no setup loaded (kzg_blob_setup_load_g1_lagrange)");
+                           return KB200_CRYPTO_ERR_INPUT;
+                       }
+                       cudaStream_t st = c->stream;
+                       blob_stage(c, st);
+                       uint8_t* base = c->d_bl.as<uint8_t>();
+                       uint32_t* d_flag = reinterpret_cast<uint32_t*>(base + BL_FLAG);
+                       KB_CUDA(cudaMemcpyAsync(base + BL_BLOB, blob, BLOB_BYTES, cudaMemcpyHostToDevice, st));
+                       if (z) {
+                           KB_CUDA(cudaMemcpyAsync(base + BL_Z, z, 32, cudaMemcpyHostToDevice, st));
+                           blob_proof_device(c->blob, c->msm_for(2), base + BL_BLOB, base + BL_Z,
+                                             base + BL_OUT, base + BL_Y, d_flag, st);
+                       } else {
+                           blob_commit_device(c->blob, c->msm_for(2), base + BL_BLOB, base + BL_OUT,
+                                              d_flag, st);
+                       }
+                       // out (48) | pad | y (32) | pad | flag, copied back in one piece
+                       KB_CUDA(cudaMemcpyAsync(c->h_out.ptr, base + BL_OUT, BL_FLAG + 4 - BL_OUT,
+                                               cudaMemcpyDeviceToHost, st));
+                       KB_CUDA(cudaStreamSynchronize(st));
+                       const uint8_t* h = static_cast<const uint8_t*>(c->h_out.ptr);
+                       uint32_t flag;
+                       std::memcpy(&flag, h + (BL_FLAG - BL_OUT), 4);
+                       if (flag) {
+                           set_last_error("kzg blob ops: a field element is not below r");
+                           return KB200_CRYPTO_ERR_INPUT;
+                       }
+                       std::memcpy(out48, h, 48);
+                       if (y32) std::memcpy(y32, h + (BL_Y - BL_OUT), 32);
+                       return KB200_CRYPTO_OK;
+                   });
+}
+
 // ---- KZG -------------------------------------------------------------------
 
 static void commit_on_device(DeviceCtx* c, uint32_t* d_evals, size_t n, uint8_t* d_out48,
@@ -415,6 +503,37 @@ int kb200_msm_device(uint32_t curve, const void* d_scalars, const void* d_points
                                     (cudaStream_t)stream, opt);
                        return KB200_GPUKIT_OK;
                    });
+}
+
+int kzg_blob_setup_load_g1_lagrange(const uint8_t* points48, size_t n) {
+    return blob_setup_host(points48, n);
+}
+
+int kzg_blob_setup_generate(const uint8_t tau32le[32]) {
+    if (!tau32le) return KB200_CRYPTO_ERR_INPUT;
+    return guarded(KB200_CRYPTO_ERR_BACKEND, KB200_CRYPTO_ERR_LENGTH, KB200_CRYPTO_ERR_INTERNAL,
+                   [&]() -> int {
+                       DeviceCtx* c = get_ctx();
+                       std::lock_guard<std::mutex> lk(c->mu);
+                       cudaStream_t st = c->stream;
+                       blob_stage(c, st);
+                       uint8_t* d_tau = c->d_bl.as<uint8_t>() + BL_Z;
+                       KB_CUDA(cudaMemcpyAsync(d_tau, tau32le, 32, cudaMemcpyHostToDevice, st));
+                       blob_setup_generate(c->blob_get(), c->fb_for(2), d_tau, st);
+                       KB_CUDA(cudaStreamSynchronize(st));
+                       return KB200_CRYPTO_OK;
+                   });
+}
+
+int kzg_blob_to_commit(const uint8_t blob[131072], uint8_t commit[48]) {
+    if (!blob || !commit) return KB200_CRYPTO_ERR_INPUT;
+    return blob_op_host(blob, nullptr, commit, nullptr);
+}
+
+int kzg_commit_to_proof(const uint8_t blob[131072], const uint8_t z[32], uint8_t proof[48],
+                        uint8_t y[32]) {
+    if (!blob || !z || !proof || !y) return KB200_CRYPTO_ERR_INPUT;
+    return blob_op_host(blob, z, proof, y);
 }
 
 int bls12_381_g1_msm(uint8_t rx[64], uint8_t ry[64], const uint8_t* xycs, size_t size) {

@@ -16,6 +16,7 @@
 // G1 MSM of msm.cu on the resulting table.
 #include "curve.cuh"
 #include "eip2537.cuh"
+#include "g1check.cuh"
 #include "runtime.cuh"
 
 namespace kb200 {
@@ -24,68 +25,12 @@ namespace {
 using F = FpBLS;
 using FR = FrBLS;
 
-// |u| for the BLS12-381 parameter u = -0xd201000000010000.
-constexpr uint64_t BLS_U_ABS = 0xd201000000010000ull;
-
-// beta: the primitive cube root of unity of Fp for which sigma acts on G1
-// as multiplication by -u^2 (canonical, little-endian 32-bit words).
-__constant__ uint32_t kBeta[12] = {0xfffefffe, 0x2e01ffff, 0x620a0002, 0xde17d813,
-                                   0xe6f89688, 0xddb3a93b, 0x6a0f77ea, 0xba69c607,
-                                   0xdf76ce51, 0x5f19672f, 0x00000000, 0x00000000};
-
-template <class Fx>
-__device__ __forceinline__ bool below_modulus(const Fe<Fx>& a) {
-    for (int i = Fx::N - 1; i >= 0; --i) {
-        if (a.v[i] != Fx::P(i)) return a.v[i] < Fx::P(i);
-    }
-    return false;
-}
-
 // A 64-byte big-endian coordinate below p (its top 16 bytes zero).
 __device__ bool coord_ok(const uint8_t* c, Fe<F>& v) {
     uint32_t hi = 0;
     for (int i = 0; i < 16; ++i) hi |= c[i];
     fe_from_be_bytes(v, c + 16);
     return hi == 0 && below_modulus(v);
-}
-
-// [|u|] base, double-and-add from the top bit (bit 63 is set).
-__device__ void mul_abs_u(Xyzz<F>& acc, const Xyzz<F>& base) {
-    acc = base;
-    for (int b = 62; b >= 0; --b) {
-        xyzz_dbl(acc, acc);
-        if ((BLS_U_ABS >> b) & 1ull) xyzz_add(acc, base);
-    }
-}
-
-// a finite affine point on the curve (Montgomery form): in G1?
-__device__ bool in_g1(const Affine<F>& a) {
-    Xyzz<F> p, q1, q2;
-    xyzz_from_affine(p, a);
-    mul_abs_u(q1, p);
-    mul_abs_u(q2, q1);  // [u^2] P
-    if (xyzz_is_inf(q2)) return false;
-    Fe<F> beta, t;
-    fe_load(beta, kBeta);
-    fe_to_mont(beta, beta);
-    fe_mul(t, beta, a.x);
-    fe_mul(t, t, q2.ZZ);
-    if (!fe_eq(t, q2.X)) return false;  // beta x == X / ZZ
-    fe_neg(t, a.y);
-    fe_mul(t, t, q2.ZZZ);
-    return fe_eq(t, q2.Y);              // -y == Y / ZZZ
-}
-
-__device__ bool on_curve(const Affine<F>& a) {
-    Fe<F> l, r, b;
-    fe_sqr(l, a.y);
-    fe_sqr(r, a.x);
-    fe_mul(r, r, a.x);
-    fe_one(b);
-    fe_add(b, b, b);
-    fe_add(b, b, b);  // 4 in Montgomery form
-    fe_add(r, r, b);
-    return fe_eq(l, r);
 }
 
 __global__ void __launch_bounds__(128) k_g1msm_unpack(const uint8_t* __restrict__ xycs, uint32_t n,
@@ -107,7 +52,7 @@ __global__ void __launch_bounds__(128) k_g1msm_unpack(const uint8_t* __restrict_
             Affine<F> a;
             fe_to_mont(a.x, x);
             fe_to_mont(a.y, y);
-            ok = on_curve(a) && in_g1(a);
+            ok = g1_on_curve(a) && g1_in_subgroup(a);
             fe_store(row, a.x);
             fe_store(row + F::N, a.y);
         }

@@ -69,6 +69,30 @@ int gpukit_multi_pippenger(uint32_t curve, const uint8_t* scalars, const uint8_t
 int gpukit_multi_pippenger_cuda(uint32_t curve, const uint8_t* scalars,
                                 const uint8_t* points, size_t n, uint8_t* result);
 
+/* ---- EIP-4844 blobs (replaces kzg_blob_to_commit / kzg_commit_to_proof,
+ * crypto.h:238-239, bodies kzg/c-abi/c_kzg_blob.cpp:26-43) ------------------ */
+
+/* The reference embeds the mainnet trusted setup and evaluates through
+ * c-kzg-4844.  Here the setup is loaded once per device: the setup's 4096
+ * G1 Lagrange points, 48-byte compressed, in the trusted-setup file's order
+ * (natural order of the roots of unity; they are kept bit-reversed, as
+ * c-kzg does).  Each point is checked (encoding, curve, G1).  Returns
+ * CRYPTO_OK, CRYPTO_ERR_LENGTH (n != 4096), CRYPTO_ERR_INPUT (a bad point;
+ * the setup is then unusable until a good load). */
+int kzg_blob_setup_load_g1_lagrange(const uint8_t* points48, size_t n);
+/* Test setup [L_i(tau)]G1 for a 32-byte little-endian tau. */
+int kzg_blob_setup_generate(const uint8_t tau32le[32]);
+/* EIP-4844 blob_to_kzg_commitment: blob = 4096 big-endian field elements,
+ * element i the polynomial's value at w^brp(i) (w = 7^((r-1)/4096)); commit
+ * = 48-byte compressed [p(tau)]G1.  CRYPTO_ERR_INPUT for null pointers, an
+ * element not below r, or no loaded setup. */
+int kzg_blob_to_commit(const uint8_t blob[131072], uint8_t commit[48]);
+/* EIP-4844 compute_kzg_proof(blob, z): y = p(z) (32 B big-endian) and the
+ * 48-byte compressed proof [(p(X) - y)/(X - z) at tau]G1; z is 32 B
+ * big-endian below r (a domain point is allowed).  Same errors. */
+int kzg_commit_to_proof(const uint8_t blob[131072], const uint8_t z[32], uint8_t proof[48],
+                        uint8_t y[32]);
+
 /* ---- EIP-2537 G1 MSM (replaces bls12_381_g1_msm, bls/c-abi/c_bls_pairing.h:
  * 153-156, body bls/cpp/bls.cpp:194-254) ----------------------------------- */
 

@@ -812,3 +812,68 @@ invalid:
     free(scs);
     return 0;
 }
+
+/* ---- EIP-4844 blob commitment and opening proof (kzg/c-abi/c_kzg_blob.cpp:26-43;
+ * the reference calls c-kzg-4844 v2.1.7, absent here).  Restated from the
+ * published EIP-4844 definitions by a route independent of the device's:
+ * the blob (4096 big-endian elements, element i = p(w^brp(i))) is put in
+ * natural order, interpolated to monomial coefficients by the inverse NTT,
+ * and committed against a MONOMIAL setup [tau^i]G1 (n x 96 B BE); y = p(z)
+ * by Horner; the quotient (p(X) - y)/(X - z) by synthetic division.
+ * Returns 0, or -1 if an element or z is not below r. */
+#define ORC_BLOB_N 4096
+
+static int blob_to_coeffs(const uint8_t* blob_be, uint8_t* coeffs_le) {
+    const field* F = &F_BLS_FR;
+    for (uint32_t i = 0; i < ORC_BLOB_N; ++i) {
+        fe v = fe_from_be(F, blob_be + 32 * i);
+        if (fe_cmp(F, &v, &F->p) >= 0) return -1;
+        uint32_t j = 0;
+        for (int b = 0; b < 12; ++b) j |= ((i >> b) & 1u) << (11 - b);
+        fe_to_le(F, &v, coeffs_le + 32 * j);
+    }
+    return orc_ntt(ORC_CURVE_BLS12_381, coeffs_le, ORC_BLOB_N, 1, 0) ? -1 : 0;
+}
+
+int orc_kzg_blob_commit(const uint8_t* blob_be, const uint8_t* srs, uint8_t commit48[48]) {
+    uint8_t* c = (uint8_t*)malloc(32 * ORC_BLOB_N);
+    if (blob_to_coeffs(blob_be, c)) {
+        free(c);
+        return -1;
+    }
+    uint8_t pt[96];
+    orc_msm(ORC_CURVE_BLS12_381, c, srs, ORC_BLOB_N, pt);
+    free(c);
+    return orc_g1_compress(pt, commit48);
+}
+
+int orc_kzg_blob_proof(const uint8_t* blob_be, const uint8_t z_be[32], const uint8_t* srs,
+                       uint8_t proof48[48], uint8_t y_be[32]) {
+    const field* F = &F_BLS_FR;
+    fe z = fe_from_be(F, z_be);
+    if (fe_cmp(F, &z, &F->p) >= 0) return -1;
+    uint8_t* c = (uint8_t*)malloc(32 * ORC_BLOB_N);
+    if (blob_to_coeffs(blob_be, c)) {
+        free(c);
+        return -1;
+    }
+    fe zm = f_to_mont(F, z);
+    fe* a = (fe*)malloc(ORC_BLOB_N * sizeof(fe));
+    for (int k = 0; k < ORC_BLOB_N; ++k) a[k] = f_to_mont(F, fe_from_le(F, c + 32 * k));
+    /* synthetic division: q_{k-1} = a_k + z q_k, remainder a_0 + z q_0 = y */
+    fe acc = a[ORC_BLOB_N - 1];
+    memset(c, 0, 32 * ORC_BLOB_N);
+    for (int k = ORC_BLOB_N - 1; k >= 1; --k) {
+        fe q = acc; /* q_{k-1} */
+        fe qc = f_from_mont(F, q);
+        fe_to_le(F, &qc, c + 32 * (k - 1));
+        acc = f_add(F, a[k - 1], f_mul(F, zm, q));
+    }
+    fe y = f_from_mont(F, acc);
+    fe_to_be(F, &y, y_be);
+    uint8_t pt[96];
+    orc_msm(ORC_CURVE_BLS12_381, c, srs, ORC_BLOB_N, pt);
+    free(a);
+    free(c);
+    return orc_g1_compress(pt, proof48);
+}

@@ -98,6 +98,15 @@ int orc_fr_powers(uint32_t curve, const uint8_t* tau, size_t n, uint8_t* out);
  * skipped. */
 int orc_bls12_381_g1_msm(uint8_t rx[64], uint8_t ry[64], const uint8_t* xycs, size_t size);
 
+/* EIP-4844 blob commitment / opening proof (kzg/c-abi/c_kzg_blob.cpp:26-43)
+ * against a monomial setup srs = [tau^i]G1, i < 4096 (96 B BE each): blob =
+ * 4096 x 32 B big-endian elements in bit-reversed evaluation order; z and y
+ * 32 B big-endian; commitment and proof 48 B compressed.  Returns 0, or -1
+ * if an element or z is not below r. */
+int orc_kzg_blob_commit(const uint8_t* blob_be, const uint8_t* srs, uint8_t commit48[48]);
+int orc_kzg_blob_proof(const uint8_t* blob_be, const uint8_t z_be[32], const uint8_t* srs,
+                       uint8_t proof48[48], uint8_t y_be[32]);
+
 /* Word-prime NTT with the contract of the reference's ntt_forward /
  * ntt_inverse (ntt/c-abi/c_ntt.cpp:81-179): in place on n uint64 words;
  * n <= 2^16 natural order (Cyclone prime 998244353 with its pinned root on

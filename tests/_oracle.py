@@ -46,6 +46,9 @@ def orc() -> ctypes.CDLL:
             "orc_field_mul": [ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_void_p],
             "orc_field_inv": [ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p],
             "orc_bls12_381_g1_msm": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p, sz],
+            "orc_kzg_blob_commit": [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_void_p],
+            "orc_kzg_blob_proof": [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_void_p,
+                                   ctypes.c_void_p],
             "orc_word_ntt_forward": [ctypes.c_void_p, sz, ctypes.c_uint64, ctypes.c_uint64],
             "orc_word_ntt_inverse": [ctypes.c_void_p, sz, ctypes.c_uint64, ctypes.c_uint64],
         }.items():
@@ -162,6 +165,19 @@ def bls12_381_g1_msm(xycs: bytes):
     ry = ctypes.create_string_buffer(64)
     rc = orc().orc_bls12_381_g1_msm(rx, ry, xycs, len(xycs))
     return rc, rx.raw + ry.raw
+
+
+def kzg_blob_commit(blob: bytes, srs: bytes):
+    out = ctypes.create_string_buffer(48)
+    rc = orc().orc_kzg_blob_commit(blob, srs, out)
+    return rc, out.raw
+
+
+def kzg_blob_proof(blob: bytes, z: bytes, srs: bytes):
+    proof = ctypes.create_string_buffer(48)
+    y = ctypes.create_string_buffer(32)
+    rc = orc().orc_kzg_blob_proof(blob, z, srs, proof, y)
+    return rc, proof.raw, y.raw
 
 
 def word_ntt(words, q: int, root: int, inverse: bool = False):
