@@ -200,7 +200,9 @@ def bench_extra(args, peak_imad: float) -> dict:
     """The other single-transform configurations: BLS12-381 MSM 2^20, BN254 MSM
     2^24 (uniform and skewed scalars), BLS12-381 Fr NTT 2^24 forward + inverse,
     BN254 coset NTT 2^26 forward + inverse, word-prime NTT 2^20 (Goldilocks and
-    Cyclone-FFT primes).  Device-resident inputs."""
+    Cyclone-FFT primes), the EIP-2537 G1 MSM at 2^16 entries and the EIP-4844
+    blob commitment and proof.  Device-resident inputs unless a case says
+    otherwise."""
     import torch
     import crypto_b200 as kb
     L = kb.lib()
@@ -291,6 +293,62 @@ def bench_extra(args, peak_imad: float) -> dict:
         del d
         torch.cuda.empty_cache()
 
+    def eip2537_case(logn, label):
+        """bls12_381_g1_msm (EIP-2537 input: 160-byte entries, all checks)
+        through the host C ABI, against the plain MSM of the same points."""
+        import numpy as np
+        n = 1 << logn
+        ks = kb.gen_scalars(2, 91 + logn, n)
+        d_ks = torch.frombuffer(bytearray(ks), dtype=torch.uint8).cuda()
+        d_pts = torch.empty(n * 96, dtype=torch.uint8, device="cuda")
+        assert L.kb200_g1_fixed_base_device(2, d_ks.data_ptr(), n, d_pts.data_ptr(), sp) == 0
+        pts = d_pts.cpu().numpy().reshape(n, 96)
+        sc = np.frombuffer(kb.gen_scalars(2, 92 + logn, n), dtype=np.uint8).reshape(n, 32)
+        ent = np.zeros((n, 160), dtype=np.uint8)
+        ent[:, 16:64] = pts[:, :48]
+        ent[:, 80:128] = pts[:, 48:]
+        ent[:, 128:] = sc[:, ::-1]  # little-endian scalars -> big-endian
+        xycs = ent.tobytes()
+        rx = ctypes.create_string_buffer(64)
+        ry = ctypes.create_string_buffer(64)
+        assert L.bls12_381_g1_msm(rx, ry, xycs, len(xycs)) == 1
+        reps = 3
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            assert L.bls12_381_g1_msm(rx, ry, xycs, len(xycs)) == 1
+        ms = (time.perf_counter() - t0) * 1e3 / reps
+        want = kb.gpukit_multi_pippenger(2, sc.tobytes(), pts.tobytes(), n)
+        assert rx.raw[16:] + ry.raw[16:] == want, "EIP-2537 MSM differs from the plain MSM"
+        out[label] = {"n": n, "e2e_ms": ms, "mpts_per_s": n / ms / 1e3,
+                      "api": "bls12_381_g1_msm (host entries; range, curve and G1 checks included)"}
+        del d_ks, d_pts
+        torch.cuda.empty_cache()
+
+    def blob_case(label):
+        """kzg_blob_to_commit and kzg_commit_to_proof on one 4096-element blob
+        over a resident test setup (host C ABI, copies included)."""
+        import random
+        r = 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001
+        rng = random.Random(9)
+        assert L.kzg_blob_setup_generate((12345).to_bytes(32, "little")) == 0
+        blob = b"".join(rng.randrange(r).to_bytes(32, "big") for _ in range(4096))
+        z = rng.randrange(r).to_bytes(32, "big")
+        c = ctypes.create_string_buffer(48)
+        pr = ctypes.create_string_buffer(48)
+        y = ctypes.create_string_buffer(32)
+        assert L.kzg_blob_to_commit(blob, c) == 0 and L.kzg_commit_to_proof(blob, z, pr, y) == 0
+        reps = 20
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            assert L.kzg_blob_to_commit(blob, c) == 0
+        commit_ms = (time.perf_counter() - t0) * 1e3 / reps
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            assert L.kzg_commit_to_proof(blob, z, pr, y) == 0
+        proof_ms = (time.perf_counter() - t0) * 1e3 / reps
+        out[label] = {"blob_to_commit_ms": commit_ms, "commit_to_proof_ms": proof_ms,
+                      "api": "kzg_blob_to_commit / kzg_commit_to_proof (host, synchronous)"}
+
     msm_case(2, 20, 0, "msm_bls12_381_2^20")
     msm_case(1, 24, 0, "msm_bn254_2^24_uniform")
     msm_case(1, 24, 1, "msm_bn254_2^24_skewed")
@@ -298,6 +356,8 @@ def bench_extra(args, peak_imad: float) -> dict:
     ntt_case(1, 26, 1, "ntt_bn254_2^26_coset")
     word_ntt_case(0xFFFFFFFF00000001, 7, 20, "word_ntt_goldilocks_2^20")
     word_ntt_case(998244353, 3, 20, "word_ntt_cyclone_2^20")
+    eip2537_case(16, "eip2537_g1_msm_2^16")
+    blob_case("eip4844_blob_4096")
     return out
 
 
