@@ -1,5 +1,6 @@
 // Batched KZG commits: see batch.cuh.
 #include "batch.cuh"
+#include "kzg.cuh"
 #include "msm.cuh"
 #include "ntt.cuh"
 #include "runtime.cuh"
@@ -16,8 +17,10 @@ namespace {
 struct Signature {
     std::vector<size_t> sizes;
     const uint32_t* srs;
+    uint64_t shift_gen;  // shifted-table generation (0 = none)
     bool operator<(const Signature& o) const {
         if (srs != o.srs) return srs < o.srs;
+        if (shift_gen != o.shift_gen) return shift_gen < o.shift_gen;
         return sizes < o.sizes;
     }
 };
@@ -28,6 +31,7 @@ struct Prepared {
     std::vector<size_t> class_off;                   // start in the offsets list
     DevBuf d_vec_off;                                // element offsets grouped by class
     size_t total = 0;                                // evaluations
+    const uint32_t* table = nullptr;                 // MSM table (SRS or its shifted levels)
     cudaGraphExec_t graph = nullptr;
     ~Prepared() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -46,6 +50,7 @@ class CommitBatcher {
     HostBuf h_out;
     std::map<Signature, std::unique_ptr<Prepared>> cache;
     Prepared* current = nullptr;
+    ShiftTables* shifts = nullptr;
     unsigned long long graph_launches = 0, graph_captures = 0;
     ~CommitBatcher() {
         cache.clear();
@@ -65,9 +70,13 @@ CommitBatcher* commit_batcher_create() {
 
 void commit_batcher_destroy(CommitBatcher* b) { delete b; }
 
+void commit_batcher_set_shift(CommitBatcher* b, ShiftTables* shifts) { b->shifts = shifts; }
+
 static Prepared* prepare(CommitBatcher* B, const size_t* sizes, size_t count,
                          const uint32_t* srs, size_t srs_n, cudaStream_t st) {
-    Signature sig{std::vector<size_t>(sizes, sizes + count), srs};
+    const bool shifted = B->shifts && shift_tables_stride(B->shifts) == srs_n;
+    Signature sig{std::vector<size_t>(sizes, sizes + count), srs,
+                  shifted ? shift_tables_generation(B->shifts) : 0};
     auto it = B->cache.find(sig);
     if (it != B->cache.end()) return it->second.get();
     auto P = std::make_unique<Prepared>();
@@ -95,6 +104,15 @@ static Prepared* prepare(CommitBatcher* B, const size_t* sizes, size_t count,
         KB_CUDA(cudaMemcpyAsync(P->d_vec_off.ptr, offs.data(), offs.size() * 8,
                                 cudaMemcpyHostToDevice, st));
     MsmOptions opt;
+    P->table = srs;
+    if (shifted) {
+        const int c = shift_c_for(sizes, count);
+        if (const uint32_t* t = shift_tables_get(B->shifts, c, st)) {
+            opt.shift_c = c;
+            opt.shift_stride = srs_n;
+            P->table = t;
+        }
+    }
     P->plan = msm_batch_plan_create(2, items.data(), count, opt, st);
     msm_engine_reserve(B->msm, P->plan, st);
     B->evals.reserve(std::max<size_t>(1, off) * 32 + 16, st);
@@ -125,7 +143,8 @@ static void enqueue(CommitBatcher* B, Prepared* P, const uint32_t* srs, cudaStre
                      P->d_vec_off.as<unsigned long long>() + P->class_off[k],
                      B->scratch.as<uint32_t>(), st);
     }
-    msm_engine_launch(B->msm, P->plan, B->evals.as<uint8_t>(), srs, B->out_wire.as<uint8_t>(),
+    (void)srs;
+    msm_engine_launch(B->msm, P->plan, B->evals.as<uint8_t>(), P->table, B->out_wire.as<uint8_t>(),
                       B->out_comp.as<uint8_t>(), st);
 }
 

@@ -18,8 +18,11 @@
 namespace kb200 {
 
 class CommitBatcher;
+struct ShiftTables;
 CommitBatcher* commit_batcher_create();
 void commit_batcher_destroy(CommitBatcher* b);
+// Shifted tables over the SRS the batcher is given (null = plain MSMs).
+void commit_batcher_set_shift(CommitBatcher* b, ShiftTables* shifts);
 
 // Commits `count` polynomials.  h_evals: host evaluations (32 B LE each,
 // back to back in the order of sizes); h_out: 48 * count bytes.  srs_table:

@@ -42,6 +42,11 @@ struct DeviceCtx {
     FixedBase* fb[3] = {nullptr, nullptr, nullptr};
     CommitBatcher* batcher = nullptr;
     WordNttCache* wntt = nullptr;
+    ShiftTables* srs_shift = nullptr;  // shifted levels of d_srs
+    ShiftTables* srs_shift_get() {
+        if (!srs_shift) srs_shift = shift_tables_create();
+        return srs_shift;
+    }
     BlobSetup* blob = nullptr;
     DevBuf d_bl;  // blob ops: input, z, outputs, flag
     BlobSetup* blob_get() {
@@ -69,7 +74,10 @@ struct DeviceCtx {
         return wntt;
     }
     CommitBatcher* batcher_get() {
-        if (!batcher) batcher = commit_batcher_create();
+        if (!batcher) {
+            batcher = commit_batcher_create();
+            commit_batcher_set_shift(batcher, srs_shift_get());
+        }
         return batcher;
     }
 };
@@ -116,6 +124,12 @@ static int guarded(int backend_err, int size_err, int internal_err, Fn&& fn) {
         set_last_error(e.what());
         return internal_err;
     }
+}
+
+ShiftTables* resident_srs_shifts() {
+    DeviceCtx* c = get_ctx();
+    std::lock_guard<std::mutex> lk(c->mu);
+    return c->srs_shift_get();
 }
 
 void resident_srs(const uint32_t** table, size_t* n) {
@@ -350,8 +364,15 @@ static void commit_on_device(DeviceCtx* c, uint32_t* d_evals, size_t n, uint8_t*
     ntt_run(c->ntt_for(2), d_evals, n, /*inverse=*/1, /*coset=*/0, 1, st);
     c->d_tmp.reserve(256, st);
     MsmOptions opt;
-    msm_run_table(c->msm_for(2), reinterpret_cast<const uint8_t*>(d_evals),
-                  c->d_srs.as<uint32_t>(), n, c->d_tmp.as<uint8_t>(), d_out48, st, opt);
+    const uint32_t* table = c->d_srs.as<uint32_t>();
+    const int sc = shift_c_for(&n, 1);
+    if (const uint32_t* t = shift_tables_get(c->srs_shift_get(), sc, st)) {
+        opt.shift_c = sc;
+        opt.shift_stride = c->srs_n;
+        table = t;
+    }
+    msm_run_table(c->msm_for(2), reinterpret_cast<const uint8_t*>(d_evals), table, n,
+                  c->d_tmp.as<uint8_t>(), d_out48, st, opt);
 }
 
 }  // namespace kb200
@@ -394,6 +415,7 @@ int kzg_srs_load_g1(const uint8_t* points96be, size_t n) {
                        }
                        KB_CUDA(cudaStreamSynchronize(st));
                        c->srs_n = n;
+                       shift_tables_reset(c->srs_shift_get(), c->d_srs.as<uint32_t>(), n);
                        return KB200_CRYPTO_OK;
                    });
 }
@@ -414,6 +436,7 @@ int kzg_srs_generate_g1(const uint8_t tau32le[32], size_t n) {
                                       nullptr, st);
                        KB_CUDA(cudaStreamSynchronize(st));
                        c->srs_n = n;
+                       shift_tables_reset(c->srs_shift_get(), c->d_srs.as<uint32_t>(), n);
                        return KB200_CRYPTO_OK;
                    });
 }

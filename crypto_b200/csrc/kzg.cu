@@ -1,6 +1,10 @@
 // Fixed-base G1 multiplication and Fr powers.  See kzg.cuh.
 #include "curve.cuh"
 #include "kzg.cuh"
+#include "msm.cuh"
+
+#include <map>
+#include <mutex>
 #include "runtime.cuh"
 
 namespace kb200 {
@@ -125,7 +129,102 @@ __global__ void k_fr_powers(const uint8_t* __restrict__ tau, size_t n, uint8_t* 
     for (int k = 0; k < F::N; ++k) o[k] = acc.v[k];
 }
 
+// Levels 1..W-1 of a shifted table: level w row i = [2^(c w)] (base row i).
+// One thread per point: c doublings per level, then an affine conversion.
+__global__ void __launch_bounds__(128) k_shift_levels(const uint32_t* __restrict__ base, size_t n,
+                                                      int c, int W, uint32_t* __restrict__ out) {
+    using F = FpBLS;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t* src = base + i * 2 * F::N;
+    for (int k = 0; k < 2 * F::N; ++k) out[i * 2 * F::N + k] = src[k];
+    const bool inf = aff_is_inf_words<F>(src);
+    Affine<F> a;
+    aff_load(a, src);
+    Xyzz<F> p;
+    xyzz_from_affine(p, a);
+    for (int w = 1; w < W; ++w) {
+        uint32_t* dst = out + ((size_t)w * n + i) * 2 * F::N;
+        if (!inf)
+            for (int k = 0; k < c; ++k) xyzz_dbl(p, p);
+        Affine<F> r;
+        if (inf || !xyzz_to_affine(r, p)) {
+            for (int k = 0; k < 2 * F::N; ++k) dst[k] = 0;
+            dst[F::N - 1] = INF_FLAG;
+        } else {
+            fe_store(dst, r.x);
+            fe_store(dst + F::N, r.y);
+        }
+    }
+}
+
 }  // namespace
+
+struct ShiftTables {
+    const uint32_t* base = nullptr;
+    size_t n = 0;
+    uint64_t generation = 0;
+    std::map<int, DevBuf> levels;
+    std::mutex mu;
+};
+
+ShiftTables* shift_tables_create() { return new ShiftTables(); }
+
+void shift_tables_destroy(ShiftTables* t) {
+    if (!t) return;
+    for (auto& kv : t->levels) kv.second.release();
+    delete t;
+}
+
+void shift_tables_reset(ShiftTables* t, const uint32_t* d_base, size_t n) {
+    std::lock_guard<std::mutex> lk(t->mu);
+    for (auto& kv : t->levels) kv.second.release();  // cudaFree waits for the device
+    t->levels.clear();
+    t->base = d_base;
+    t->n = n;
+    ++t->generation;
+}
+
+uint64_t shift_tables_generation(const ShiftTables* t) { return t->generation; }
+size_t shift_tables_stride(const ShiftTables* t) { return t->n; }
+
+// Cap on one shifted table (HBM is 180 GB; a 2^20-point table at c = 20 is 1.3 GB).
+constexpr size_t SHIFT_TABLE_MAX_BYTES = (size_t)8 << 30;
+
+const uint32_t* shift_tables_get(ShiftTables* t, int c, cudaStream_t st) {
+    std::lock_guard<std::mutex> lk(t->mu);
+    if (!t->base || t->n == 0 || c < 2) return nullptr;
+    auto it = t->levels.find(c);
+    if (it != t->levels.end()) return it->second.as<uint32_t>();
+    const int W = msm_windows_for(c);
+    const size_t bytes = (size_t)W * t->n * 2 * FpBLS::N * 4;
+    if (bytes > SHIFT_TABLE_MAX_BYTES) return nullptr;
+    DevBuf& b = t->levels[c];
+    b.reserve(bytes, st);
+    k_shift_levels<<<ceil_div_u(t->n, 128), 128, 0, st>>>(t->base, t->n, c, W, b.as<uint32_t>());
+    KB_LAUNCH_CHECK();
+    KB_CUDA(cudaStreamSynchronize(st));  // usable from any stream once returned
+    return b.as<uint32_t>();
+}
+
+int shift_c_for(const size_t* sizes, size_t count) {
+    // Accumulation: one mixed addition per entry over the windows canonical
+    // scalars populate; reduction: ~2.8 additions per bucket of the single
+    // shared window of each item.  Only four window sizes are offered, so a
+    // resident setup carries at most four shifted tables.
+    int best_c = 13;
+    double best = 1e300;
+    for (int c : {10, 13, 16, 19}) {
+        const double wl = (double)((255 + c - 1) / c);
+        double cost = 0;
+        for (size_t i = 0; i < count; ++i) cost += wl * (double)sizes[i] + 2.8 * (double)(1u << (c - 1));
+        if (cost < best) {
+            best = cost;
+            best_c = c;
+        }
+    }
+    return best_c;
+}
 
 struct FixedBase {
     int curve;

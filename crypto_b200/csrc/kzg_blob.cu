@@ -358,10 +358,28 @@ struct BlobSetup {
     DevBuf p_mont, p_le, inv, term, q_le, misc, sum, y_mont, wire;
     bool ready = false;
     bool roots_ready = false;
+    ShiftTables* shifts = shift_tables_create();  // shifted levels of `table`
+    ~BlobSetup() { shift_tables_destroy(shifts); }
 };
 
 BlobSetup* blob_setup_create() { return new BlobSetup(); }
 void blob_setup_destroy(BlobSetup* s) { delete s; }
+
+// The MSM against the setup: through its shifted levels (one shared bucket
+// window per blob, no doubling chain), or the plain table if unavailable.
+static void blob_msm(BlobSetup* s, MsmEngine* eng, const uint8_t* d_scalars, uint8_t* d_out48,
+                     cudaStream_t st) {
+    MsmOptions opt;
+    const uint32_t* table = s->table.as<uint32_t>();
+    const size_t n = BLOB_N;
+    const int c = shift_c_for(&n, 1);
+    if (const uint32_t* t = shift_tables_get(s->shifts, c, st)) {
+        opt.shift_c = c;
+        opt.shift_stride = BLOB_N;
+        table = t;
+    }
+    msm_run_table(eng, d_scalars, table, BLOB_N, s->wire.as<uint8_t>(), d_out48, st, opt);
+}
 bool blob_setup_ready(const BlobSetup* s) { return s && s->ready; }
 
 static void ensure_buffers(BlobSetup* s, cudaStream_t st) {
@@ -388,6 +406,7 @@ void blob_setup_load_lagrange(BlobSetup* s, const uint8_t* d_pts48, uint32_t* d_
     KB_CUDA(cudaMemsetAsync(d_flag, 0, 4, st));
     k_setup_decompress<<<BLOB_N / 128, 128, 0, st>>>(d_pts48, s->table.as<uint32_t>(), d_flag);
     KB_LAUNCH_CHECK();
+    shift_tables_reset(s->shifts, s->table.as<uint32_t>(), BLOB_N);
     s->ready = true;  // the caller clears it if the flag comes back set
 }
 
@@ -399,6 +418,7 @@ void blob_setup_generate(BlobSetup* s, FixedBase* fb, const uint8_t* d_tau_le, c
                                                      s->q_le.as<uint8_t>());
     KB_LAUNCH_CHECK();
     fixed_base_mul(fb, s->q_le.as<uint8_t>(), BLOB_N, s->table.as<uint32_t>(), nullptr, st);
+    shift_tables_reset(s->shifts, s->table.as<uint32_t>(), BLOB_N);
     s->ready = true;
 }
 
@@ -409,9 +429,7 @@ void blob_commit_device(BlobSetup* s, MsmEngine* eng, const uint8_t* d_blob, uin
     k_blob_load<<<BLOB_N / 128, 128, 0, st>>>(d_blob, s->p_mont.as<uint32_t>(), s->p_le.as<uint8_t>(),
                                               d_flag);
     KB_LAUNCH_CHECK();
-    MsmOptions opt;
-    msm_run_table(eng, s->p_le.as<uint8_t>(), s->table.as<uint32_t>(), BLOB_N, s->wire.as<uint8_t>(),
-                  d_commit48, st, opt);
+    blob_msm(s, eng, s->p_le.as<uint8_t>(), d_commit48, st);
 }
 
 void blob_proof_device(BlobSetup* s, MsmEngine* eng, const uint8_t* d_blob, const uint8_t* d_z_be,
@@ -434,9 +452,7 @@ void blob_proof_device(BlobSetup* s, MsmEngine* eng, const uint8_t* d_blob, cons
     k_blob_sum<<<1, RED_T, 0, st>>>(s->term.as<uint32_t>(), s->sum.as<uint32_t>());
     k_blob_qm<<<1, 1, 0, st>>>(s->sum.as<uint32_t>(), misc, s->q_le.as<uint8_t>());
     KB_LAUNCH_CHECK();
-    MsmOptions opt;
-    msm_run_table(eng, s->q_le.as<uint8_t>(), s->table.as<uint32_t>(), BLOB_N, s->wire.as<uint8_t>(),
-                  d_proof48, st, opt);
+    blob_msm(s, eng, s->q_le.as<uint8_t>(), d_proof48, st);
 }
 
 }  // namespace kb200

@@ -131,6 +131,7 @@ int reference_best_c(size_t n) {
 }
 
 static int windows_for(int c) { return (257 + c - 1) / c; }
+int msm_windows_for(int c) { return windows_for(c); }
 
 // Live buckets of the top window: its raw digit has 256 - c(W-1) bits plus a
 // carry, so its largest magnitude is 2^(256 - c(W-1)).
@@ -226,7 +227,16 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         if (n >= (1ull << 31) || items[i].point_off + n >= (1ull << 31))
             throw std::invalid_argument("msm: more than 2^31 points");
         max_n = std::max(max_n, n);
-        plans[i] = make_msm_plan(curve, n, opt);
+        if (opt.shift_c > 0) {
+            MsmOptions o2 = opt;
+            o2.force_c = opt.shift_c;
+            plans[i] = make_msm_plan(curve, n, o2);
+            if (items[i].point_off + n > opt.shift_stride ||
+                (unsigned long long)plans[i].W * opt.shift_stride >= (1ull << 31))
+                throw std::invalid_argument("msm: item outside the shifted table");
+        } else {
+            plans[i] = make_msm_plan(curve, n, opt);
+        }
         ItemDesc& d = P.items[i];
         d.scalar_off = items[i].scalar_off;
         d.n = (uint32_t)n;
@@ -235,11 +245,14 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         d.c = (uint32_t)plans[i].c;
         d.M = plans[i].M;
         d.W = n ? (uint32_t)plans[i].W : 0u;
-        if (n) total_live += (size_t)(d.W - 1) * d.M + plans[i].M_top;
+        const bool shifted = opt.shift_c > 0;
+        d.row_stride = shifted ? (uint32_t)opt.shift_stride : 0u;
+        d.Wr = shifted ? (n ? 1u : 0u) : d.W;
+        if (n) total_live += shifted ? d.M : (size_t)(d.W - 1) * d.M + plans[i].M_top;
         d.entry_base = L;
         d.bucket_base = (uint32_t)B;
         L += (unsigned long long)d.W * n;
-        B += (unsigned long long)d.W * d.M;
+        B += (unsigned long long)d.Wr * d.M;
         tot_sc = std::max<unsigned long long>(tot_sc, d.scalar_off + n);
     }
     if (B >= 0xffffffffull || L >= 0xffffffffull)
@@ -260,16 +273,16 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
     for (size_t i = 0; i < count; ++i) {
         ItemDesc& d = P.items[i];
         d.win_base = (uint32_t)P.wins.size();
-        for (uint32_t w = 0; w < d.W; ++w) {
+        for (uint32_t w = 0; w < d.Wr; ++w) {
             WinDesc wd;
             wd.bucket_base = d.bucket_base + w * d.M;
-            wd.Mw = (w == d.W - 1) ? plans[i].M_top : d.M;
+            wd.Mw = d.row_stride ? d.M : ((w == d.W - 1) ? plans[i].M_top : d.M);
             uint32_t ls = (uint32_t)log_S;
             while (((wd.Mw + (RED_THREADS << ls) - 1) >> (8 + ls)) > (uint32_t)RED_THREADS) ++ls;
             wd.log_S = ls;
             wd.log_blk = 8 + ls;
             wd.nb = (wd.Mw + (1u << wd.log_blk) - 1) >> wd.log_blk;
-            wd.shift = d.c * w;
+            wd.shift = d.row_stride ? 0u : d.c * w;
             wd.blk_base = (uint32_t)P.blks.size();
             for (uint32_t b = 0; b < wd.nb; ++b)
                 P.blks.push_back(BlkDesc{(uint32_t)P.wins.size(), b});
@@ -342,7 +355,7 @@ class MsmEngine {
     int curve = 0;
     DevBuf table, keys, vals, counts, offsets, cursor, sorted, rec_first, rec_last, fold_buf,
         buckets, blk_out, win_out, scan_tmp, queue, fold_counts, fold_prefix;
-    std::map<std::tuple<size_t, bool, int, int>, MsmBatchPlan*> single_plans;
+    std::map<std::tuple<size_t, bool, int, int, int, size_t>, MsmBatchPlan*> single_plans;
     cudaEvent_t ev[N_STAGE_EVENTS] = {};
     bool ev_ready = false, ev_recorded = false;
     void mark(int i, cudaStream_t st) {
@@ -524,7 +537,8 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
 }
 
 static MsmBatchPlan* single_plan(MsmEngine* e, size_t n, const MsmOptions& opt, cudaStream_t st) {
-    auto key = std::make_tuple(n, opt.ref_carry_quirk, opt.force_c, opt.force_K);
+    auto key = std::make_tuple(n, opt.ref_carry_quirk, opt.force_c, opt.force_K, opt.shift_c,
+                               opt.shift_stride);
     auto it = e->single_plans.find(key);
     if (it != e->single_plans.end()) return it->second;
     MsmItem item{0, n, 0};

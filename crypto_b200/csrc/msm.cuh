@@ -47,7 +47,18 @@ struct MsmOptions {
     bool ref_carry_quirk = false;
     int force_c = 0;  // 0 = autotuned / cost model
     int force_K = 0;
+    // Shifted fixed-base table: the table passed to the launch holds
+    // msm_windows_for(shift_c) levels of shift_stride rows, level w row i =
+    // [2^(shift_c * w)] (row i of level 0).  Every item then uses window
+    // size shift_c and one bucket range shared by all its windows: no
+    // per-window reduction and no doubling chain in the combine.
+    // 0 = plain table.
+    int shift_c = 0;
+    size_t shift_stride = 0;
 };
+
+// Windows of a c-bit signed-digit decomposition of 256-bit scalars.
+int msm_windows_for(int c);
 
 // Reference window size for n: multi_pippenger.cpp:69-88.
 int reference_best_c(size_t n);

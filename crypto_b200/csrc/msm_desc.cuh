@@ -21,6 +21,8 @@ struct ItemDesc {
     uint32_t bucket_base;           // first global bucket of the item
     uint32_t win_base;              // first WinDesc of the item
     int32_t quirk_c;                // reference carry emulation (0, 4 or 8)
+    uint32_t row_stride;            // shifted table: rows per level (0 = plain table)
+    uint32_t Wr;                    // windows reduced and combined (W, or 1 when shifted)
 };
 
 // One window of one item.

@@ -117,6 +117,11 @@ __global__ void k_recode(const ItemDesc* __restrict__ items, uint32_t n_items,
         const unsigned long long slot = it.entry_base + (unsigned long long)w * it.n + j;
         if (d == 0 || inf) {
             keys[slot] = KEY_SENTINEL;
+        } else if (it.row_stride) {
+            // shifted table: level w holds 2^(c*w) times the point, so every
+            // window feeds the same buckets
+            keys[slot] = it.bucket_base + (d - 1);
+            vals[slot] = (row + (uint32_t)w * it.row_stride) | ((sign ^ neg) << 31);
         } else {
             keys[slot] = it.bucket_base + (uint32_t)w * M + (d - 1);
             vals[slot] = row | ((sign ^ neg) << 31);
@@ -484,8 +489,8 @@ __global__ void k_combine(const ItemDesc* __restrict__ items, uint32_t n_items,
         xyzz_set_inf(acc);
     } else {
         // windows arrive already weighted by 2^(c*w): a plain sum
-        xyzz_load(acc, wins + (size_t)(it.win_base + it.W - 1) * PW);
-        for (int w = (int)it.W - 2; w >= 0; --w) {
+        xyzz_load(acc, wins + (size_t)(it.win_base + it.Wr - 1) * PW);
+        for (int w = (int)it.Wr - 2; w >= 0; --w) {
             xyzz_load(t, wins + (size_t)(it.win_base + (uint32_t)w) * PW);
             xyzz_add(acc, t);
         }

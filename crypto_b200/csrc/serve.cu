@@ -16,6 +16,7 @@
 // in any mix.
 #include "../../include/kinet_b200/crypto_b200.h"
 #include "batch.cuh"
+#include "kzg.cuh"
 #include "runtime.cuh"
 
 #include <algorithm>
@@ -33,6 +34,7 @@ namespace kb200 {
 
 // Resident SRS of the calling thread's device (owned by the C-ABI context).
 void resident_srs(const uint32_t** table, size_t* n);
+ShiftTables* resident_srs_shifts();
 
 namespace {
 
@@ -213,6 +215,7 @@ void* kzg_server_create(size_t max_batch, int slots, size_t mem_budget_bytes) {
             KB_CUDA(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
             KB_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
             sl.batcher = commit_batcher_create();
+            commit_batcher_set_shift(sl.batcher, resident_srs_shifts());
         }
         s->worker = std::thread([s] { s->loop(); });
         return s;
