@@ -25,17 +25,22 @@ struct Signature {
     }
 };
 
-struct Prepared {
+struct MsmGroup {
     MsmBatchPlan* plan = nullptr;
+    const uint32_t* table = nullptr;  // SRS, or its shifted levels for the group's window size
+};
+
+struct Prepared {
+    std::vector<MsmGroup> groups;                    // the first ngroups are in use
+    size_t ngroups = 0;
     std::vector<std::pair<size_t, size_t>> classes;  // (n, count) per size class
     std::vector<size_t> class_off;                   // start in the offsets list
     DevBuf d_vec_off;                                // element offsets grouped by class
     size_t total = 0;                                // evaluations
-    const uint32_t* table = nullptr;                 // MSM table (SRS or its shifted levels)
     cudaGraphExec_t graph = nullptr;
     ~Prepared() {
         if (graph) cudaGraphExecDestroy(graph);
-        if (plan) msm_batch_plan_destroy(plan);
+        for (MsmGroup& g : groups) msm_batch_plan_destroy(g.plan);
         d_vec_off.release();
     }
 };
@@ -51,6 +56,11 @@ class CommitBatcher {
     std::map<Signature, std::unique_ptr<Prepared>> cache;
     Prepared* current = nullptr;
     ShiftTables* shifts = nullptr;
+    // Transient mode (serving, where batch signatures rarely repeat): one
+    // Prepared is rebuilt in place for every batch, reusing its device
+    // buffers, instead of caching (and later freeing) one per signature.
+    bool transient = false;
+    std::unique_ptr<Prepared> scratch_prep;
     unsigned long long graph_launches = 0, graph_captures = 0;
     ~CommitBatcher() {
         cache.clear();
@@ -71,15 +81,26 @@ CommitBatcher* commit_batcher_create() {
 void commit_batcher_destroy(CommitBatcher* b) { delete b; }
 
 void commit_batcher_set_shift(CommitBatcher* b, ShiftTables* shifts) { b->shifts = shifts; }
+void commit_batcher_set_transient(CommitBatcher* b, bool transient) { b->transient = transient; }
 
 static Prepared* prepare(CommitBatcher* B, const size_t* sizes, size_t count,
                          const uint32_t* srs, size_t srs_n, cudaStream_t st) {
     const bool shifted = B->shifts && shift_tables_stride(B->shifts) == srs_n;
     Signature sig{std::vector<size_t>(sizes, sizes + count), srs,
                   shifted ? shift_tables_generation(B->shifts) : 0};
-    auto it = B->cache.find(sig);
-    if (it != B->cache.end()) return it->second.get();
-    auto P = std::make_unique<Prepared>();
+    std::unique_ptr<Prepared> fresh;
+    Prepared* P;
+    if (B->transient) {
+        if (!B->scratch_prep) B->scratch_prep = std::make_unique<Prepared>();
+        P = B->scratch_prep.get();
+        P->classes.clear();
+        P->class_off.clear();
+    } else {
+        auto it = B->cache.find(sig);
+        if (it != B->cache.end()) return it->second.get();
+        fresh = std::make_unique<Prepared>();
+        P = fresh.get();
+    }
     std::vector<MsmItem> items(count);
     std::map<size_t, std::vector<unsigned long long>> by_size;
     size_t off = 0;
@@ -103,26 +124,49 @@ static Prepared* prepare(CommitBatcher* B, const size_t* sizes, size_t count,
     if (!offs.empty())
         KB_CUDA(cudaMemcpyAsync(P->d_vec_off.ptr, offs.data(), offs.size() * 8,
                                 cudaMemcpyHostToDevice, st));
-    MsmOptions opt;
-    P->table = srs;
-    if (shifted) {
-        const int c = shift_c_for(sizes, count);
-        if (const uint32_t* t = shift_tables_get(B->shifts, c, st)) {
-            opt.shift_c = c;
-            opt.shift_stride = srs_n;
-            P->table = t;
-        }
+    // MSM groups: against shifted tables every commit joins the group of its
+    // own best window size (results go to its slot through out_index), so a
+    // large commit does not impose its window on the small ones; otherwise
+    // one plain plan for the whole batch.
+    std::map<int, std::vector<MsmItem>> by_c;
+    for (size_t i = 0; i < count; ++i) {
+        MsmItem it = items[i];
+        it.out_index = i;
+        by_c[shifted ? shift_c_for(&sizes[i], 1) : 0].push_back(it);
     }
-    P->plan = msm_batch_plan_create(2, items.data(), count, opt, st);
-    msm_engine_reserve(B->msm, P->plan, st);
+    P->ngroups = 0;
+    for (auto& kv : by_c) {
+        MsmOptions opt;
+        const uint32_t* table = srs;
+        if (kv.first > 0) {
+            if (const uint32_t* t = shift_tables_get(B->shifts, kv.first, st)) {
+                opt.shift_c = kv.first;
+                opt.shift_stride = srs_n;
+                table = t;
+            }
+        }
+        if (P->ngroups < P->groups.size()) {
+            MsmGroup& g = P->groups[P->ngroups];
+            msm_batch_plan_update(g.plan, kv.second.data(), kv.second.size(), opt, st);
+            g.table = table;
+        } else {
+            MsmGroup g;
+            g.table = table;
+            g.plan = msm_batch_plan_create(2, kv.second.data(), kv.second.size(), opt, st);
+            P->groups.push_back(g);
+        }
+        msm_engine_reserve(B->msm, P->groups[P->ngroups].plan, st);
+        ++P->ngroups;
+    }
     B->evals.reserve(std::max<size_t>(1, off) * 32 + 16, st);
     B->scratch.reserve(std::max<size_t>(1, off) * 32 + 16, st);
     B->out_wire.reserve(std::max<size_t>(1, count) * 96, st);
     B->out_comp.reserve(std::max<size_t>(1, count) * 48, st);
     B->h_out.reserve(std::max<size_t>(1, count) * 48, st);
+    if (B->transient) return P;
     KB_CUDA(cudaStreamSynchronize(st));
-    Prepared* raw = P.get();
-    B->cache[sig] = std::move(P);
+    Prepared* raw = fresh.get();
+    B->cache[sig] = std::move(fresh);
     if (B->cache.size() > 32) {
         // Bound the cache; keep the current signature.
         for (auto i2 = B->cache.begin(); i2 != B->cache.end();) {
@@ -144,13 +188,14 @@ static void enqueue(CommitBatcher* B, Prepared* P, const uint32_t* srs, cudaStre
                      B->scratch.as<uint32_t>(), st);
     }
     (void)srs;
-    msm_engine_launch(B->msm, P->plan, B->evals.as<uint8_t>(), P->table, B->out_wire.as<uint8_t>(),
-                      B->out_comp.as<uint8_t>(), st);
+    for (size_t k = 0; k < P->ngroups; ++k)
+        msm_engine_launch(B->msm, P->groups[k].plan, B->evals.as<uint8_t>(), P->groups[k].table,
+                          B->out_wire.as<uint8_t>(), B->out_comp.as<uint8_t>(), st);
 }
 
 static void run(CommitBatcher* B, Prepared* P, const uint32_t* srs, cudaStream_t st,
                 bool use_graph) {
-    if (!use_graph) {
+    if (!use_graph || B->transient) {
         enqueue(B, P, srs, st);
         return;
     }

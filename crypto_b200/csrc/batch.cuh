@@ -23,6 +23,9 @@ CommitBatcher* commit_batcher_create();
 void commit_batcher_destroy(CommitBatcher* b);
 // Shifted tables over the SRS the batcher is given (null = plain MSMs).
 void commit_batcher_set_shift(CommitBatcher* b, ShiftTables* shifts);
+// Transient mode: no per-signature cache or graphs; one plan set rebuilt in
+// place per batch without synchronising (for streams of unrepeated batches).
+void commit_batcher_set_transient(CommitBatcher* b, bool transient);
 
 // Commits `count` polynomials.  h_evals: host evaluations (32 B LE each,
 // back to back in the order of sizes); h_out: 48 * count bytes.  srs_table:

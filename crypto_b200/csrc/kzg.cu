@@ -130,31 +130,108 @@ __global__ void k_fr_powers(const uint8_t* __restrict__ tau, size_t n, uint8_t* 
 }
 
 // Levels 1..W-1 of a shifted table: level w row i = [2^(c w)] (base row i).
-// One thread per point: c doublings per level, then an affine conversion.
-__global__ void __launch_bounds__(128) k_shift_levels(const uint32_t* __restrict__ base, size_t n,
-                                                      int c, int W, uint32_t* __restrict__ out) {
+// One thread per point: c doublings per level, then the affine conversion
+// with one inversion per block per level (Montgomery's trick: inclusive
+// prefix and suffix products of ZZ*ZZZ across the block's 128 points, so
+// 1/d_t = 1/(d_0...d_127) * P_{t-1} * S_{t+1}).
+constexpr int SHIFT_T = 128;
+
+template <class F>
+__device__ __forceinline__ void smw_load(Fe<F>& r, const uint32_t* sm, int t) {
+#pragma unroll
+    for (int k = 0; k < F::N; ++k) r.v[k] = sm[k * SHIFT_T + t];
+}
+template <class F>
+__device__ __forceinline__ void smw_store(uint32_t* sm, int t, const Fe<F>& a) {
+#pragma unroll
+    for (int k = 0; k < F::N; ++k) sm[k * SHIFT_T + t] = a.v[k];
+}
+
+__global__ void __launch_bounds__(SHIFT_T) k_shift_levels(const uint32_t* __restrict__ base, size_t n,
+                                                          int c, int W, uint32_t* __restrict__ out) {
     using F = FpBLS;
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t* src = base + i * 2 * F::N;
-    for (int k = 0; k < 2 * F::N; ++k) out[i * 2 * F::N + k] = src[k];
-    const bool inf = aff_is_inf_words<F>(src);
-    Affine<F> a;
-    aff_load(a, src);
+    __shared__ uint32_t s_pre[SHIFT_T * F::N];
+    __shared__ uint32_t s_suf[SHIFT_T * F::N];
+    __shared__ uint32_t s_inv[F::N];
+    const int t = threadIdx.x;
+    const size_t i = (size_t)blockIdx.x * SHIFT_T + t;
+    const bool live = i < n;
+    bool inf = true;
     Xyzz<F> p;
-    xyzz_from_affine(p, a);
-    for (int w = 1; w < W; ++w) {
-        uint32_t* dst = out + ((size_t)w * n + i) * 2 * F::N;
-        if (!inf)
-            for (int k = 0; k < c; ++k) xyzz_dbl(p, p);
-        Affine<F> r;
-        if (inf || !xyzz_to_affine(r, p)) {
-            for (int k = 0; k < 2 * F::N; ++k) dst[k] = 0;
-            dst[F::N - 1] = INF_FLAG;
-        } else {
-            fe_store(dst, r.x);
-            fe_store(dst + F::N, r.y);
+    xyzz_set_inf(p);
+    if (live) {
+        const uint32_t* src = base + i * 2 * F::N;
+        for (int k = 0; k < 2 * F::N; ++k) out[i * 2 * F::N + k] = src[k];
+        inf = aff_is_inf_words<F>(src);
+        if (!inf) {
+            Affine<F> a;
+            aff_load(a, src);
+            xyzz_from_affine(p, a);
         }
+    }
+    for (int w = 1; w < W; ++w) {
+        if (!inf) {
+            for (int k = 0; k < c; ++k) xyzz_dbl(p, p);
+            inf = xyzz_is_inf(p);
+        }
+        Fe<F> d;
+        if (inf)
+            fe_one(d);
+        else
+            fe_mul(d, p.ZZ, p.ZZZ);
+        smw_store(s_pre, t, d);
+        smw_store(s_suf, t, d);
+        __syncthreads();
+        for (int k = 1; k < SHIFT_T; k <<= 1) {
+            Fe<F> a, b, o;
+            smw_load(a, s_pre, t);
+            smw_load(b, s_suf, t);
+            if (t >= k) {
+                smw_load(o, s_pre, t - k);
+                fe_mul(a, a, o);
+            }
+            if (t + k < SHIFT_T) {
+                smw_load(o, s_suf, t + k);
+                fe_mul(b, b, o);
+            }
+            __syncthreads();
+            smw_store(s_pre, t, a);
+            smw_store(s_suf, t, b);
+            __syncthreads();
+        }
+        if (t == 0) {
+            Fe<F> tot, inv;
+            smw_load(tot, s_pre, SHIFT_T - 1);
+            fe_inv(inv, tot);
+            fe_store(s_inv, inv);
+        }
+        __syncthreads();
+        Fe<F> r, o;
+        fe_load(r, s_inv);
+        if (t > 0) {
+            smw_load(o, s_pre, t - 1);
+            fe_mul(r, r, o);
+        }
+        if (t + 1 < SHIFT_T) {
+            smw_load(o, s_suf, t + 1);
+            fe_mul(r, r, o);
+        }
+        if (live) {
+            uint32_t* dst = out + ((size_t)w * n + i) * 2 * F::N;
+            if (inf) {
+                for (int k = 0; k < 2 * F::N; ++k) dst[k] = 0;
+                dst[F::N - 1] = INF_FLAG;
+            } else {
+                Fe<F> iz, x, y;
+                fe_mul(iz, r, p.ZZZ);  // 1/ZZ
+                fe_mul(x, p.X, iz);
+                fe_mul(iz, r, p.ZZ);   // 1/ZZZ
+                fe_mul(y, p.Y, iz);
+                fe_store(dst, x);
+                fe_store(dst + F::N, y);
+            }
+        }
+        __syncthreads();  // the scans of the next level reuse the arrays
     }
 }
 
@@ -201,7 +278,7 @@ const uint32_t* shift_tables_get(ShiftTables* t, int c, cudaStream_t st) {
     if (bytes > SHIFT_TABLE_MAX_BYTES) return nullptr;
     DevBuf& b = t->levels[c];
     b.reserve(bytes, st);
-    k_shift_levels<<<ceil_div_u(t->n, 128), 128, 0, st>>>(t->base, t->n, c, W, b.as<uint32_t>());
+    k_shift_levels<<<ceil_div_u(t->n, SHIFT_T), SHIFT_T, 0, st>>>(t->base, t->n, c, W, b.as<uint32_t>());
     KB_LAUNCH_CHECK();
     KB_CUDA(cudaStreamSynchronize(st));  // usable from any stream once returned
     return b.as<uint32_t>();
@@ -210,11 +287,11 @@ const uint32_t* shift_tables_get(ShiftTables* t, int c, cudaStream_t st) {
 int shift_c_for(const size_t* sizes, size_t count) {
     // Accumulation: one mixed addition per entry over the windows canonical
     // scalars populate; reduction: ~2.8 additions per bucket of the single
-    // shared window of each item.  Only four window sizes are offered, so a
-    // resident setup carries at most four shifted tables.
+    // shared window of each item.  Only three window sizes are offered, so a
+    // resident setup carries at most three shifted tables.
     int best_c = 13;
     double best = 1e300;
-    for (int c : {10, 13, 16, 19}) {
+    for (int c : {13, 16, 19}) {
         const double wl = (double)((255 + c - 1) / c);
         double cost = 0;
         for (size_t i = 0; i < count; ++i) cost += wl * (double)sizes[i] + 2.8 * (double)(1u << (c - 1));

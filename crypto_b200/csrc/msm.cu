@@ -239,6 +239,7 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         }
         ItemDesc& d = P.items[i];
         d.scalar_off = items[i].scalar_off;
+        d.out_index = items[i].out_index == SIZE_MAX ? (uint32_t)i : (uint32_t)items[i].out_index;
         d.n = (uint32_t)n;
         d.point_off = (uint32_t)items[i].point_off;
         d.quirk_c = opt.ref_carry_quirk ? reference_best_c(n) : 0;
@@ -316,29 +317,42 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
     P.big_cap = P.nchunks / (size_t)P.K2 + 2;
 }
 
+static void upload_plan(MsmBatchPlan* P, cudaStream_t st) {
+    P->d_items.reserve(std::max<size_t>(1, P->items.size()) * sizeof(ItemDesc), st);
+    P->d_wins.reserve(std::max<size_t>(1, P->wins.size()) * sizeof(WinDesc), st);
+    P->d_blks.reserve(std::max<size_t>(1, P->blks.size()) * sizeof(BlkDesc), st);
+    if (!P->items.empty())
+        KB_CUDA(cudaMemcpyAsync(P->d_items.ptr, P->items.data(), P->items.size() * sizeof(ItemDesc),
+                                cudaMemcpyHostToDevice, st));
+    if (!P->wins.empty())
+        KB_CUDA(cudaMemcpyAsync(P->d_wins.ptr, P->wins.data(), P->wins.size() * sizeof(WinDesc),
+                                cudaMemcpyHostToDevice, st));
+    if (!P->blks.empty())
+        KB_CUDA(cudaMemcpyAsync(P->d_blks.ptr, P->blks.data(), P->blks.size() * sizeof(BlkDesc),
+                                cudaMemcpyHostToDevice, st));
+}
+
 MsmBatchPlan* msm_batch_plan_create(int curve, const MsmItem* items, size_t count,
                                     const MsmOptions& opt, cudaStream_t st) {
     auto* P = new MsmBatchPlan();
     try {
         build_plan_host(*P, curve, items, count, opt);
-        P->d_items.reserve(std::max<size_t>(1, P->items.size()) * sizeof(ItemDesc), st);
-        P->d_wins.reserve(std::max<size_t>(1, P->wins.size()) * sizeof(WinDesc), st);
-        P->d_blks.reserve(std::max<size_t>(1, P->blks.size()) * sizeof(BlkDesc), st);
-        if (!P->items.empty())
-            KB_CUDA(cudaMemcpyAsync(P->d_items.ptr, P->items.data(),
-                                    P->items.size() * sizeof(ItemDesc), cudaMemcpyHostToDevice, st));
-        if (!P->wins.empty())
-            KB_CUDA(cudaMemcpyAsync(P->d_wins.ptr, P->wins.data(), P->wins.size() * sizeof(WinDesc),
-                                    cudaMemcpyHostToDevice, st));
-        if (!P->blks.empty())
-            KB_CUDA(cudaMemcpyAsync(P->d_blks.ptr, P->blks.data(), P->blks.size() * sizeof(BlkDesc),
-                                    cudaMemcpyHostToDevice, st));
+        upload_plan(P, st);
         KB_CUDA(cudaStreamSynchronize(st));
     } catch (...) {
         delete P;
         throw;
     }
     return P;
+}
+
+void msm_batch_plan_update(MsmBatchPlan* P, const MsmItem* items, size_t count,
+                           const MsmOptions& opt, cudaStream_t st) {
+    P->items.clear();
+    P->wins.clear();
+    P->blks.clear();
+    build_plan_host(*P, P->curve, items, count, opt);
+    upload_plan(P, st);  // stream-ordered after every earlier launch that read it
 }
 
 void msm_batch_plan_destroy(MsmBatchPlan* p) { delete p; }

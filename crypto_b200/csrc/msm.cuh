@@ -27,6 +27,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <climits>
 #include <vector>
 
 namespace kb200 {
@@ -71,6 +72,7 @@ struct MsmItem {
     size_t scalar_off;
     size_t n;
     size_t point_off;
+    size_t out_index = SIZE_MAX;  // result slot (default: the item's position)
 };
 
 class MsmBatchPlan;
@@ -78,6 +80,12 @@ class MsmBatchPlan;
 MsmBatchPlan* msm_batch_plan_create(int curve, const MsmItem* items, size_t count,
                                     const MsmOptions& opt, cudaStream_t stream);
 void msm_batch_plan_destroy(MsmBatchPlan* p);
+// Rebuilds an existing plan for new items in place, reusing its device
+// descriptor buffers (grow-only) and without synchronising: the upload is
+// ordered on `stream` after earlier launches that used the plan, which must
+// have been on the same stream.
+void msm_batch_plan_update(MsmBatchPlan* p, const MsmItem* items, size_t count,
+                           const MsmOptions& opt, cudaStream_t stream);
 size_t msm_batch_plan_count(const MsmBatchPlan* p);
 
 class MsmEngine;

@@ -23,6 +23,7 @@ struct ItemDesc {
     int32_t quirk_c;                // reference carry emulation (0, 4 or 8)
     uint32_t row_stride;            // shifted table: rows per level (0 = plain table)
     uint32_t Wr;                    // windows reduced and combined (W, or 1 when shifted)
+    uint32_t out_index;             // result slot in the output arrays
 };
 
 // One window of one item.

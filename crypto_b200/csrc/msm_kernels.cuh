@@ -482,8 +482,8 @@ __global__ void k_combine(const ItemDesc* __restrict__ items, uint32_t n_items,
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_items) return;
     const ItemDesc it = items[i];
-    uint8_t* ow = out_wire + (size_t)i * C::WIRE;
-    uint8_t* oc = out_comp ? out_comp + (size_t)i * 48 : nullptr;
+    uint8_t* ow = out_wire + (size_t)it.out_index * C::WIRE;
+    uint8_t* oc = out_comp ? out_comp + (size_t)it.out_index * 48 : nullptr;
     Xyzz<F> acc, t;
     if (it.n == 0) {
         xyzz_set_inf(acc);

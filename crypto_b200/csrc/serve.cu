@@ -26,6 +26,7 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <set>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -216,6 +217,14 @@ void* kzg_server_create(size_t max_batch, int slots, size_t mem_budget_bytes) {
             KB_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
             sl.batcher = commit_batcher_create();
             commit_batcher_set_shift(sl.batcher, resident_srs_shifts());
+            commit_batcher_set_transient(sl.batcher, true);
+        }
+        // Build the shifted SRS tables every commit size can select now, so
+        // no request pays for a table build.
+        if (ShiftTables* sh = resident_srs_shifts()) {
+            std::set<int> cs;
+            for (size_t n = 1; n <= s->srs_n; n <<= 1) cs.insert(shift_c_for(&n, 1));
+            for (int c : cs) shift_tables_get(sh, c, s->slots[0].stream);
         }
         s->worker = std::thread([s] { s->loop(); });
         return s;

@@ -177,7 +177,10 @@ int kzg_commit_batch(const uint8_t* evals32le, const size_t* sizes, size_t count
  * device memory free up; batches on different slots overlap on the device.
  * max_batch: requests per batch (0 = 64); slots: concurrent batches
  * (0 = 2); mem_budget_bytes: cap on a batch's computed device footprint
- * (0 = free device memory).  Returns NULL on failure (kb200_last_error). */
+ * (0 = free device memory).  Creation builds, once per SRS, the shifted SRS
+ * tables the commit sizes use (up to three window sizes; about 5 GB and
+ * well under a second for a 2^20 SRS), so no request waits for one.
+ * Returns NULL on failure (kb200_last_error). */
 void* kzg_server_create(size_t max_batch, int slots, size_t mem_budget_bytes);
 /* Queue one polynomial (n evaluations, 32 B LE); *ticket identifies it. */
 int kzg_server_submit(void* server, const uint8_t* evals32le, size_t n, uint64_t* ticket);
