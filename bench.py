@@ -629,7 +629,7 @@ def main():
     ap.add_argument("--case", default="msm", choices=["msm", "ntt"],
                     help="msm: the benchmark line; ntt: one Fr NTT size only (profiling)")
     ap.add_argument("--commits", type=int, default=512)
-    ap.add_argument("--serve-rates", type=float, nargs="*", default=[100.0, 400.0])
+    ap.add_argument("--serve-rates", type=float, nargs="*", default=[100.0, 400.0, 1600.0])
     ap.add_argument("--serve-requests", type=int, default=80)
     args = ap.parse_args()
     sys.path.insert(0, str(ROOT / "tests"))

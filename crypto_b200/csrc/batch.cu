@@ -61,6 +61,7 @@ class CommitBatcher {
     // buffers, instead of caching (and later freeing) one per signature.
     bool transient = false;
     std::unique_ptr<Prepared> scratch_prep;
+    std::vector<size_t> scratch_sizes;  // sizes scratch_prep was last built for
     unsigned long long graph_launches = 0, graph_captures = 0;
     ~CommitBatcher() {
         cache.clear();
@@ -93,6 +94,10 @@ static Prepared* prepare(CommitBatcher* B, const size_t* sizes, size_t count,
     if (B->transient) {
         if (!B->scratch_prep) B->scratch_prep = std::make_unique<Prepared>();
         P = B->scratch_prep.get();
+        // commit_batch_device_input and commit_batch_device prepare the same
+        // batch back to back: build it once
+        if (P->ngroups && B->scratch_sizes == sig.sizes) return P;
+        B->scratch_sizes = sig.sizes;
         P->classes.clear();
         P->class_off.clear();
     } else {
@@ -249,10 +254,13 @@ void commit_batch_device(CommitBatcher* B, const size_t* sizes, size_t count,
 
 const uint8_t* commit_batch_device_output(CommitBatcher* B) { return B->out_comp.as<uint8_t>(); }
 
+size_t commit_item_scratch_bytes(size_t n) { return 2 * n * 32 + 144 + msm_item_scratch_bytes(2, n); }
+size_t commit_batch_fixed_bytes() { return msm_batch_fixed_bytes(2); }
+
 size_t commit_batch_scratch_bytes(const size_t* sizes, size_t count) {
-    size_t total = 0;
-    for (size_t i = 0; i < count; ++i) total += sizes[i];
-    return 2 * total * 32 + count * 144 + msm_scratch_bytes(2, sizes, count);
+    size_t b = commit_batch_fixed_bytes();
+    for (size_t i = 0; i < count; ++i) b += commit_item_scratch_bytes(sizes[i]);
+    return b;
 }
 
 unsigned long long commit_batcher_graph_launches(CommitBatcher* b) { return b->graph_launches; }

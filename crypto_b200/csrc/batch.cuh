@@ -47,6 +47,9 @@ const uint8_t* commit_batch_device_output(CommitBatcher* b);
 
 // Device bytes a batch of these sizes needs (evaluations, NTT scratch, MSM).
 size_t commit_batch_scratch_bytes(const size_t* sizes, size_t count);
+// Its additive parts: per commit and per batch.
+size_t commit_item_scratch_bytes(size_t n);
+size_t commit_batch_fixed_bytes();
 
 // Number of graph replays / captures so far (for tests).
 unsigned long long commit_batcher_graph_launches(CommitBatcher* b);

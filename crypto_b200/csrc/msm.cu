@@ -402,27 +402,29 @@ MsmEngine* msm_engine_create(int curve) {
 
 void msm_engine_destroy(MsmEngine* e) { delete e; }
 
-static size_t plan_scratch_bytes(const MsmBatchPlan& P) {
-    const size_t PW = (size_t)(P.curve == 2 ? 48 : 32);
-    size_t bytes = 3 * (size_t)P.L * 4;                      // keys, vals, sorted
-    bytes += 3 * ((size_t)P.B + 1) * 4;                      // counts, offsets, cursor
-    bytes += (P.levels >= 1 ? 3 : 2) * P.nchunks * PW * 4;   // chunk records (+ fold buffer)
-    bytes += P.big_cap * 4;
-    bytes += (size_t)P.B * PW * 4;                           // bucket accumulators
-    bytes += P.blks.size() * 2 * PW * 4 + P.wins.size() * PW * 4;
-    return bytes + (1u << 20);
+// Upper bounds without building a plan (admission control calls these per
+// request).  Per item, with its plain-table window plan: keys, vals and the
+// sorted list (4 B per entry each), three 4 B bucket arrays and the bucket
+// accumulators (per bucket), and the reduction blocks of its windows.
+size_t msm_item_scratch_bytes(int curve, size_t n) {
+    const size_t PW = (size_t)(curve == 2 ? 48 : 32) * 4;
+    const MsmPlan p = make_msm_plan(curve, n, MsmOptions());
+    const size_t L = (size_t)p.W * n, B = (size_t)p.W * p.M;
+    return 12 * L + 12 * (B + 1) + B * PW + (size_t)p.W * (2 * RED_THREADS + 1) * PW +
+           (L / 64 + 1) * (3 * PW + 4);  // chunk records once lists are long (K = 64)
+}
+
+// Per batch: the chunk records of short lists (K < 64 keeps at most about two
+// chunks per resident accumulation thread) and 1 MiB of descriptors.
+size_t msm_batch_fixed_bytes(int curve) {
+    const size_t PW = (size_t)(curve == 2 ? 48 : 32) * 4;
+    return (size_t)2 * 148 * 8 * 128 * (3 * PW + 4) + ((size_t)1 << 20);
 }
 
 size_t msm_scratch_bytes(int curve, const size_t* ns, size_t count) {
-    std::vector<MsmItem> items(count);
-    size_t off = 0;
-    for (size_t i = 0; i < count; ++i) {
-        items[i] = MsmItem{off, ns[i], 0};
-        off += ns[i];
-    }
-    MsmBatchPlan P;
-    build_plan_host(P, curve, items.data(), count, MsmOptions());
-    return plan_scratch_bytes(P);
+    size_t b = msm_batch_fixed_bytes(curve);
+    for (size_t i = 0; i < count; ++i) b += msm_item_scratch_bytes(curve, ns[i]);
+    return b;
 }
 
 void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {

@@ -121,6 +121,9 @@ int msm_stage_ms(MsmEngine* e, float* out, int max);
 int table_words(int curve);
 // Device scratch bytes an MSM batch of these sizes needs (admission control).
 size_t msm_scratch_bytes(int curve, const size_t* ns, size_t count);
+// The same bound split into per-item and per-batch parts (additive).
+size_t msm_item_scratch_bytes(int curve, size_t n);
+size_t msm_batch_fixed_bytes(int curve);
 
 // Autotuner: record the best window for a size class (log2 n) and curve.
 void msm_tune_set(int curve, int log_n, int c);

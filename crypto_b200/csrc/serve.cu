@@ -23,6 +23,8 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -41,9 +43,51 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// Pinned host slabs for request payloads, recycled by power-of-two size
+// class: a request is copied once, at submit, into page-locked memory, and
+// its batch's host-to-device copy reads it from there asynchronously.
+class PinnedPool {
+   public:
+    ~PinnedPool() {
+        for (void* p : all_) cudaFreeHost(p);
+    }
+    static size_t size_class(size_t bytes) {
+        size_t c = 4096;
+        while (c < bytes) c <<= 1;
+        return c;
+    }
+    uint8_t* get(size_t bytes) {
+        const size_t c = size_class(bytes);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            auto& v = free_[c];
+            if (!v.empty()) {
+                void* p = v.back();
+                v.pop_back();
+                return static_cast<uint8_t*>(p);
+            }
+        }
+        void* p = nullptr;
+        KB_CUDA(cudaHostAlloc(&p, c, cudaHostAllocPortable));
+        std::lock_guard<std::mutex> lk(mu_);
+        all_.push_back(p);
+        return static_cast<uint8_t*>(p);
+    }
+    void put(uint8_t* p, size_t bytes) {
+        if (!p) return;
+        std::lock_guard<std::mutex> lk(mu_);
+        free_[size_class(bytes)].push_back(p);
+    }
+
+   private:
+    std::mutex mu_;
+    std::map<size_t, std::vector<void*>> free_;
+    std::vector<void*> all_;
+};
+
 struct Request {
     uint64_t ticket = 0;
-    std::vector<uint8_t> evals;
+    uint8_t* evals = nullptr;  // pinned slab of n * 32 bytes (returned at completion)
     size_t n = 0;
     uint8_t commit[48] = {};
     int status = 1;  // 1 pending, 0 done, < 0 error
@@ -54,9 +98,10 @@ struct Slot {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
     CommitBatcher* batcher = nullptr;
-    HostBuf h_in, h_out;
+    HostBuf h_out;
     std::vector<Request*> reqs;
     bool busy = false;
+    std::chrono::steady_clock::time_point t_launch;
 };
 
 }  // namespace
@@ -74,11 +119,13 @@ class KzgServer {
     std::deque<Request*> queue;
     std::map<uint64_t, Request*> by_ticket;
     std::vector<double> latencies_ms;
+    PinnedPool pool;
     uint64_t next_ticket = 1;
     uint64_t completed = 0;
     Clock::time_point first_submit, last_done;
     bool have_first = false;
     std::atomic<bool> stop{false};
+    bool trace = std::getenv("KB200_SERVE_TRACE") != nullptr;  // per-batch log on stderr
     std::string error;
     std::thread worker;
 
@@ -89,10 +136,15 @@ class KzgServer {
 
 void KzgServer::finish(Slot& s) {
     const auto now = Clock::now();
+    if (trace)
+        std::fprintf(stderr, "[kzg_server] slot %d: done after %.3f ms\n", (int)(&s - slots.data()),
+                     std::chrono::duration<double, std::milli>(now - s.t_launch).count());
     std::lock_guard<std::mutex> lk(mu);
     for (size_t i = 0; i < s.reqs.size(); ++i) {
         Request* r = s.reqs[i];
         std::memcpy(r->commit, s.h_out.as<uint8_t>() + 48 * i, 48);
+        pool.put(r->evals, r->n * 32);
+        r->evals = nullptr;
         r->t_done = now;
         r->status = 0;
         latencies_ms.push_back(std::chrono::duration<double, std::milli>(now - r->t_submit).count());
@@ -117,40 +169,49 @@ bool KzgServer::launch_batch(Slot& s) {
         const size_t headroom = (size_t)256 << 20;
         const size_t avail = free_b > headroom ? free_b - headroom : 0;
         const size_t cap = mem_budget ? std::min(mem_budget, avail + 0) : avail;
+        size_t need = commit_batch_fixed_bytes();
         while (!queue.empty() && take.size() < max_batch) {
             Request* r = queue.front();
-            sizes.push_back(r->n);
-            const size_t need = commit_batch_scratch_bytes(sizes.data(), sizes.size());
+            const size_t item = commit_item_scratch_bytes(r->n);
             // Admit at least one request when the device is otherwise idle, so
             // a single oversized request is attempted rather than starved.
-            if (need > cap && !take.empty()) {
-                sizes.pop_back();
-                break;
-            }
+            if (need + item > cap && !take.empty()) break;
+            need += item;
+            sizes.push_back(r->n);
             take.push_back(r);
             queue.pop_front();
         }
     }
     if (take.empty()) return false;
+    const auto t_launch = Clock::now();
     size_t total = 0;
     for (Request* r : take) total += r->n;
-    s.h_in.reserve(total * 32, s.stream);
-    s.h_out.reserve(take.size() * 48, s.stream);
-    size_t off = 0;
-    for (Request* r : take) {
-        std::memcpy(s.h_in.as<uint8_t>() + off * 32, r->evals.data(), r->n * 32);
-        off += r->n;
-    }
+    if (s.h_out.bytes < take.size() * 48) s.h_out.reserve(std::max<size_t>(max_batch, take.size()) * 48, s.stream);
     uint8_t* d_in = commit_batch_device_input(s.batcher, sizes.data(), sizes.size(), srs, srs_n,
                                               s.stream);
-    KB_CUDA(cudaMemcpyAsync(d_in, s.h_in.ptr, total * 32, cudaMemcpyHostToDevice, s.stream));
+    size_t off = 0;
+    for (Request* r : take) {
+        KB_CUDA(cudaMemcpyAsync(d_in + off * 32, r->evals, r->n * 32, cudaMemcpyHostToDevice,
+                                s.stream));
+        off += r->n;
+    }
     commit_batch_device(s.batcher, sizes.data(), sizes.size(), srs, srs_n, s.stream,
                         /*use_graph=*/false);
     KB_CUDA(cudaMemcpyAsync(s.h_out.ptr, commit_batch_device_output(s.batcher), take.size() * 48,
                             cudaMemcpyDeviceToHost, s.stream));
     KB_CUDA(cudaEventRecord(s.done, s.stream));
+    if (trace) {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        std::fprintf(stderr, "[kzg_server] slot %d: %zu requests (%zu evaluations), host %.3f ms, "
+                             "queue left %zu, free %.1f GB\n",
+                     (int)(&s - slots.data()), take.size(), total,
+                     std::chrono::duration<double, std::milli>(Clock::now() - t_launch).count(),
+                     queue.size(), free_b / 1e9);
+    }
     s.reqs = std::move(take);
     s.busy = true;
+    s.t_launch = t_launch;
     return true;
 }
 
@@ -226,6 +287,26 @@ void* kzg_server_create(size_t max_batch, int slots, size_t mem_budget_bytes) {
             for (size_t n = 1; n <= s->srs_n; n <<= 1) cs.insert(shift_c_for(&n, 1));
             for (int c : cs) shift_tables_get(sh, c, s->slots[0].stream);
         }
+        // Warm every slot with one batch of the largest shape it is likely to
+        // see (a full-SRS commit plus max_batch - 1 commits of up to 2^16), so
+        // its engines and staging reach their working size before the first
+        // request instead of growing (and synchronising) under load.
+        {
+            std::vector<size_t> sizes{s->srs_n};
+            const size_t mid = std::min<size_t>(s->srs_n, (size_t)1 << 16);
+            for (size_t k = 1; k < s->max_batch; ++k) sizes.push_back(mid);
+            size_t total = 0;
+            for (size_t v : sizes) total += v;
+            for (Slot& sl : s->slots) {
+                uint8_t* d_in = commit_batch_device_input(sl.batcher, sizes.data(), sizes.size(), s->srs,
+                                                          s->srs_n, sl.stream);
+                KB_CUDA(cudaMemsetAsync(d_in, 0, total * 32, sl.stream));
+                commit_batch_device(sl.batcher, sizes.data(), sizes.size(), s->srs, s->srs_n, sl.stream,
+                                    /*use_graph=*/false);
+                sl.h_out.reserve(s->max_batch * 48, sl.stream);
+                KB_CUDA(cudaStreamSynchronize(sl.stream));
+            }
+        }
         s->worker = std::thread([s] { s->loop(); });
         return s;
     } catch (const std::exception& e) {
@@ -240,12 +321,20 @@ int kzg_server_submit(void* handle, const uint8_t* evals32le, size_t n, uint64_t
     if (n == 0 || (n & (n - 1))) return KB200_CRYPTO_ERR_LENGTH;
     if (n > s->srs_n) return KB200_CRYPTO_ERR_LENGTH;
     auto* r = new Request();
-    r->evals.assign(evals32le, evals32le + n * 32);
+    try {
+        r->evals = s->pool.get(n * 32);
+    } catch (const std::exception& e) {
+        delete r;
+        set_last_error(e.what());
+        return KB200_CRYPTO_ERR_BACKEND;
+    }
+    std::memcpy(r->evals, evals32le, n * 32);
     r->n = n;
     r->t_submit = Clock::now();
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (!s->error.empty()) {
+            s->pool.put(r->evals, n * 32);
             delete r;
             set_last_error(s->error);
             return KB200_CRYPTO_ERR_BACKEND;
@@ -331,7 +420,6 @@ int kzg_server_destroy(void* handle) {
     for (Slot& sl : s->slots) {
         if (sl.stream) cudaStreamSynchronize(sl.stream);
         commit_batcher_destroy(sl.batcher);
-        sl.h_in.release();
         sl.h_out.release();
         if (sl.done) cudaEventDestroy(sl.done);
         if (sl.stream) cudaStreamDestroy(sl.stream);

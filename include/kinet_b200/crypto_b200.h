@@ -179,7 +179,8 @@ int kzg_commit_batch(const uint8_t* evals32le, const size_t* sizes, size_t count
  * (0 = 2); mem_budget_bytes: cap on a batch's computed device footprint
  * (0 = free device memory).  Creation builds, once per SRS, the shifted SRS
  * tables the commit sizes use (up to three window sizes; about 5 GB and
- * well under a second for a 2^20 SRS), so no request waits for one.
+ * well under a second for a 2^20 SRS) and runs one warm-up batch per slot,
+ * so no request waits for a table build or a buffer to grow.
  * Returns NULL on failure (kb200_last_error). */
 void* kzg_server_create(size_t max_batch, int slots, size_t mem_budget_bytes);
 /* Queue one polynomial (n evaluations, 32 B LE); *ticket identifies it. */
