@@ -124,6 +124,54 @@ KB_DEV void xyzz_dbl_inl(Xyzz<F>& p) {
     fe_sub(p.Y, p.Y, W);
 }
 
+// Lane k's copy of a field element, for every lane of the warp.
+template <class F>
+KB_DEV void fe_bcast(Fe<F>& r, const Fe<F>& a, int k) {
+#pragma unroll
+    for (int i = 0; i < F::N; ++i) r.v[i] = __shfl_sync(0xffffffffu, a.v[i], k);
+}
+
+// dbl-2008-s-1 with the products spread over the lanes of a full warp: every
+// lane holds the same point; each of the three stages runs its independent
+// products on lanes 0..3 at once and broadcasts them, so a doubling costs
+// three product latencies on the critical path instead of nine.  For long
+// serial doubling chains (window weighting).  All 32 lanes must call it.
+template <class F>
+KB_DEV void xyzz_dbl_warp(Xyzz<F>& p) {
+    const int lane = threadIdx.x & 31;
+    Fe<F> U, a, b, r;
+    fe_dbl(U, p.Y);
+    // stage 1: V = U^2 (lane 0), t = X^2 (lane 1)
+    a = lane == 1 ? p.X : U;
+    fe_mul_inl(r, a, a);
+    Fe<F> V, t, M;
+    fe_bcast(V, r, 0);
+    fe_bcast(t, r, 1);
+    fe_dbl(M, t);
+    fe_add(M, M, t);
+    // stage 2: W = U V (0), S = X V (1), ZZ3 = V ZZ (2), M^2 (3)
+    a = lane == 1 ? p.X : (lane == 2 ? p.ZZ : (lane == 3 ? M : U));
+    b = lane == 3 ? M : V;
+    fe_mul_inl(r, a, b);
+    Fe<F> W, S, M2;
+    fe_bcast(W, r, 0);
+    fe_bcast(S, r, 1);
+    fe_bcast(p.ZZ, r, 2);
+    fe_bcast(M2, r, 3);
+    fe_sub(p.X, M2, S);
+    fe_sub(p.X, p.X, S);  // X3 = M^2 - 2S
+    fe_sub(S, S, p.X);
+    // stage 3: M (S - X3) (0), W Y (1), W ZZZ (2)
+    a = lane == 0 ? M : W;
+    b = lane == 0 ? S : (lane == 1 ? p.Y : p.ZZZ);
+    fe_mul_inl(r, a, b);
+    Fe<F> Ya, WY;
+    fe_bcast(Ya, r, 0);
+    fe_bcast(WY, r, 1);
+    fe_bcast(p.ZZZ, r, 2);
+    fe_sub(p.Y, Ya, WY);  // Y3 = M(S - X3) - W Y
+}
+
 // mdbl-2008-s-1: r = 2 * (affine a).
 template <class F>
 KB_DEV void xyzz_mdbl(Xyzz<F>& r, const Affine<F>& a) {
@@ -234,6 +282,23 @@ KB_DEV bool xyzz_to_affine(Affine<F>& a, const Xyzz<F>& p) {
     Fe<F> t, inv;
     fe_mul(t, p.ZZ, p.ZZZ);
     fe_inv(inv, t);           // 1 / (ZZ * ZZZ)
+    Fe<F> izz, izzz;
+    fe_mul(izz, inv, p.ZZZ);  // 1 / ZZ
+    fe_mul(izzz, inv, p.ZZ);  // 1 / ZZZ
+    fe_mul(a.x, p.X, izz);
+    fe_mul(a.y, p.Y, izzz);
+    return true;
+}
+
+// xyzz_to_affine with the binary-Euclid inversion: for one conversion on a
+// thread's critical path (an MSM result), not for bulk conversions where a
+// warp's lanes would diverge.
+template <class F>
+KB_DEV bool xyzz_to_affine_single(Affine<F>& a, const Xyzz<F>& p) {
+    if (xyzz_is_inf(p)) return false;
+    Fe<F> t, inv;
+    fe_mul(t, p.ZZ, p.ZZZ);
+    fe_inv_binary(inv, t);    // 1 / (ZZ * ZZZ)
     Fe<F> izz, izzz;
     fe_mul(izz, inv, p.ZZZ);  // 1 / ZZ
     fe_mul(izzz, inv, p.ZZ);  // 1 / ZZZ

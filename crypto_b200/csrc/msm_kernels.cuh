@@ -456,18 +456,24 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_windows(RedArgs a) {
     __syncthreads();
     smem_tree_sum<F>(sA);
     smem_tree_sum<F>(sB);
-    if (t == 0) {
+    // Warp 0 finishes: V = 2^log_blk * (sum over b >= 1 of Y_b) + sum Fb + Y_0,
+    // then the window weight 2^(c*w).  The doubling chains run with their
+    // products spread over the warp's lanes (three product latencies per
+    // doubling), one chain per window block, all windows in parallel.
+    if (t < 32) {
         Xyzz<F> V, u;
         sm_load(V, sA, 0);
-        xyzz_dbl_n(V, (int)wd.log_blk);
-        sm_load(u, sB, 0);
-        xyzz_add(V, u);
-        xyzz_add(V, Y0);
-        // Weight the window by 2^(c*w) here, one doubling chain per window
-        // running in parallel, instead of a Horner chain over all windows
-        // (c*(W-1) sequential doublings) in the combine.
-        for (uint32_t k = 0; k < wd.shift; ++k) xyzz_dbl_inl(V);
-        xyzz_store(a.win_out + (size_t)blockIdx.x * PW, V);
+        for (uint32_t k = 0; k < wd.log_blk; ++k) xyzz_dbl_warp(V);
+        if (t == 0) {
+            sm_load(u, sB, 0);
+            xyzz_add(V, u);
+            xyzz_add(V, Y0);
+            sm_store(sA, 0, V);
+        }
+        __syncwarp();
+        sm_load(V, sA, 0);
+        for (uint32_t k = 0; k < wd.shift; ++k) xyzz_dbl_warp(V);
+        if (t == 0) xyzz_store(a.win_out + (size_t)blockIdx.x * PW, V);
     }
 }
 
@@ -496,7 +502,7 @@ __global__ void k_combine(const ItemDesc* __restrict__ items, uint32_t n_items,
         }
     }
     Affine<F> af;
-    const bool fin = xyzz_to_affine(af, acc);
+    const bool fin = xyzz_to_affine_single(af, acc);
     Fe<F> x, y;
     if (fin) {
         fe_from_mont(x, af.x);
