@@ -542,8 +542,7 @@ def run_ours(args, ws, rank, local):
     peak_imad = SM_COUNT * IMAD_PER_CLK_SM * sm_mhz * 1e6
     # dominant kernel: bucket accumulation (one launch per MSM)
     plan_c = kb.msm_window(CURVE, n)
-    windows = (257 + plan_c - 1) // plan_c
-    entries = n * windows * (1 - 2.0 ** -plan_c)
+    entries = kb.lib().kb200_msm_entries(CURVE, n)
     acc_ms = stage.get("accumulate")
     acc_imad = entries * 6 * mont_imad(N_LIMBS)
     roofline = None

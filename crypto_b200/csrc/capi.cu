@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -685,8 +686,19 @@ int kb200_msm_stage_ms(uint32_t curve, float* out, int max) {
     }
 }
 
+double kb200_msm_entries(uint32_t curve, size_t n) {
+    MsmOptions opt;
+    if (curve == 2) {  // the wire path splits BLS12-381 scalars (GLV)
+        const MsmPlan p = make_msm_plan_glv(n, opt);
+        return 2.0 * (double)n * (double)((128 + p.c - 1) / p.c) * (1.0 - std::ldexp(1.0, -p.c));
+    }
+    const MsmPlan p = make_msm_plan((int)curve, n, opt);
+    return (double)n * (double)((255 + p.c - 1) / p.c) * (1.0 - std::ldexp(1.0, -p.c));
+}
+
 int kb200_msm_window(uint32_t curve, size_t n) {
     MsmOptions opt;
+    if (curve == 2) return make_msm_plan_glv(n, opt).c;
     return make_msm_plan((int)curve, n, opt).c;
 }
 

@@ -5,6 +5,7 @@
 #include "runtime.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <limits>
 #include <map>
 #include <mutex>
@@ -135,8 +136,8 @@ int msm_windows_for(int c) { return windows_for(c); }
 
 // Live buckets of the top window: its raw digit has 256 - c(W-1) bits plus a
 // carry, so its largest magnitude is 2^(256 - c(W-1)).
-static uint32_t top_buckets(int c, int W) {
-    const int bits = 256 - c * (W - 1);
+static uint32_t top_buckets(int c, int W, int scalar_bits = 256) {
+    const int bits = scalar_bits - c * (W - 1);
     const uint32_t M = 1u << (c - 1);
     if (bits <= 0) return 1;
     if (bits >= c - 1) return M;
@@ -173,6 +174,30 @@ MsmPlan make_msm_plan(int curve, size_t n, const MsmOptions& opt) {
     p.W = windows_for(c);
     p.M = 1u << (c - 1);
     p.M_top = top_buckets(c, p.W);
+    return p;
+}
+
+MsmPlan make_msm_plan_glv(size_t n, const MsmOptions& opt) {
+    MsmPlan p;
+    int c = opt.force_c;
+    if (c <= 0) {
+        // 2n points, ceil(128/c) populated windows of the 128-bit halves.
+        double best = 1e300;
+        for (int cc = 4; cc <= 20; ++cc) {
+            const double wl = (double)((128 + cc - 1) / cc);
+            const double cost = wl * 2.0 * (double)n + 2.8 * wl * (double)(1u << (cc - 1));
+            if (cost < best) {
+                best = cost;
+                c = cc;
+            }
+        }
+    }
+    if (c < 2) c = 2;
+    if (c > 22) c = 22;
+    p.c = c;
+    p.W = (129 + c - 1) / c;
+    p.M = 1u << (c - 1);
+    p.M_top = top_buckets(c, p.W, 128);
     return p;
 }
 
@@ -227,7 +252,12 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         if (n >= (1ull << 31) || items[i].point_off + n >= (1ull << 31))
             throw std::invalid_argument("msm: more than 2^31 points");
         max_n = std::max(max_n, n);
-        if (opt.shift_c > 0) {
+        const bool glv = opt.glv && curve == 2 && opt.shift_c <= 0;
+        if (glv) {
+            plans[i] = make_msm_plan_glv(n, opt);
+            if (items[i].point_off + n > opt.glv_rows || 2 * opt.glv_rows >= (1ull << 31))
+                throw std::invalid_argument("msm: item outside the GLV table");
+        } else if (opt.shift_c > 0) {
             MsmOptions o2 = opt;
             o2.force_c = opt.shift_c;
             plans[i] = make_msm_plan(curve, n, o2);
@@ -246,13 +276,15 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         d.c = (uint32_t)plans[i].c;
         d.M = plans[i].M;
         d.W = n ? (uint32_t)plans[i].W : 0u;
-        const bool shifted = opt.shift_c > 0;
+        d.glv = glv ? 1u : 0u;
+        d.glv_off = glv ? (uint32_t)opt.glv_rows : 0u;
+        const bool shifted = opt.shift_c > 0 && !glv;
         d.row_stride = shifted ? (uint32_t)opt.shift_stride : 0u;
         d.Wr = shifted ? (n ? 1u : 0u) : d.W;
         if (n) total_live += shifted ? d.M : (size_t)(d.W - 1) * d.M + plans[i].M_top;
         d.entry_base = L;
         d.bucket_base = (uint32_t)B;
-        L += (unsigned long long)d.W * n;
+        L += (unsigned long long)d.W * n * (glv ? 2u : 1u);
         B += (unsigned long long)d.Wr * d.M;
         tot_sc = std::max<unsigned long long>(tot_sc, d.scalar_off + n);
     }
@@ -369,7 +401,7 @@ class MsmEngine {
     int curve = 0;
     DevBuf table, keys, vals, counts, offsets, cursor, sorted, rec_first, rec_last, fold_buf,
         buckets, blk_out, win_out, scan_tmp, queue, fold_counts, fold_prefix;
-    std::map<std::tuple<size_t, bool, int, int, int, size_t>, MsmBatchPlan*> single_plans;
+    std::map<std::tuple<size_t, bool, int, int, int, size_t, bool, size_t>, MsmBatchPlan*> single_plans;
     cudaEvent_t ev[N_STAGE_EVENTS] = {};
     bool ev_ready = false, ev_recorded = false;
     void mark(int i, cudaStream_t st) {
@@ -554,7 +586,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
 
 static MsmBatchPlan* single_plan(MsmEngine* e, size_t n, const MsmOptions& opt, cudaStream_t st) {
     auto key = std::make_tuple(n, opt.ref_carry_quirk, opt.force_c, opt.force_K, opt.shift_c,
-                               opt.shift_stride);
+                               opt.shift_stride, opt.glv, opt.glv_rows);
     auto it = e->single_plans.find(key);
     if (it != e->single_plans.end()) return it->second;
     MsmItem item{0, n, 0};
@@ -581,12 +613,27 @@ void msm_run_table(MsmEngine* e, const uint8_t* d_scalars, const uint32_t* d_tab
 void msm_run_wire(MsmEngine* e, const uint8_t* d_scalars, const uint8_t* d_points, size_t n,
                   uint8_t* d_out_wire, uint8_t* d_out_comp, cudaStream_t st,
                   const MsmOptions& opt) {
-    MsmBatchPlan* p = single_plan(e, n, opt, st);
+    // BLS12-381: GLV split (the table gains the phi(P) rows).  phi(P) =
+    // [lambda]P holds on G1, the prime-order subgroup every caller's points
+    // live in; KB200_MSM_NO_GLV=1 keeps 256-bit windows, whose sum is also
+    // exact for curve points outside G1.
+    static const bool glv_env_off = [] {
+        const char* v = std::getenv("KB200_MSM_NO_GLV");
+        return v && *v && *v != '0';
+    }();
+    MsmOptions o2 = opt;
+    const bool glv = e->curve == 2 && opt.shift_c <= 0 && !opt.no_glv && !glv_env_off;
+    if (glv) {
+        o2.glv = true;
+        o2.glv_rows = n;
+    }
+    MsmBatchPlan* p = single_plan(e, n, o2, st);
     msm_engine_reserve(e, p, st);
     const MsmLaunchers& K = msm_launchers(e->curve);
-    e->table.reserve(std::max<size_t>(1, n) * (size_t)K.table_words * 4, st);
+    e->table.reserve(std::max<size_t>(1, n) * (glv ? 2 : 1) * (size_t)K.table_words * 4, st);
     e->mark(0, st);
     K.wire_to_table(d_points, e->table.as<uint32_t>(), n, st);
+    if (glv) K.glv_rows(e->table.as<uint32_t>(), n, st);
     e->mark(1, st);
     msm_engine_launch(e, p, d_scalars, e->table.as<uint32_t>(), d_out_wire, d_out_comp, st);
 }

@@ -56,6 +56,12 @@ struct MsmOptions {
     // 0 = plain table.
     int shift_c = 0;
     size_t shift_stride = 0;
+    // GLV split (BLS12-381 only, plain tables): rows glv_rows + i of the
+    // table hold phi(row i) = [lambda] row i; scalars split into two 128-bit
+    // halves (half the windows over twice the points).
+    bool glv = false;
+    size_t glv_rows = 0;
+    bool no_glv = false;  // msm_run_wire: keep the plain 256-bit windows
 };
 
 // Windows of a c-bit signed-digit decomposition of 256-bit scalars.
@@ -65,6 +71,8 @@ int msm_windows_for(int c);
 int reference_best_c(size_t n);
 // Window plan for one MSM of size n (autotuner cache, else cost model).
 MsmPlan make_msm_plan(int curve, size_t n, const MsmOptions& opt);
+// Window plan for a GLV-split MSM of n scalars (2n points, 128-bit halves).
+MsmPlan make_msm_plan_glv(size_t n, const MsmOptions& opt);
 
 // One MSM of a batch: n scalars starting at scalar index `scalar_off` of the
 // batch's scalar array, against table rows point_off .. point_off + n - 1.

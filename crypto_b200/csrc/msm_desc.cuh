@@ -24,6 +24,8 @@ struct ItemDesc {
     uint32_t row_stride;            // shifted table: rows per level (0 = plain table)
     uint32_t Wr;                    // windows reduced and combined (W, or 1 when shifted)
     uint32_t out_index;             // result slot in the output arrays
+    uint32_t glv;                   // 1: GLV split (BLS12-381), 2 W n entries
+    uint32_t glv_off;               // row offset of the phi(P) rows in the table
 };
 
 // One window of one item.
@@ -94,6 +96,7 @@ struct MsmLaunchers {
     void (*recode)(const ItemDesc*, uint32_t, unsigned long long, const uint32_t*,
                    const uint32_t*, uint32_t*, uint32_t*, cudaStream_t);
     void (*accumulate)(const AccArgs&, unsigned, cudaStream_t);
+    void (*glv_rows)(uint32_t*, size_t, cudaStream_t);
     void (*fold)(const FoldArgs&, int, const uint32_t*, uint32_t*, unsigned, cudaStream_t);
     void (*reduce_blocks)(const RedArgs&, unsigned, cudaStream_t);
     void (*reduce_windows)(const RedArgs&, unsigned, cudaStream_t);

@@ -38,8 +38,87 @@ __global__ void k_table_to_wire(const uint32_t* __restrict__ table, uint8_t* __r
     fe_to_be_bytes(o + F::BYTES, y);
 }
 
+// GLV split for BLS12-381 G1: with u = -0xd201000000010000 the curve
+// parameter, lambda = u^2 - 1 (128 bits) is a cube root of unity mod r and
+// phi(x, y) = (beta2 x, y), beta2 a cube root of unity mod p, acts on G1 as
+// [lambda].  A scalar k < r = lambda^2 + lambda + 1 splits as
+// k = k1 + k2 lambda with k1 = k mod lambda and k2 = k div lambda, both
+// below 2^128, so k P = k1 P + k2 phi(P): twice the points, half the
+// windows.  The quotient comes from Barrett reduction with
+// mu = floor(2^384 / lambda) (exact for k < r; a correction loop covers the
+// bound).  Little-endian 32-bit words.
+static __constant__ uint32_t kGlvLambda[4] = {0xffffffff, 0x00000000, 0x0001a402, 0xac45a401};
+static __constant__ uint32_t kGlvMu[9] = {0x896c72dd, 0xda5e4f8d, 0x268bf7a3, 0x389f49a7, 0xf6cfee30,
+                                   0x63f6e522, 0xe01faadd, 0x7c6becf1, 0x00000001};
+static __constant__ uint32_t kGlvBeta2[12] = {0x0000aaac, 0x8bfd0000, 0x4f49fffd, 0x409427eb,
+                                       0x0fb85f9b, 0x897d2965, 0x89759ad4, 0xaa0d857d,
+                                       0x63d4de85, 0xec024086, 0x397fe699, 0x1a0111ea};
+// 2^256 mod r: the reference's dropped top carry subtracts 2^256.
+static __constant__ uint32_t kR256ModR[8] = {0xfffffffe, 0x00000001, 0x00034802, 0x5884b7fa,
+                                      0xecbc4ff5, 0x998c4fef, 0xacc5056f, 0x1824b159};
+
+__device__ __forceinline__ bool geq_words(const uint32_t* a, const uint32_t* b, int n) {
+    for (int i = n - 1; i >= 0; --i)
+        if (a[i] != b[i]) return a[i] > b[i];
+    return true;
+}
+__device__ __forceinline__ void sub_words(uint32_t* a, const uint32_t* b, int n) {
+    uint32_t br = 0;
+    for (int i = 0; i < n; ++i) {
+        const uint64_t d = (uint64_t)a[i] - b[i] - br;
+        a[i] = (uint32_t)d;
+        br = (uint32_t)(d >> 63);
+    }
+}
+
+// k (8 words, < r) -> k1 = k mod lambda, k2 = k div lambda (4 words each).
+static __device__ void glv_split(const uint32_t k[8], uint32_t k1[4], uint32_t k2[4]) {
+    uint32_t prod[17];
+    for (int i = 0; i < 17; ++i) prod[i] = 0;
+    for (int i = 0; i < 8; ++i) {
+        uint64_t carry = 0;
+        for (int j = 0; j < 9; ++j) {
+            const uint64_t t = (uint64_t)k[i] * kGlvMu[j] + prod[i + j] + carry;
+            prod[i + j] = (uint32_t)t;
+            carry = t >> 32;
+        }
+        prod[i + 9] = (uint32_t)carry;
+    }
+    uint32_t q[5];
+    for (int i = 0; i < 5; ++i) q[i] = prod[12 + i];  // floor(k mu / 2^384)
+    // rem = k - q lambda (fits: 0 <= rem < 2^129 before correction)
+    uint32_t ql[9];
+    for (int i = 0; i < 9; ++i) ql[i] = 0;
+    for (int i = 0; i < 5; ++i) {
+        uint64_t carry = 0;
+        for (int j = 0; j < 4; ++j) {
+            const uint64_t t = (uint64_t)q[i] * kGlvLambda[j] + ql[i + j] + carry;
+            ql[i + j] = (uint32_t)t;
+            carry = t >> 32;
+        }
+        if (i + 4 < 9) ql[i + 4] = (uint32_t)carry;
+    }
+    uint32_t rem[8];
+    for (int i = 0; i < 8; ++i) rem[i] = k[i];
+    sub_words(rem, ql, 8);
+    uint32_t lam8[8] = {kGlvLambda[0], kGlvLambda[1], kGlvLambda[2], kGlvLambda[3], 0, 0, 0, 0};
+    for (int guard = 0; guard < 4 && geq_words(rem, lam8, 8); ++guard) {
+        sub_words(rem, lam8, 8);
+        uint32_t c = 1;
+        for (int i = 0; i < 5 && c; ++i) {
+            q[i] += c;
+            c = q[i] == 0;
+        }
+    }
+    for (int i = 0; i < 4; ++i) {
+        k1[i] = rem[i];
+        k2[i] = q[i];
+    }
+}
+
 // Signed-digit recoding, one thread per scalar of the batch.  Entry (w, j)
-// of item i lives at entry_base_i + w * n_i + j.
+// of item i lives at entry_base_i + w * n_i + j (GLV items: k1's digit at
+// entry_base_i + w * 2 n_i + j, k2's at entry_base_i + w * 2 n_i + n_i + j).
 // quirk_c: 0, or the reference window size (4 or 8) whose dropped top carry
 // is reproduced by negating (s, P) -> (2^256 - s, -P) for s above the
 // carry threshold 0x8888...88 (c = 4) or 0x8080...80 (c = 8).
@@ -71,6 +150,7 @@ __global__ void k_recode(const ItemDesc* __restrict__ items, uint32_t n_items,
     s[0] = a.x; s[1] = a.y; s[2] = a.z; s[3] = a.w;
     s[4] = b.x; s[5] = b.y; s[6] = b.z; s[7] = b.w;
     uint32_t neg = 0;
+    bool dropped_carry = false;
     if (it.quirk_c == 4 || it.quirk_c == 8) {
         const uint32_t t = it.quirk_c == 4 ? 0x88888888u : 0x80808080u;
         int gt = 0;
@@ -81,52 +161,113 @@ __global__ void k_recode(const ItemDesc* __restrict__ items, uint32_t n_items,
                 else if (s[k] < t) gt = -1;
             }
         }
-        if (gt == 1) {
-            uint32_t carry = 1;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint64_t v = (uint64_t)(~s[k]) + carry;
-                s[k] = (uint32_t)v;
-                carry = (uint32_t)(v >> 32);
-            }
-            neg = 1;
-        }
+        dropped_carry = gt == 1;
     }
     const int c = (int)it.c;
     const uint32_t M = it.M;
     const uint32_t mask = (1u << c) - 1u;
-    uint32_t carry = 0;
-    for (int w = 0; w < (int)it.W; ++w) {
-        const int off = w * c;
-        const int wd = off >> 5, sh = off & 31;
-        uint32_t raw = 0;
-        if (wd < 8) {
-            const uint64_t lo64 = s[wd];
-            const uint64_t hi64 = (wd + 1 < 8) ? s[wd + 1] : 0;
-            raw = (uint32_t)(((hi64 << 32) | lo64) >> sh) & mask;
+    // Signed digits of the nw-word scalar sc over the item's W windows; the
+    // digit of window w goes to entry slot0 + w * wstride with point row prow.
+    auto emit = [&](const uint32_t* sc, int nw, uint32_t prow, unsigned long long slot0,
+                    unsigned long long wstride, uint32_t negbit) {
+        uint32_t carry = 0;
+        for (int w = 0; w < (int)it.W; ++w) {
+            const int off = w * c;
+            const int wd = off >> 5, sh = off & 31;
+            uint32_t raw = 0;
+            if (wd < nw) {
+                const uint64_t lo64 = sc[wd];
+                const uint64_t hi64 = (wd + 1 < nw) ? sc[wd + 1] : 0;
+                raw = (uint32_t)(((hi64 << 32) | lo64) >> sh) & mask;
+            }
+            uint32_t d = raw + carry;
+            uint32_t sign = 0;
+            if (d > M) {
+                d = (1u << c) - d;
+                sign = 1;
+                carry = 1;
+            } else {
+                carry = 0;
+            }
+            const unsigned long long slot = slot0 + (unsigned long long)w * wstride;
+            if (d == 0 || inf) {
+                keys[slot] = KEY_SENTINEL;
+            } else if (it.row_stride) {
+                // shifted table: level w holds 2^(c*w) times the point, so every
+                // window feeds the same buckets
+                keys[slot] = it.bucket_base + (d - 1);
+                vals[slot] = (prow + (uint32_t)w * it.row_stride) | ((sign ^ negbit) << 31);
+            } else {
+                keys[slot] = it.bucket_base + (uint32_t)w * M + (d - 1);
+                vals[slot] = prow | ((sign ^ negbit) << 31);
+            }
         }
-        uint32_t d = raw + carry;
-        uint32_t sign = 0;
-        if (d > M) {
-            d = (1u << c) - d;
-            sign = 1;
-            carry = 1;
-        } else {
-            carry = 0;
-        }
-        const unsigned long long slot = it.entry_base + (unsigned long long)w * it.n + j;
-        if (d == 0 || inf) {
-            keys[slot] = KEY_SENTINEL;
-        } else if (it.row_stride) {
-            // shifted table: level w holds 2^(c*w) times the point, so every
-            // window feeds the same buckets
-            keys[slot] = it.bucket_base + (d - 1);
-            vals[slot] = (row + (uint32_t)w * it.row_stride) | ((sign ^ neg) << 31);
-        } else {
-            keys[slot] = it.bucket_base + (uint32_t)w * M + (d - 1);
-            vals[slot] = row | ((sign ^ neg) << 31);
+    };
+    if constexpr (C::CURVE_ID == 2) {
+        if (it.glv) {
+            // k = s mod r (s < 2^256 < 3r), minus 2^256 where the reference
+            // drops its top carry
+            uint32_t k[8], r8[8];
+            for (int i = 0; i < 8; ++i) {
+                k[i] = s[i];
+                r8[i] = FrBLS::P(i);
+            }
+            for (int guard = 0; guard < 3 && geq_words(k, r8, 8); ++guard) sub_words(k, r8, 8);
+            if (dropped_carry) {
+                uint32_t t[8];
+                for (int i = 0; i < 8; ++i) t[i] = kR256ModR[i];
+                if (geq_words(k, t, 8)) {
+                    sub_words(k, t, 8);
+                } else {  // k + r - t
+                    uint64_t cy = 0;
+                    for (int i = 0; i < 8; ++i) {
+                        cy += (uint64_t)k[i] + r8[i];
+                        k[i] = (uint32_t)cy;
+                        cy >>= 32;
+                    }
+                    sub_words(k, t, 8);
+                }
+            }
+            uint32_t k1[4], k2[4];
+            glv_split(k, k1, k2);
+            const unsigned long long base = it.entry_base + j;
+            emit(k1, 4, row, base, 2ull * it.n, 0u);
+            emit(k2, 4, row + it.glv_off, base + it.n, 2ull * it.n, 0u);
+            return;
         }
     }
+    if (dropped_carry) {
+        uint32_t cy = 1;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint64_t v = (uint64_t)(~s[k]) + cy;
+            s[k] = (uint32_t)v;
+            cy = (uint32_t)(v >> 32);
+        }
+        neg = 1;
+    }
+    emit(s, 8, row, it.entry_base + j, (unsigned long long)it.n, neg);
+}
+
+// GLV rows: table[n + i] = phi(table[i]) = (beta2 x, y); infinity stays.
+template <class C>
+__global__ void k_glv_rows(uint32_t* __restrict__ table, size_t n) {
+    using F = typename C::F;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t* src = table + i * 2 * F::N;
+    uint32_t* dst = table + (n + i) * 2 * F::N;
+    if (aff_is_inf_words<F>(src)) {
+        for (int k = 0; k < 2 * F::N; ++k) dst[k] = src[k];
+        return;
+    }
+    Fe<F> x, b;
+    fe_load(x, src);
+    for (int k = 0; k < F::N; ++k) b.v[k] = kGlvBeta2[k];
+    fe_to_mont(b, b);
+    fe_mul(x, x, b);
+    fe_store(dst, x);
+    for (int k = 0; k < F::N; ++k) dst[F::N + k] = src[F::N + k];
 }
 
 template <class F>
@@ -559,6 +700,13 @@ struct MsmLaunchImpl {
                                                            keys, vals);
         KB_LAUNCH_CHECK();
     }
+    static void glv_rows(uint32_t* table, size_t n, cudaStream_t st) {
+        if constexpr (C::CURVE_ID == 2) {
+            if (!n) return;
+            k_glv_rows<C><<<ceil_div_u(n, 128), 128, 0, st>>>(table, n);
+            KB_LAUNCH_CHECK();
+        }
+    }
     static void accumulate(const AccArgs& a, unsigned grid, cudaStream_t st) {
         k_accumulate<C><<<grid, 128, 0, st>>>(a);
         KB_LAUNCH_CHECK();
@@ -599,6 +747,7 @@ struct MsmLaunchImpl {
         L.table_to_wire = &table_to_wire;
         L.recode = &recode;
         L.accumulate = &accumulate;
+        L.glv_rows = &glv_rows;
         L.fold = &fold;
         L.reduce_blocks = &reduce_blocks;
         L.reduce_windows = &reduce_windows;

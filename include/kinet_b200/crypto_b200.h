@@ -60,7 +60,10 @@ extern "C" {
  * secp256k1 (0) and banderwagon (3) return GPUKIT_ERR_NOTIMPL so the
  * reference dispatcher's CPU fallback still covers them; unknown ids return
  * GPUKIT_ERR_BACKEND as the CPU body does.  Points must be on the curve
- * (neither implementation checks; off-curve input is undefined). */
+ * (neither implementation checks; off-curve input is undefined).  For
+ * BLS12-381 the sum is computed with the GLV endomorphism, which equals the
+ * reference's sum for points of G1 (the prime-order subgroup); for curve
+ * points outside G1 set KB200_MSM_NO_GLV=1 to keep plain 256-bit windows. */
 int gpukit_multi_pippenger(uint32_t curve, const uint8_t* scalars, const uint8_t* points,
                            size_t n, uint8_t* result);
 
@@ -255,8 +258,12 @@ void kb200_tune_set(int kind, uint32_t curve, int log_n, int value);
 const char* kb200_last_error(void);
 /* 1 if a CUDA device is usable, else 0. */
 int kb200_device_available(void);
-/* Window size the MSM planner picks for n (for tests of the planner). */
+/* Window size the MSM planner picks for n (for tests of the planner; for
+ * BLS12-381 the window of the GLV-split 128-bit halves). */
 int kb200_msm_window(uint32_t curve, size_t n);
+/* Expected bucket additions of one n-point MSM through the wire path (entries
+ * of non-zero digits: points x populated windows x (1 - 2^-c)). */
+double kb200_msm_entries(uint32_t curve, size_t n);
 /* Number of this library's kernel launches since load. */
 unsigned long long kb200_launch_count(void);
 /* Per-stage CUDA-event timing of MSMs (off by default). */
