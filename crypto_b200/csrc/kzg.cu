@@ -285,16 +285,16 @@ const uint32_t* shift_tables_get(ShiftTables* t, int c, cudaStream_t st) {
 }
 
 int shift_c_for(const size_t* sizes, size_t count) {
-    // Accumulation: one mixed addition per entry over the windows canonical
-    // scalars populate; reduction: ~2.8 additions per bucket of the single
-    // shared window of each item.  Only three window sizes are offered, so a
+    // Accumulation: one entry per window canonical scalars populate;
+    // reduction: ~7 entry-equivalents per bucket of the single shared window
+    // of each item.  Only three window sizes are offered, so a
     // resident setup carries at most three shifted tables.
     int best_c = 13;
     double best = 1e300;
     for (int c : {13, 16, 19}) {
         const double wl = (double)((255 + c - 1) / c);
         double cost = 0;
-        for (size_t i = 0; i < count; ++i) cost += wl * (double)sizes[i] + 2.8 * (double)(1u << (c - 1));
+        for (size_t i = 0; i < count; ++i) cost += wl * (double)sizes[i] + RED_COST * (double)(1u << (c - 1));
         if (cost < best) {
             best = cost;
             best_c = c;

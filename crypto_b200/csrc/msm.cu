@@ -155,13 +155,14 @@ MsmPlan make_msm_plan(int curve, size_t n, const MsmOptions& opt) {
     int c = opt.force_c;
     if (c <= 0) c = msm_tune_get(curve, ceil_log2(n ? n : 1));
     if (c <= 0) {
-        // Cost model in mixed-addition units: one per entry over the windows
-        // that canonical (< 2^255) scalars populate, plus ~2.8 per bucket
-        // for the two full additions of the reduction.
+        // Cost model in accumulation-entry units: one per entry over the
+        // windows that canonical (< 2^255) scalars populate, plus ~7 per
+        // bucket for the reduction (its two full additions, scan and tree
+        // phases; measured on B200 at 2^20-2^22).
         double best = 1e300;
         for (int cc = 4; cc <= 20; ++cc) {
             const double wl = (double)((255 + cc - 1) / cc);
-            const double cost = wl * (double)n + 2.8 * wl * (double)(1u << (cc - 1));
+            const double cost = wl * (double)n + RED_COST * wl * (double)(1u << (cc - 1));
             if (cost < best) {
                 best = cost;
                 c = cc;
@@ -185,7 +186,7 @@ MsmPlan make_msm_plan_glv(size_t n, const MsmOptions& opt) {
         double best = 1e300;
         for (int cc = 4; cc <= 20; ++cc) {
             const double wl = (double)((128 + cc - 1) / cc);
-            const double cost = wl * 2.0 * (double)n + 2.8 * wl * (double)(1u << (cc - 1));
+            const double cost = wl * 2.0 * (double)n + RED_COST * wl * (double)(1u << (cc - 1));
             if (cost < best) {
                 best = cost;
                 c = cc;
