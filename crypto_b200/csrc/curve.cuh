@@ -172,6 +172,22 @@ KB_DEV void xyzz_dbl_warp(Xyzz<F>& p) {
     fe_sub(p.Y, Ya, WY);  // Y3 = M(S - X3) - W Y
 }
 
+// V = [k] V for a small k >= 0 by double-and-add, the doublings spread over
+// the warp (xyzz_dbl_warp); every lane holds the same point and performs the
+// same additions.  All 32 lanes must call it.
+template <class F>
+KB_DEV void xyzz_mul_small_warp(Xyzz<F>& V, uint32_t k) {
+    if (k == 0) {
+        xyzz_set_inf(V);
+        return;
+    }
+    const Xyzz<F> R = V;
+    for (int b = 30 - __clz(k); b >= 0; --b) {
+        xyzz_dbl_warp(V);
+        if ((k >> b) & 1u) xyzz_add(V, R);
+    }
+}
+
 // mdbl-2008-s-1: r = 2 * (affine a).
 template <class F>
 KB_DEV void xyzz_mdbl(Xyzz<F>& r, const Affine<F>& a) {

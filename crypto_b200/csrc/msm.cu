@@ -298,12 +298,12 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
     P.L = L;
     P.B = (uint32_t)B;
     P.total_scalars = tot_sc;
-    // Reduction granularity: buckets per thread S (power of two) so that
-    // stage 1 fills about one wave (two resident 256-thread blocks per SM),
-    // and every window has at most RED_THREADS stage-1 blocks.
+    // Reduction granularity: buckets per thread S (any integer) so that
+    // stage 1 fills one wave of two resident 256-thread blocks per SM as
+    // evenly as the bucket count allows, and every window has at most
+    // RED_THREADS stage-1 blocks.
     const size_t per_wave = (size_t)2 * device_sms() * RED_THREADS;
-    int log_S = 0;
-    while (((size_t)1 << log_S) * per_wave < total_live && log_S < 6) ++log_S;
+    const uint32_t S0 = (uint32_t)std::max<size_t>(1, (total_live + per_wave - 1) / per_wave);
     for (size_t i = 0; i < count; ++i) {
         ItemDesc& d = P.items[i];
         d.win_base = (uint32_t)P.wins.size();
@@ -311,11 +311,12 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
             WinDesc wd;
             wd.bucket_base = d.bucket_base + w * d.M;
             wd.Mw = d.row_stride ? d.M : ((w == d.W - 1) ? plans[i].M_top : d.M);
-            uint32_t ls = (uint32_t)log_S;
-            while (((wd.Mw + (RED_THREADS << ls) - 1) >> (8 + ls)) > (uint32_t)RED_THREADS) ++ls;
-            wd.log_S = ls;
-            wd.log_blk = 8 + ls;
-            wd.nb = (wd.Mw + (1u << wd.log_blk) - 1) >> wd.log_blk;
+            const uint32_t per_block_min =
+                (uint32_t)(((size_t)wd.Mw + (size_t)RED_THREADS * RED_THREADS - 1) /
+                           ((size_t)RED_THREADS * RED_THREADS));
+            wd.S = std::max<uint32_t>(S0, std::max<uint32_t>(1, per_block_min));
+            wd.blk = (uint32_t)RED_THREADS * wd.S;
+            wd.nb = (wd.Mw + wd.blk - 1) / wd.blk;
             wd.shift = d.row_stride ? 0u : d.c * w;
             wd.blk_base = (uint32_t)P.blks.size();
             for (uint32_t b = 0; b < wd.nb; ++b)

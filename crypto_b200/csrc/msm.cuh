@@ -33,9 +33,10 @@
 namespace kb200 {
 
 // Planner cost of one bucket of the reduction, in units of one accumulated
-// entry (mixed addition): two full additions plus the scan/tree phases,
-// measured on B200 at 2^20-2^22 (3.7 ns per bucket against 0.49 ns per entry).
-constexpr double RED_COST = 7.0;
+// entry (mixed addition): its two full additions.  (The reduction also has
+// a fixed per-block part, the scan and tree phases, that the per-bucket
+// model does not see; window choices were checked against measured times.)
+constexpr double RED_COST = 2.8;
 
 struct MsmPlan {
     int c = 0;          // window bits

@@ -32,10 +32,10 @@ struct ItemDesc {
 struct WinDesc {
     uint32_t bucket_base;  // global id of the window's bucket 0
     uint32_t Mw;           // live buckets of the window
-    uint32_t log_S;        // buckets per thread in reduction stage 1
+    uint32_t S;            // buckets per thread in reduction stage 1
     uint32_t blk_base;     // first stage-1 block of the window
     uint32_t nb;           // stage-1 blocks (<= RED_THREADS)
-    uint32_t log_blk;      // log2(RED_THREADS << log_S)
+    uint32_t blk;          // buckets per stage-1 block (RED_THREADS * S)
     uint32_t shift;        // c * w: the window's weight is 2^shift
 };
 

@@ -493,14 +493,16 @@ __device__ __forceinline__ void smem_tree_sum(uint32_t* sm) {
 }
 
 // Reduction stage 1.  Block -> (window, b) via its BlkDesc.  Thread t owns
-// S = 2^log_S consecutive buckets of the block's range; with R_t = sum_j B
-// and T_t = sum_j j B (j relative), the block's
+// S consecutive buckets of the block's range (S sized by the planner to fill
+// one wave evenly); with R_t = sum_j B and T_t = sum_j j B (j relative), the
+// block's
 //   Fb = sum_k k B_k = sum_t T_t + S * sum_{t>=1} Y_t,   Sb = Y_0,
 // where Y_t = sum_{t'>=t} R_t' (suffix scan in shared memory).
 // Every point lives in shared memory (SmXyzz): sA holds R_t, sB holds T_t,
 // and the two double as the ping-pong buffers of the scan once T is summed;
-// sX holds two stashed points (sum of T, Y_0).  Registers carry only the
-// addition formula's temporaries, so two 256-thread blocks fit per SM.
+// sX holds three stashed points (sum of T, Y_0, a copy for the [S] product).
+// Registers carry only the addition formula's temporaries, so two 256-thread
+// blocks fit per SM.
 template <class C>
 __global__ void __launch_bounds__(RED_THREADS, 2) k_reduce_blocks(RedArgs a) {
     using F = typename C::F;
@@ -513,8 +515,8 @@ __global__ void __launch_bounds__(RED_THREADS, 2) k_reduce_blocks(RedArgs a) {
     uint32_t* sX = smr + 2 * RED_THREADS * PW;
     const BlkDesc bd = a.blks[blockIdx.x];
     const WinDesc wd = a.wins[bd.win];
-    const uint32_t S = 1u << wd.log_S;
-    const uint32_t first = bd.b * (RED_THREADS << wd.log_S) + threadIdx.x * S;
+    const uint32_t S = wd.S;
+    const uint32_t first = bd.b * wd.blk + threadIdx.x * S;
     const int me = threadIdx.x;
     {
         const SP R{sA + me}, T{sB + me};
@@ -554,8 +556,14 @@ __global__ void __launch_bounds__(RED_THREADS, 2) k_reduce_blocks(RedArgs a) {
         __syncthreads();
     }
     if (me == 0) {
+        // Fb = [S] (sum of Y_t, t >= 1) + sum of T_t, by double-and-add
         const SP Fb{src};
-        for (uint32_t k = 0; k < wd.log_S; ++k) xyzz_dbl(Fb);
+        const S1 R{sX + 2 * PW};
+        xyzz_copy(R, Fb);
+        for (int b = 30 - __clz(S); b >= 0; --b) {
+            xyzz_dbl(Fb);
+            if ((S >> b) & 1u) xyzz_add(Fb, R);
+        }
         xyzz_add(Fb, S1{sX});
         Fb.to_global(a.blk_out + ((size_t)blockIdx.x * 2) * PW);
         S1{sX + PW}.to_global(a.blk_out + ((size_t)blockIdx.x * 2 + 1) * PW);
@@ -597,14 +605,14 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_windows(RedArgs a) {
     __syncthreads();
     smem_tree_sum<F>(sA);
     smem_tree_sum<F>(sB);
-    // Warp 0 finishes: V = 2^log_blk * (sum over b >= 1 of Y_b) + sum Fb + Y_0,
+    // Warp 0 finishes: V = [blk] (sum over b >= 1 of Y_b) + sum Fb + Y_0,
     // then the window weight 2^(c*w).  The doubling chains run with their
     // products spread over the warp's lanes (three product latencies per
     // doubling), one chain per window block, all windows in parallel.
     if (t < 32) {
         Xyzz<F> V, u;
         sm_load(V, sA, 0);
-        for (uint32_t k = 0; k < wd.log_blk; ++k) xyzz_dbl_warp(V);
+        xyzz_mul_small_warp(V, wd.blk);
         if (t == 0) {
             sm_load(u, sB, 0);
             xyzz_add(V, u);
@@ -717,7 +725,7 @@ struct MsmLaunchImpl {
         KB_LAUNCH_CHECK();
     }
     static size_t red_smem() { return (size_t)2 * RED_THREADS * 4 * F::N * 4; }
-    static size_t red_blocks_smem() { return red_smem() + (size_t)2 * 4 * F::N * 4; }
+    static size_t red_blocks_smem() { return red_smem() + (size_t)3 * 4 * F::N * 4; }
     static void reduce_blocks(const RedArgs& a, unsigned nblk, cudaStream_t st) {
         if (!nblk) return;
         set_smem_attr((const void*)k_reduce_blocks<C>, red_blocks_smem());
