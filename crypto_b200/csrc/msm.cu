@@ -300,10 +300,12 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
     P.total_scalars = tot_sc;
     // Reduction granularity: buckets per thread S (any integer) so that
     // stage 1 fills one wave of two resident 256-thread blocks per SM as
-    // evenly as the bucket count allows, and every window has at most
-    // RED_THREADS stage-1 blocks.
+    // evenly as the bucket count allows, up to 64 buckets per thread (past
+    // that, more waves of shorter serial chains run faster: BN254 at 2^24),
+    // and every window has at most RED_THREADS stage-1 blocks.
     const size_t per_wave = (size_t)2 * device_sms() * RED_THREADS;
-    const uint32_t S0 = (uint32_t)std::max<size_t>(1, (total_live + per_wave - 1) / per_wave);
+    const uint32_t S0 = (uint32_t)std::min<size_t>(
+        64, std::max<size_t>(1, (total_live + per_wave - 1) / per_wave));
     for (size_t i = 0; i < count; ++i) {
         ItemDesc& d = P.items[i];
         d.win_base = (uint32_t)P.wins.size();
