@@ -252,7 +252,6 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         const size_t n = items[i].n;
         if (n >= (1ull << 31) || items[i].point_off + n >= (1ull << 31))
             throw std::invalid_argument("msm: more than 2^31 points");
-        max_n = std::max(max_n, n);
         const bool glv = opt.glv && curve == 2 && opt.shift_c <= 0;
         if (glv) {
             plans[i] = make_msm_plan_glv(n, opt);
@@ -283,6 +282,10 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         d.row_stride = shifted ? (uint32_t)opt.shift_stride : 0u;
         d.Wr = shifted ? (n ? 1u : 0u) : d.W;
         if (n) total_live += shifted ? d.M : (size_t)(d.W - 1) * d.M + plans[i].M_top;
+        // Largest bucket: one entry per point per window feeding it (both GLV
+        // halves feed a window's buckets; a shifted table's windows share one
+        // bucket range).
+        max_n = std::max<size_t>(max_n, n * (glv ? 2 : 1) * (shifted ? d.W : 1));
         d.entry_base = L;
         d.bucket_base = (uint32_t)B;
         L += (unsigned long long)d.W * n * (glv ? 2u : 1u);
@@ -338,7 +341,7 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
     P.K = K;
     P.K2 = 8;
     P.nchunks = (size_t)((L + (unsigned long long)K - 1) / (unsigned long long)K);
-    // A bucket holds at most max_n entries, so spans at most max_n / K + 1
+    // A bucket holds at most max_n entries (see above), so spans at most max_n / K + 1
     // chunks; its chunk records fold in ceil(log_FK(span)) levels.  A big
     // bucket spans more than K2 + 1 chunks, so it owns at least K2 interior
     // chunks outright: at most nchunks / K2 buckets can be big.

@@ -79,3 +79,22 @@ def test_commit_errors(cuda_lib):
     assert L.kzg_commit_fr(None, 4, out) == -1
     # zero polynomial commits to infinity (0xC0 || 0...)
     assert kb().kzg_commit(b"\0" * 32 * 16) == b"\xc0" + bytes(47)
+
+
+def test_commit_with_every_window_in_one_bucket(cuda_lib):
+    """Coefficients whose digit is 1 in every window of the shifted-table
+    MSM: all W n entries land in one shared bucket (the planner's
+    largest-bucket bound must count every window)."""
+    n = 4096
+    rng = random.Random(77)
+    tau = rng.randrange(O.FR[2])
+    kb().kzg_srs_generate(tau.to_bytes(32, "little"), n)
+    srs = kb().kzg_srs_read(0, n)
+    coeffs = []
+    for i in range(n):
+        c = [13, 16, 19][i % 3]  # every window size the shifted tables use
+        v = sum(1 << (c * w) for w in range(255 // c))
+        coeffs.append((v % O.FR[2]).to_bytes(32, "little"))
+    ev = O.ntt(2, b"".join(coeffs))          # evaluations of that polynomial
+    want = O.compress(O.msm(2, b"".join(coeffs), srs, n))
+    assert kb().kzg_commit(ev) == want

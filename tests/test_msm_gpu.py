@@ -164,3 +164,20 @@ def test_many_big_buckets(cuda_lib, curve, logn, bits):
     scs = b"".join(rng.getrandbits(bits).to_bytes(32, "little") for _ in range(n))
     want = O.ref_msm(curve, scs, pts, n, threads=16) if O.ref_available() else O.msm(curve, scs, pts, n)
     assert kb().gpukit_multi_pippenger(curve, scs, pts, n) == want
+
+
+def test_glv_halves_share_a_bucket(cuda_lib):
+    """Scalars a + a*lambda: both GLV halves carry the same small digit, so
+    one bucket of window 0 receives 2n entries (the planner's largest-bucket
+    bound must count both halves)."""
+    lam = 0xAC45A4010001A40200000000FFFFFFFF
+    n = 1 << 14
+    pts = rand_points(2, n, seed=66)
+    rng = random.Random(66)
+    scs = []
+    for i in range(n):
+        a = rng.choice((3, 5)) if i % 7 else rng.randrange(1, 200)
+        scs.append(((a + a * lam) % O.FR[2]).to_bytes(32, "little"))
+    S = b"".join(scs)
+    want = O.ref_msm(2, S, pts, n, threads=16) if O.ref_available() else O.msm(2, S, pts, n)
+    assert kb().gpukit_multi_pippenger(2, S, pts, n) == want
