@@ -176,7 +176,7 @@ def test_glv_halves_share_a_bucket(cuda_lib):
     rng = random.Random(66)
     scs = []
     for i in range(n):
-        a = rng.choice((3, 5)) if i % 7 else rng.randrange(1, 200)
+        a = 3 if i % 10 else rng.randrange(1, 200)  # bucket 3 gets ~1.8 n entries
         scs.append(((a + a * lam) % O.FR[2]).to_bytes(32, "little"))
     S = b"".join(scs)
     want = O.ref_msm(2, S, pts, n, threads=16) if O.ref_available() else O.msm(2, S, pts, n)
