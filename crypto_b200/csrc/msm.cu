@@ -35,6 +35,12 @@ void set_smem_attr(const void* kernel, size_t bytes) {
 // Curve-independent sort kernels
 // ---------------------------------------------------------------------------
 
+// cnt[b] = ceil(m_b / 2) for the runs of a pairing level.
+__global__ void k_pair_counts(const uint32_t* __restrict__ in_off, uint32_t B, uint32_t* __restrict__ cnt) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < B) cnt[b] = (in_off[b + 1] - in_off[b] + 1) >> 1;
+}
+
 __global__ void k_histogram(const uint32_t* __restrict__ keys, unsigned long long total,
                             uint32_t* __restrict__ counts) {
     const unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -213,6 +219,10 @@ class MsmBatchPlan {
     uint32_t B = 0;
     int K = 64, K2 = 8, FK = 4, levels = 0;
     size_t nchunks = 0, big_cap = 0;
+    // Batch-affine pairing levels before the accumulation, and bounds on
+    // each level's output length (level l: (len_{l-1} + B) / 2).
+    int pair_levels = 0;
+    std::vector<unsigned long long> pair_len;
     DevBuf d_items, d_wins, d_blks;
     ~MsmBatchPlan() {
         d_items.release();
@@ -329,6 +339,24 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
             P.wins.push_back(wd);
         }
     }
+    // Pairing levels: while buckets hold at least PAIR_MIN_RUN entries on
+    // average, pairing every run's neighbours in affine coordinates (about 6
+    // products per addition) beats the mixed XYZZ accumulation (10).  Each
+    // level's output is bounded by (len + B) / 2 (a run of m gives ceil(m/2)).
+    P.pair_levels = 0;
+    P.pair_len.clear();
+    {
+        const int max_levels = opt.pair_levels >= 0 ? opt.pair_levels : 4;
+        unsigned long long len = L;
+        while (P.pair_levels < max_levels && total_live > 0 &&
+               (opt.pair_levels >= 0 || (double)len >= PAIR_MIN_RUN * (double)total_live)) {
+            len = (len + B) / 2;
+            P.pair_len.push_back(len);
+            ++P.pair_levels;
+        }
+        L = len;  // entries left for the accumulation (upper bound)
+        for (int l = 0; l < P.pair_levels; ++l) max_n = (max_n + 1) / 2;
+    }
     // Chunk length: long chunks amortise the per-chunk records, but there must
     // be at least two chunks per resident accumulation thread.
     int K = opt.force_K;
@@ -407,7 +435,8 @@ class MsmEngine {
    public:
     int curve = 0;
     DevBuf table, keys, vals, counts, offsets, cursor, sorted, rec_first, rec_last, fold_buf,
-        buckets, blk_out, win_out, scan_tmp, queue, fold_counts, fold_prefix;
+        buckets, blk_out, win_out, scan_tmp, queue, fold_counts, fold_prefix, pair_off[2],
+        pair_rows[2];
     std::map<std::tuple<size_t, bool, int, int, int, size_t, bool, size_t>, MsmBatchPlan*> single_plans;
     cudaEvent_t ev[N_STAGE_EVENTS] = {};
     bool ev_ready = false, ev_recorded = false;
@@ -487,6 +516,13 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
     e->fold_counts.reserve((P.big_cap + 1) * 4, st);
     e->fold_prefix.reserve((P.big_cap + 1) * 4, st);
     e->queue.reserve((P.big_cap + 8) * 4, st);
+    if (P.pair_levels > 0) {
+        const size_t TW = (size_t)msm_launchers(e->curve).table_words;
+        for (int k = 0; k < 2 && k < P.pair_levels; ++k) {
+            e->pair_off[k].reserve(((size_t)P.B + 1) * 4, st);
+            e->pair_rows[k].reserve(std::max<unsigned long long>(1, P.pair_len[k]) * TW * 4, st);
+        }
+    }
 }
 
 void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_scalars,
@@ -517,10 +553,33 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
                                                        e->sorted.as<uint32_t>());
         KB_LAUNCH_CHECK();
     }
+    // Pairing levels: the sorted runs shrink to about half per level, the
+    // accumulation then reads the last level's rows directly.
+    const uint32_t* off = e->offsets.as<uint32_t>();
+    const uint32_t* acc_sorted = e->sorted.as<uint32_t>();
+    const uint32_t* acc_table = d_table;
+    for (int l = 0; l < P.pair_levels && P.L > 0; ++l) {
+        uint32_t* out_off = e->pair_off[l & 1].as<uint32_t>();
+        k_pair_counts<<<ceil_div_u(P.B, 256), 256, 0, st>>>(off, P.B, e->counts.as<uint32_t>());
+        KB_LAUNCH_CHECK();
+        exclusive_scan_u32(e->counts.as<uint32_t>(), out_off, P.B, 0, e->scan_tmp.as<uint32_t>(), st);
+        PairArgs pa;
+        pa.in_off = off;
+        pa.out_off = out_off;
+        pa.B = P.B;
+        pa.sorted = acc_sorted;
+        pa.src = acc_table;
+        pa.dst = e->pair_rows[l & 1].as<uint32_t>();
+        const unsigned long long slots = P.pair_len[l];
+        K.pair_level(pa, (unsigned)ceil_div_u(slots, (unsigned long long)128 * 8), st);
+        off = out_off;
+        acc_sorted = nullptr;
+        acc_table = e->pair_rows[l & 1].as<uint32_t>();
+    }
     KB_CUDA(cudaMemsetAsync(e->queue.ptr, 0, 8, st));  // work counter, big-bucket count
     uint32_t* big_list = e->queue.as<uint32_t>() + 1;
     if (P.B > 0 && P.levels >= 1) {
-        k_list_big<<<ceil_div_u(P.B, 256), 256, 0, st>>>(e->offsets.as<uint32_t>(), P.B,
+        k_list_big<<<ceil_div_u(P.B, 256), 256, 0, st>>>(off, P.B,
                                                         (uint32_t)P.K, P.K2, (uint32_t)P.big_cap,
                                                         big_list);
         KB_LAUNCH_CHECK();
@@ -528,11 +587,11 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
     e->mark(3, st);
 
     AccArgs acc;
-    acc.sorted = e->sorted.as<uint32_t>();
-    acc.offsets = e->offsets.as<uint32_t>();
+    acc.sorted = acc_sorted;
+    acc.offsets = off;
     acc.B = P.B;
     acc.K = (uint32_t)P.K;
-    acc.table = d_table;
+    acc.table = acc_table;
     acc.rec_first = e->rec_first.as<uint32_t>();
     acc.rec_last = e->rec_last.as<uint32_t>();
     acc.buckets = e->buckets.as<uint32_t>();
@@ -547,7 +606,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
 
     if (P.levels >= 1 && P.L > 0) {
         FoldArgs fa;
-        fa.offsets = e->offsets.as<uint32_t>();
+        fa.offsets = off;
         fa.B = P.B;
         fa.K = (uint32_t)P.K;
         fa.K2 = P.K2;
@@ -560,7 +619,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
         uint32_t* out = e->fold_buf.as<uint32_t>();
         for (int l = 2; l <= P.levels + 1; ++l) {
             k_fold_counts<<<ceil_div_u(P.big_cap, 256), 256, 0, st>>>(
-                e->offsets.as<uint32_t>(), (uint32_t)P.K, P.FK, l, big_list, (uint32_t)P.big_cap,
+                off, (uint32_t)P.K, P.FK, l, big_list, (uint32_t)P.big_cap,
                 e->fold_counts.as<uint32_t>());
             KB_LAUNCH_CHECK();
             exclusive_scan_u32(e->fold_counts.as<uint32_t>(), e->fold_prefix.as<uint32_t>(),
@@ -572,7 +631,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
     e->mark(5, st);
 
     RedArgs ra;
-    ra.offsets = e->offsets.as<uint32_t>();
+    ra.offsets = off;
     ra.B = P.B;
     ra.buckets = e->buckets.as<uint32_t>();
     ra.rec_first = e->rec_first.as<uint32_t>();

@@ -68,7 +68,12 @@ struct MsmOptions {
     bool glv = false;
     size_t glv_rows = 0;
     bool no_glv = false;  // msm_run_wire: keep the plain 256-bit windows
+    int pair_levels = -1; // batch-affine pairing levels (-1: planner's choice)
 };
+
+// Average entries per live bucket from which a batch-affine pairing level
+// runs before the accumulation.
+constexpr double PAIR_MIN_RUN = 4.0;
 
 // Windows of a c-bit signed-digit decomposition of 256-bit scalars.
 int msm_windows_for(int c);

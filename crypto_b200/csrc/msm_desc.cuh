@@ -49,7 +49,7 @@ struct BlkDesc {
 // bucket's run (when different) to rec_last[t], and of every bucket lying
 // strictly inside the chunk directly to buckets[].
 struct AccArgs {
-    const uint32_t* sorted;
+    const uint32_t* sorted;   // entry -> table row | sign << 31 (null: entry e is row e)
     const uint32_t* offsets;  // B + 1 bucket offsets into sorted; offsets[B] = entries
     uint32_t B;
     uint32_t K;               // entries per chunk
@@ -76,6 +76,18 @@ struct FoldArgs {
     uint32_t* rec_first;
 };
 
+// Batch-affine pairing level: the bucket-sorted list (runs in_off[b] ..
+// in_off[b+1]) -> each run's consecutive pairs added in affine coordinates
+// (an odd run's last point passes through), output runs at out_off.
+struct PairArgs {
+    const uint32_t* in_off;   // B + 1
+    const uint32_t* out_off;  // B + 1
+    uint32_t B;
+    const uint32_t* sorted;   // level 0: table rows | sign << 31; later levels: null
+    const uint32_t* src;      // level 0: the point table; later: previous level's rows
+    uint32_t* dst;            // output rows (affine, 2N words, infinity flagged)
+};
+
 struct RedArgs {
     const uint32_t* offsets;
     uint32_t B;
@@ -96,6 +108,7 @@ struct MsmLaunchers {
     void (*recode)(const ItemDesc*, uint32_t, unsigned long long, const uint32_t*,
                    const uint32_t*, uint32_t*, uint32_t*, cudaStream_t);
     void (*accumulate)(const AccArgs&, unsigned, cudaStream_t);
+    void (*pair_level)(const PairArgs&, unsigned, cudaStream_t);
     void (*glv_rows)(uint32_t*, size_t, cudaStream_t);
     void (*fold)(const FoldArgs&, int, const uint32_t*, uint32_t*, unsigned, cudaStream_t);
     void (*reduce_blocks)(const RedArgs&, unsigned, cudaStream_t);

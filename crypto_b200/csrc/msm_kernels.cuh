@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(128, C::ACC_MIN_BLOCKS) k_accumulate(AccArgs a
             uint32_t bend = a.offsets[b + 1];
             uint32_t run0 = e0;
             acc.set_inf();
-            uint32_t v = a.sorted[e0];
+            uint32_t v = a.sorted ? a.sorted[e0] : e0;
             for (uint32_t e = e0; e < e1; ++e) {
                 if (e == bend) {
                     // flush the finished run [run0, e) of bucket b
@@ -346,19 +346,188 @@ __global__ void __launch_bounds__(128, C::ACC_MIN_BLOCKS) k_accumulate(AccArgs a
                     bend = a.offsets[b + 1];
                     run0 = e;
                 }
-                const uint32_t vn = (e + 1 < e1) ? a.sorted[e + 1] : 0u;
+                const uint32_t vn = (e + 1 < e1) ? (a.sorted ? a.sorted[e + 1] : e + 1) : 0u;
                 if (e + 1 < e1) {
                     const uint32_t* nxt = a.table + (size_t)(vn & 0x7fffffffu) * 2 * F::N;
                     asm volatile("prefetch.global.L2 [%0];" ::"l"(nxt));
                 }
-                Affine<F> p;
-                load_table_point<F>(p, a.table, v & 0x7fffffffu);
-                if (v >> 31) fe_neg(p.y, p.y);
-                xyzz_add_affine(acc, p);
+                const uint32_t* row = a.table + (size_t)(v & 0x7fffffffu) * 2 * F::N;
+                if (!aff_is_inf_words<F>(row)) {  // pairing levels can produce infinity
+                    Affine<F> p;
+                    load_table_point<F>(p, a.table, v & 0x7fffffffu);
+                    if (v >> 31) fe_neg(p.y, p.y);
+                    xyzz_add_affine(acc, p);
+                }
                 v = vn;
             }
             uint32_t* dst = (run0 == e0) ? a.rec_first + (size_t)t * PW : a.rec_last + (size_t)t * PW;
             acc.to_global(dst);
+        }
+    }
+}
+
+// ---- Batch-affine pairing levels -------------------------------------------
+// Thread t of the grid owns output slots [PAIR_J t, PAIR_J t + PAIR_J).  Slot k
+// of bucket b adds input points i0 = in_off[b] + 2 (k - out_off[b]) and
+// i0 + 1 (if still in the run) in affine coordinates:
+//   lambda = (y1 - y0) / (x1 - x0)  (or 3 x0^2 / 2 y0 when the points are
+//   equal), x3 = lambda^2 - x0 - x1, y3 = lambda (x0 - x3) - y0,
+// and infinity where the points cancel.  The denominators of a warp's 256
+// slots share one inversion (Montgomery's trick): per-thread prefix products
+// in shared memory, inclusive prefix and suffix products of the thread
+// totals across the warp by shuffles, one binary-Euclid inversion on lane 0,
+// then a backward pass that recovers each slot's inverse.  About 6 products
+// per addition against the 10 of a mixed XYZZ addition.
+constexpr int PAIR_T = 128;
+constexpr int PAIR_J = 8;
+
+enum PairCase : int { PAIR_PASS0 = 0, PAIR_PASS1 = 1, PAIR_INF = 2, PAIR_ADD = 3, PAIR_DBL = 4 };
+
+template <class F>
+__device__ __forceinline__ void pair_load(const PairArgs& a, uint32_t i, Affine<F>& P, bool& inf) {
+    if (a.sorted) {
+        const uint32_t v = a.sorted[i];
+        aff_load(P, a.src + (size_t)(v & 0x7fffffffu) * 2 * F::N);
+        if (v >> 31) fe_neg(P.y, P.y);
+        inf = false;  // the recode drops infinity entries
+    } else {
+        const uint32_t* row = a.src + (size_t)i * 2 * F::N;
+        inf = aff_is_inf_words<F>(row);
+        aff_load(P, row);
+    }
+}
+
+// Loads slot k's operands (bucket b) and classifies it; den is the
+// denominator that joins the batch inversion (one for the non-additions).
+template <class F>
+__device__ __forceinline__ int pair_setup(const PairArgs& a, uint32_t k, uint32_t b, Affine<F>& P0,
+                                          Affine<F>& P1, bool& inf0, Fe<F>& den) {
+    const uint32_t i0 = a.in_off[b] + 2 * (k - a.out_off[b]);
+    const bool has1 = i0 + 1 < a.in_off[b + 1];
+    bool inf1 = true;
+    pair_load<F>(a, i0, P0, inf0);
+    if (has1) pair_load<F>(a, i0 + 1, P1, inf1);
+    fe_one(den);
+    if (inf1) return PAIR_PASS0;
+    if (inf0) return PAIR_PASS1;
+    if (!fe_eq(P0.x, P1.x)) {
+        fe_sub(den, P1.x, P0.x);
+        return PAIR_ADD;
+    }
+    if (fe_eq(P0.y, P1.y) && !fe_is_zero(P0.y)) {
+        fe_dbl(den, P0.y);
+        return PAIR_DBL;
+    }
+    return PAIR_INF;
+}
+
+template <class F>
+__device__ __forceinline__ void smp_store(uint32_t* sm, int j, int t, const Fe<F>& x) {
+#pragma unroll
+    for (int q = 0; q < F::N; ++q) sm[(j * F::N + q) * PAIR_T + t] = x.v[q];
+}
+template <class F>
+__device__ __forceinline__ void smp_load(Fe<F>& x, const uint32_t* sm, int j, int t) {
+#pragma unroll
+    for (int q = 0; q < F::N; ++q) x.v[q] = sm[(j * F::N + q) * PAIR_T + t];
+}
+
+template <class C>
+__global__ void __launch_bounds__(PAIR_T) k_pair_level(PairArgs a) {
+    using F = typename C::F;
+    constexpr int N = F::N;
+    __shared__ uint32_t s_pre[PAIR_J * N * PAIR_T];
+    const int t = threadIdx.x;
+    const int lane = t & 31;
+    const uint32_t total = a.out_off[a.B];
+    const uint32_t k0 = (blockIdx.x * PAIR_T + (uint32_t)t) * PAIR_J;
+    uint32_t b0 = k0 < total ? bucket_of(a.out_off, a.B, k0) : 0u;
+    // pass 1: prefix products of the denominators
+    Fe<F> run;
+    fe_one(run);
+    {
+        uint32_t b = b0;
+        for (int j = 0; j < PAIR_J; ++j) {
+            const uint32_t k = k0 + (uint32_t)j;
+            if (k < total) {
+                while (a.out_off[b + 1] <= k) ++b;
+                Affine<F> P0, P1;
+                bool inf0;
+                Fe<F> den;
+                pair_setup<F>(a, k, b, P0, P1, inf0, den);
+                fe_mul(run, run, den);
+            }
+            smp_store(s_pre, j, t, run);
+        }
+    }
+    // warp: inclusive prefix P and suffix S of the thread totals
+    Fe<F> P = run, S = run, o;
+    for (int d = 1; d < 32; d <<= 1) {
+#pragma unroll
+        for (int q = 0; q < N; ++q) o.v[q] = __shfl_up_sync(0xffffffffu, P.v[q], d);
+        if (lane >= d) fe_mul(P, P, o);
+#pragma unroll
+        for (int q = 0; q < N; ++q) o.v[q] = __shfl_down_sync(0xffffffffu, S.v[q], d);
+        if (lane + d < 32) fe_mul(S, S, o);
+    }
+    Fe<F> inv_total;
+    fe_bcast(inv_total, P, 31);
+    if (lane == 0) fe_inv_binary(inv_total, inv_total);
+    fe_bcast(inv_total, inv_total, 0);
+    // inverse of this thread's total: inv_total * P_{lane-1} * S_{lane+1}
+    Fe<F> inv_run = inv_total;
+#pragma unroll
+    for (int q = 0; q < N; ++q) o.v[q] = __shfl_up_sync(0xffffffffu, P.v[q], 1);
+    if (lane > 0) fe_mul(inv_run, inv_run, o);
+#pragma unroll
+    for (int q = 0; q < N; ++q) o.v[q] = __shfl_down_sync(0xffffffffu, S.v[q], 1);
+    if (lane < 31) fe_mul(inv_run, inv_run, o);
+    // pass 2 (backward): each slot's inverse, then its sum
+    if (k0 >= total) return;
+    const uint32_t kend = min(k0 + (uint32_t)PAIR_J, total);
+    uint32_t bend = bucket_of(a.out_off, a.B, kend - 1);
+    for (int j = (int)(kend - k0) - 1; j >= 0; --j) {
+        const uint32_t k = k0 + (uint32_t)j;
+        while (a.out_off[bend] > k) --bend;
+        Affine<F> P0, P1;
+        bool inf0;
+        Fe<F> den, inv;
+        const int kind = pair_setup<F>(a, k, bend, P0, P1, inf0, den);
+        if (j > 0) {
+            Fe<F> pre;
+            smp_load(pre, s_pre, j - 1, t);
+            fe_mul(inv, inv_run, pre);
+        } else {
+            inv = inv_run;
+        }
+        fe_mul(inv_run, inv_run, den);
+        uint32_t* dst = a.dst + (size_t)k * 2 * N;
+        if (kind == PAIR_ADD || kind == PAIR_DBL) {
+            Fe<F> lam, x3, y3;
+            if (kind == PAIR_ADD) {
+                fe_sub(lam, P1.y, P0.y);
+            } else {
+                fe_sqr(lam, P0.x);
+                fe_dbl(x3, lam);
+                fe_add(lam, lam, x3);  // 3 x0^2
+                P1.x = P0.x;
+            }
+            fe_mul(lam, lam, inv);
+            fe_sqr(x3, lam);
+            fe_sub(x3, x3, P0.x);
+            fe_sub(x3, x3, P1.x);
+            fe_sub(y3, P0.x, x3);
+            fe_mul(y3, lam, y3);
+            fe_sub(y3, y3, P0.y);
+            fe_store(dst, x3);
+            fe_store(dst + N, y3);
+        } else if (kind == PAIR_INF || (kind == PAIR_PASS0 && inf0)) {
+            for (int q = 0; q < 2 * N; ++q) dst[q] = 0;
+            dst[N - 1] = INF_FLAG;
+        } else {
+            const Affine<F>& R = kind == PAIR_PASS0 ? P0 : P1;
+            fe_store(dst, R.x);
+            fe_store(dst + N, R.y);
         }
     }
 }
@@ -708,6 +877,11 @@ struct MsmLaunchImpl {
                                                            keys, vals);
         KB_LAUNCH_CHECK();
     }
+    static void pair_level(const PairArgs& a, unsigned grid, cudaStream_t st) {
+        if (!grid) return;
+        k_pair_level<C><<<grid, PAIR_T, 0, st>>>(a);
+        KB_LAUNCH_CHECK();
+    }
     static void glv_rows(uint32_t* table, size_t n, cudaStream_t st) {
         if constexpr (C::CURVE_ID == 2) {
             if (!n) return;
@@ -756,6 +930,7 @@ struct MsmLaunchImpl {
         L.recode = &recode;
         L.accumulate = &accumulate;
         L.glv_rows = &glv_rows;
+        L.pair_level = &pair_level;
         L.fold = &fold;
         L.reduce_blocks = &reduce_blocks;
         L.reduce_windows = &reduce_windows;
