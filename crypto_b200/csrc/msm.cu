@@ -346,7 +346,15 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
     P.pair_levels = 0;
     P.pair_len.clear();
     {
-        const int max_levels = opt.pair_levels >= 0 ? opt.pair_levels : 4;
+        // Off unless asked for (MsmOptions::pair_levels or KB200_MSM_PAIR_LEVELS):
+        // measured on B200 at 2^22 the levels cost about twice the time per
+        // addition of the accumulation they replace (latency of the prefix
+        // chains and of the per-block inversion), so the default is none.
+        static const int env_levels = [] {
+            const char* v = std::getenv("KB200_MSM_PAIR_LEVELS");
+            return v && *v ? std::atoi(v) : 0;
+        }();
+        const int max_levels = opt.pair_levels >= 0 ? opt.pair_levels : env_levels;
         unsigned long long len = L;
         while (P.pair_levels < max_levels && total_live > 0 &&
                (opt.pair_levels >= 0 || (double)len >= PAIR_MIN_RUN * (double)total_live)) {
@@ -571,7 +579,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
         pa.src = acc_table;
         pa.dst = e->pair_rows[l & 1].as<uint32_t>();
         const unsigned long long slots = P.pair_len[l];
-        K.pair_level(pa, (unsigned)ceil_div_u(slots, (unsigned long long)128 * 8), st);
+        K.pair_level(pa, (unsigned)ceil_div_u(slots, (unsigned long long)256 * 8), st);
         off = out_off;
         acc_sorted = nullptr;
         acc_table = e->pair_rows[l & 1].as<uint32_t>();

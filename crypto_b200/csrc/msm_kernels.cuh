@@ -372,13 +372,14 @@ __global__ void __launch_bounds__(128, C::ACC_MIN_BLOCKS) k_accumulate(AccArgs a
 // i0 + 1 (if still in the run) in affine coordinates:
 //   lambda = (y1 - y0) / (x1 - x0)  (or 3 x0^2 / 2 y0 when the points are
 //   equal), x3 = lambda^2 - x0 - x1, y3 = lambda (x0 - x3) - y0,
-// and infinity where the points cancel.  The denominators of a warp's 256
+// and infinity where the points cancel.  The denominators of a block's 2048
 // slots share one inversion (Montgomery's trick): per-thread prefix products
 // in shared memory, inclusive prefix and suffix products of the thread
-// totals across the warp by shuffles, one binary-Euclid inversion on lane 0,
-// then a backward pass that recovers each slot's inverse.  About 6 products
-// per addition against the 10 of a mixed XYZZ addition.
-constexpr int PAIR_T = 128;
+// totals across the warp by shuffles, one binary-Euclid inversion per block
+// of warps (thread 0), then a backward pass that recovers each slot's
+// inverse.  About 6 products per addition against the 10 of a mixed XYZZ
+// addition.
+constexpr int PAIR_T = 256;
 constexpr int PAIR_J = 8;
 
 enum PairCase : int { PAIR_PASS0 = 0, PAIR_PASS1 = 1, PAIR_INF = 2, PAIR_ADD = 3, PAIR_DBL = 4 };
@@ -433,10 +434,13 @@ __device__ __forceinline__ void smp_load(Fe<F>& x, const uint32_t* sm, int j, in
 }
 
 template <class C>
-__global__ void __launch_bounds__(PAIR_T) k_pair_level(PairArgs a) {
+__global__ void __launch_bounds__(PAIR_T, 2) k_pair_level(PairArgs a) {
     using F = typename C::F;
     constexpr int N = F::N;
-    __shared__ uint32_t s_pre[PAIR_J * N * PAIR_T];
+    constexpr int NW = PAIR_T / 32;
+    extern __shared__ __align__(16) uint32_t s_pre[];  // PAIR_J * N * PAIR_T words
+    __shared__ uint32_t s_wt[NW * N];                  // warp totals, then their inverses
+    const int warp = threadIdx.x >> 5;
     const int t = threadIdx.x;
     const int lane = t & 31;
     const uint32_t total = a.out_off[a.B];
@@ -470,10 +474,31 @@ __global__ void __launch_bounds__(PAIR_T) k_pair_level(PairArgs a) {
         for (int q = 0; q < N; ++q) o.v[q] = __shfl_down_sync(0xffffffffu, S.v[q], d);
         if (lane + d < 32) fe_mul(S, S, o);
     }
+    // block: one inversion for all warps' totals (thread 0), then each
+    // warp's inverse by Montgomery's trick over the NW warp totals
+    if (lane == 31) fe_store(s_wt + warp * N, P);
+    __syncthreads();
+    if (t == 0) {
+        Fe<F> pre[NW], w, inv, x;
+        fe_load(pre[0], s_wt);
+        for (int q = 1; q < NW; ++q) {
+            fe_load(w, s_wt + q * N);
+            fe_mul(pre[q], pre[q - 1], w);
+        }
+        fe_inv_binary(inv, pre[NW - 1]);
+        for (int q = NW - 1; q >= 0; --q) {
+            fe_load(w, s_wt + q * N);
+            if (q > 0)
+                fe_mul(x, inv, pre[q - 1]);
+            else
+                x = inv;
+            fe_mul(inv, inv, w);
+            fe_store(s_wt + q * N, x);  // 1 / (warp q's total)
+        }
+    }
+    __syncthreads();
     Fe<F> inv_total;
-    fe_bcast(inv_total, P, 31);
-    if (lane == 0) fe_inv_binary(inv_total, inv_total);
-    fe_bcast(inv_total, inv_total, 0);
+    fe_load(inv_total, s_wt + warp * N);
     // inverse of this thread's total: inv_total * P_{lane-1} * S_{lane+1}
     Fe<F> inv_run = inv_total;
 #pragma unroll
@@ -879,7 +904,9 @@ struct MsmLaunchImpl {
     }
     static void pair_level(const PairArgs& a, unsigned grid, cudaStream_t st) {
         if (!grid) return;
-        k_pair_level<C><<<grid, PAIR_T, 0, st>>>(a);
+        const size_t smem = (size_t)PAIR_J * F::N * PAIR_T * 4;
+        set_smem_attr((const void*)k_pair_level<C>, smem);
+        k_pair_level<C><<<grid, PAIR_T, smem, st>>>(a);
         KB_LAUNCH_CHECK();
     }
     static void glv_rows(uint32_t* table, size_t n, cudaStream_t st) {

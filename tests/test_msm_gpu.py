@@ -181,3 +181,37 @@ def test_glv_halves_share_a_bucket(cuda_lib):
     S = b"".join(scs)
     want = O.ref_msm(2, S, pts, n, threads=16) if O.ref_available() else O.msm(2, S, pts, n)
     assert kb().gpukit_multi_pippenger(2, S, pts, n) == want
+
+
+def test_pairing_levels_bit_exact(cuda_lib):
+    """The batch-affine pairing levels (off by default, KB200_MSM_PAIR_LEVELS)
+    give the same bytes: run in a child process with two levels, on inputs
+    with long runs per bucket, repeated points and cancelling pairs."""
+    import os
+    import subprocess
+    import sys
+    code = r'''
+import random, sys
+sys.path.insert(0, "tests")
+import crypto_b200 as kb, _oracle as O
+for curve, n in ((2, 1 << 13), (1, 1 << 13)):
+    rng = random.Random(curve)
+    base = [O.g1_mul_gen(curve, rng.randrange(1, O.FR[curve])) for _ in range(64)]
+    pts, scs = [], []
+    for i in range(n):
+        p = base[i % 64]
+        if i % 5 == 1:
+            p = pts[-1]                                # repeated point in the same bucket
+        if i % 11 == 2:
+            p = O.g1_mul(curve, pts[-1], O.FR[curve] - 1)  # its negation: cancels
+        pts.append(p)
+        scs.append(rng.choice((1, 2, 3, 7, 1 << 70)).to_bytes(32, "little"))
+    P, S = b"".join(pts), b"".join(scs)
+    assert kb.gpukit_multi_pippenger(curve, S, P, n) == O.msm(curve, S, P, n), curve
+print("ok")
+'''
+    env = dict(os.environ, KB200_MSM_PAIR_LEVELS="2")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True,
+                         text=True, timeout=600)
+    assert out.returncode == 0 and "ok" in out.stdout, out.stdout + out.stderr
