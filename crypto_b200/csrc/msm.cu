@@ -35,6 +35,11 @@ void set_smem_attr(const void* kernel, size_t bytes) {
 // Curve-independent sort kernels
 // ---------------------------------------------------------------------------
 
+// Threads of a pairing level with at most `slots` output slots.
+static uint32_t pair_threads(unsigned long long slots) {
+    return (uint32_t)((slots + PAIR_J - 1) / PAIR_J);
+}
+
 // cnt[b] = ceil(m_b / 2) for the runs of a pairing level.
 __global__ void k_pair_counts(const uint32_t* __restrict__ in_off, uint32_t B, uint32_t* __restrict__ cnt) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -340,24 +345,26 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         }
     }
     // Pairing levels: while buckets hold at least PAIR_MIN_RUN entries on
-    // average, pairing every run's neighbours in affine coordinates (about 6
-    // products per addition) beats the mixed XYZZ accumulation (10).  Each
-    // level's output is bounded by (len + B) / 2 (a run of m gives ceil(m/2)).
+    // average, pairing every run's neighbours in affine coordinates (6
+    // products per addition, one inversion per level) beats the mixed XYZZ
+    // accumulation (10 products), once a level has enough additions to repay
+    // its fixed cost (about ten launches and one inversion on one thread,
+    // 0.25 ms against 0.13 ns saved per addition).  Each level's output is bounded by
+    // (len + B) / 2 (a run of m gives ceil(m/2)).  KB200_MSM_PAIR_LEVELS or
+    // MsmOptions::pair_levels fixes the number of levels instead.
     P.pair_levels = 0;
     P.pair_len.clear();
     {
-        // Off unless asked for (MsmOptions::pair_levels or KB200_MSM_PAIR_LEVELS):
-        // measured on B200 at 2^22 the levels cost about twice the time per
-        // addition of the accumulation they replace (latency of the prefix
-        // chains and of the per-block inversion), so the default is none.
         static const int env_levels = [] {
             const char* v = std::getenv("KB200_MSM_PAIR_LEVELS");
-            return v && *v ? std::atoi(v) : 0;
+            return v && *v ? std::atoi(v) : -1;
         }();
-        const int max_levels = opt.pair_levels >= 0 ? opt.pair_levels : env_levels;
+        const int fixed = opt.pair_levels >= 0 ? opt.pair_levels : env_levels;
+        const int max_levels = fixed >= 0 ? fixed : PAIR_MAX_LEVELS;
         unsigned long long len = L;
         while (P.pair_levels < max_levels && total_live > 0 &&
-               (opt.pair_levels >= 0 || (double)len >= PAIR_MIN_RUN * (double)total_live)) {
+               (fixed >= 0 || ((double)len >= PAIR_MIN_RUN * (double)total_live &&
+                               len / 2 >= PAIR_MIN_SLOTS))) {
             len = (len + B) / 2;
             P.pair_len.push_back(len);
             ++P.pair_levels;
@@ -444,7 +451,7 @@ class MsmEngine {
     int curve = 0;
     DevBuf table, keys, vals, counts, offsets, cursor, sorted, rec_first, rec_last, fold_buf,
         buckets, blk_out, win_out, scan_tmp, queue, fold_counts, fold_prefix, pair_off[2],
-        pair_rows[2];
+        pair_rows[2], pair_scratch;
     std::map<std::tuple<size_t, bool, int, int, int, size_t, bool, size_t>, MsmBatchPlan*> single_plans;
     cudaEvent_t ev[N_STAGE_EVENTS] = {};
     bool ev_ready = false, ev_recorded = false;
@@ -478,6 +485,16 @@ MsmEngine* msm_engine_create(int curve) {
 
 void msm_engine_destroy(MsmEngine* e) { delete e; }
 
+// Pairing levels of a batch that holds an item of L entries over B buckets
+// (counted for every item: a batch pairs globally): its share of the two
+// level row buffers ((L + B) / 2 and (L + 3B) / 4 rows of TW bytes), the
+// level offsets and the inversion scratch of the first level.
+static size_t pair_item_bytes(size_t TW, size_t L, size_t B) {
+    const size_t len0 = (L + B) / 2 + 1, len1 = (L + 3 * B) / 4 + 1;
+    return (len0 + len1) * TW + 8 * (B + 1) +
+           pair_scratch_words(pair_threads(len0) + 1, (int)(TW / 8)) * 4;
+}
+
 // Upper bounds without building a plan (admission control calls these per
 // request).  Per item, with its plain-table window plan: keys, vals and the
 // sorted list (4 B per entry each), three 4 B bucket arrays and the bucket
@@ -487,7 +504,8 @@ size_t msm_item_scratch_bytes(int curve, size_t n) {
     const MsmPlan p = make_msm_plan(curve, n, MsmOptions());
     const size_t L = (size_t)p.W * n, B = (size_t)p.W * p.M;
     return 12 * L + 12 * (B + 1) + B * PW + (size_t)p.W * (2 * RED_THREADS + 1) * PW +
-           (L / 64 + 1) * (3 * PW + 4);  // chunk records once lists are long (K = 64)
+           (L / 64 + 1) * (3 * PW + 4) +  // chunk records once lists are long (K = 64)
+           pair_item_bytes(PW / 2, L, B);
 }
 
 // Per batch: the chunk records of short lists (K < 64 keeps at most about two
@@ -530,6 +548,7 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
             e->pair_off[k].reserve(((size_t)P.B + 1) * 4, st);
             e->pair_rows[k].reserve(std::max<unsigned long long>(1, P.pair_len[k]) * TW * 4, st);
         }
+        e->pair_scratch.reserve(pair_scratch_words(pair_threads(P.pair_len[0]), (int)TW / 2) * 4, st);
     }
 }
 
@@ -579,7 +598,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
         pa.src = acc_table;
         pa.dst = e->pair_rows[l & 1].as<uint32_t>();
         const unsigned long long slots = P.pair_len[l];
-        K.pair_level(pa, (unsigned)ceil_div_u(slots, (unsigned long long)256 * 8), st);
+        K.pair_level(pa, pair_threads(slots), e->pair_scratch.as<uint32_t>(), st);
         off = out_off;
         acc_sorted = nullptr;
         acc_table = e->pair_rows[l & 1].as<uint32_t>();

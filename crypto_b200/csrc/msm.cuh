@@ -68,12 +68,14 @@ struct MsmOptions {
     bool glv = false;
     size_t glv_rows = 0;
     bool no_glv = false;  // msm_run_wire: keep the plain 256-bit windows
-    int pair_levels = -1; // batch-affine pairing levels (-1: planner's choice)
+    int pair_levels = -1; // batch-affine pairing levels (-1: planner's choice or KB200_MSM_PAIR_LEVELS)
 };
 
 // Average entries per live bucket from which a batch-affine pairing level
-// runs before the accumulation.
-constexpr double PAIR_MIN_RUN = 4.0;
+// runs before the accumulation, and the most levels the planner runs.
+constexpr double PAIR_MIN_RUN = 8.0;
+constexpr int PAIR_MAX_LEVELS = 4;
+constexpr unsigned long long PAIR_MIN_SLOTS = 1ull << 21;  // additions per level
 
 // Windows of a c-bit signed-digit decomposition of 256-bit scalars.
 int msm_windows_for(int c);

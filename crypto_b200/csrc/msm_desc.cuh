@@ -88,6 +88,26 @@ struct PairArgs {
     uint32_t* dst;            // output rows (affine, 2N words, infinity flagged)
 };
 
+// Pairing-level geometry: slots per thread of the pair passes, elements per
+// thread of the batch-inversion tree, and the size the tree's root block
+// inverts.
+constexpr int PAIR_J = 16;
+constexpr int INV_G = 16;
+constexpr int INV_ROOT = 256;
+
+// Scratch words of one pairing level with T0 pair threads and N-word field
+// elements: the pair prefixes and totals, then each tree level's prefixes
+// and totals (the layout pair_level carves).
+inline size_t pair_scratch_words(size_t T0, int N) {
+    size_t w = (size_t)PAIR_J * N * T0;
+    for (size_t M = T0; M > (size_t)INV_ROOT;) {
+        const size_t T = (M + INV_G - 1) / INV_G;
+        w += (size_t)INV_G * N * T;
+        M = T;
+    }
+    return w;
+}
+
 struct RedArgs {
     const uint32_t* offsets;
     uint32_t B;
@@ -108,7 +128,7 @@ struct MsmLaunchers {
     void (*recode)(const ItemDesc*, uint32_t, unsigned long long, const uint32_t*,
                    const uint32_t*, uint32_t*, uint32_t*, cudaStream_t);
     void (*accumulate)(const AccArgs&, unsigned, cudaStream_t);
-    void (*pair_level)(const PairArgs&, unsigned, cudaStream_t);
+    void (*pair_level)(const PairArgs&, uint32_t, uint32_t*, cudaStream_t);
     void (*glv_rows)(uint32_t*, size_t, cudaStream_t);
     void (*fold)(const FoldArgs&, int, const uint32_t*, uint32_t*, unsigned, cudaStream_t);
     void (*reduce_blocks)(const RedArgs&, unsigned, cudaStream_t);

@@ -367,35 +367,94 @@ __global__ void __launch_bounds__(128, C::ACC_MIN_BLOCKS) k_accumulate(AccArgs a
 }
 
 // ---- Batch-affine pairing levels -------------------------------------------
-// Thread t of the grid owns output slots [PAIR_J t, PAIR_J t + PAIR_J).  Slot k
-// of bucket b adds input points i0 = in_off[b] + 2 (k - out_off[b]) and
-// i0 + 1 (if still in the run) in affine coordinates:
+// One level halves every bucket's run: slot k of bucket b adds input points
+// i0 = in_off[b] + 2 (k - out_off[b]) and i0 + 1 (if still in the run) in
+// affine coordinates,
 //   lambda = (y1 - y0) / (x1 - x0)  (or 3 x0^2 / 2 y0 when the points are
 //   equal), x3 = lambda^2 - x0 - x1, y3 = lambda (x0 - x3) - y0,
-// and infinity where the points cancel.  The denominators of a block's 2048
-// slots share one inversion (Montgomery's trick): per-thread prefix products
-// in shared memory, inclusive prefix and suffix products of the thread
-// totals across the warp by shuffles, one binary-Euclid inversion per block
-// of warps (thread 0), then a backward pass that recovers each slot's
-// inverse.  About 6 products per addition against the 10 of a mixed XYZZ
-// addition.
-constexpr int PAIR_T = 256;
-constexpr int PAIR_J = 8;
-
+// with infinity where they cancel.  All denominators of a level share ONE
+// inversion (Montgomery's trick over the whole grid):
+//   k_pair_fwd   thread t owns slots [PAIR_J t, PAIR_J t + PAIR_J): running
+//                products of its denominators (prefixes to HBM), total to tot[t];
+//   k_inv_fwd    tree over the totals, INV_G elements per thread (strided so
+//                loads coalesce), down to at most INV_ROOT elements;
+//   k_inv_root   one block: warp-shuffle prefix/suffix products, one
+//                binary-Euclid inversion, each element's inverse;
+//   k_inv_bwd    back up the tree: every total replaced by its inverse;
+//   k_pair_bwd   per thread, backwards over its slots: the slot's inverse from
+//                its prefix, then the affine sum.
+// Per addition: 1 product forward, 2 to recover the inverse, 3 for the sum,
+// plus 3/PAIR_J for the tree, against 10 for a mixed XYZZ addition.  Field
+// elements in the scratch arrays are stored word-major (word q of element e
+// at q * stride + e) so that consecutive threads touch consecutive words.
 enum PairCase : int { PAIR_PASS0 = 0, PAIR_PASS1 = 1, PAIR_INF = 2, PAIR_ADD = 3, PAIR_DBL = 4 };
 
 template <class F>
-__device__ __forceinline__ void pair_load(const PairArgs& a, uint32_t i, Affine<F>& P, bool& inf) {
+__device__ __forceinline__ void fe_load_wm(Fe<F>& x, const uint32_t* v, size_t stride, size_t e) {
+#pragma unroll
+    for (int q = 0; q < F::N; ++q) x.v[q] = v[(size_t)q * stride + e];
+}
+template <class F>
+__device__ __forceinline__ void fe_store_wm(uint32_t* v, size_t stride, size_t e, const Fe<F>& x) {
+#pragma unroll
+    for (int q = 0; q < F::N; ++q) v[(size_t)q * stride + e] = x.v[q];
+}
+
+// Rows of the two operands of input position i (level 0: a table row by
+// sorted index, sign in bit 31; later levels: the previous level's rows).
+template <class F>
+__device__ __forceinline__ const uint32_t* pair_row(const PairArgs& a, uint32_t i, bool& neg) {
     if (a.sorted) {
         const uint32_t v = a.sorted[i];
-        aff_load(P, a.src + (size_t)(v & 0x7fffffffu) * 2 * F::N);
-        if (v >> 31) fe_neg(P.y, P.y);
-        inf = false;  // the recode drops infinity entries
-    } else {
-        const uint32_t* row = a.src + (size_t)i * 2 * F::N;
-        inf = aff_is_inf_words<F>(row);
-        aff_load(P, row);
+        neg = (v >> 31) != 0;
+        return a.src + (size_t)(v & 0x7fffffffu) * 2 * F::N;
     }
+    neg = false;
+    return a.src + (size_t)i * 2 * F::N;
+}
+
+// W consecutive words (W a multiple of 4, src and dst 16-byte aligned: rows
+// are 2N words and N is a multiple of 4) in 16-byte accesses.
+template <int W>
+__device__ __forceinline__ void ld_words16(uint32_t* w, const uint32_t* src) {
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+#pragma unroll
+    for (int k = 0; k < W / 4; ++k) {
+        const uint4 v = s[k];
+        w[4 * k] = v.x;
+        w[4 * k + 1] = v.y;
+        w[4 * k + 2] = v.z;
+        w[4 * k + 3] = v.w;
+    }
+}
+template <int W>
+__device__ __forceinline__ void st_words16(uint32_t* dst, const uint32_t* w) {
+    uint4* d = reinterpret_cast<uint4*>(dst);
+#pragma unroll
+    for (int k = 0; k < W / 4; ++k) d[k] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
+}
+
+template <class F>
+__device__ __forceinline__ void pair_load(const PairArgs& a, uint32_t i, Affine<F>& P, bool& inf) {
+    bool neg;
+    const uint32_t* row = pair_row<F>(a, i, neg);
+    uint32_t w[2 * F::N];
+    ld_words16<2 * F::N>(w, row);
+    inf = aff_is_inf_words<F>(w);  // level 0: never (the recode drops infinity entries)
+    aff_load(P, w);
+    if (neg) fe_neg(P.y, P.y);
+}
+
+// Output row of a pairing slot: affine (x, y), or the infinity flag.
+template <class F>
+__device__ __forceinline__ void pair_store(uint32_t* dst, const Fe<F>& x, const Fe<F>& y) {
+    uint32_t w[2 * F::N];
+#pragma unroll
+    for (int q = 0; q < F::N; ++q) {
+        w[q] = x.v[q];
+        w[F::N + q] = y.v[q];
+    }
+    st_words16<2 * F::N>(dst, w);
 }
 
 // Loads slot k's operands (bucket b) and classifies it; den is the
@@ -422,94 +481,69 @@ __device__ __forceinline__ int pair_setup(const PairArgs& a, uint32_t k, uint32_
     return PAIR_INF;
 }
 
+// Only the denominator of slot k: the x coordinates, and the y coordinates
+// when the x are equal.  Matches pair_setup's den in every case.
 template <class F>
-__device__ __forceinline__ void smp_store(uint32_t* sm, int j, int t, const Fe<F>& x) {
-#pragma unroll
-    for (int q = 0; q < F::N; ++q) sm[(j * F::N + q) * PAIR_T + t] = x.v[q];
-}
-template <class F>
-__device__ __forceinline__ void smp_load(Fe<F>& x, const uint32_t* sm, int j, int t) {
-#pragma unroll
-    for (int q = 0; q < F::N; ++q) x.v[q] = sm[(j * F::N + q) * PAIR_T + t];
+__device__ __forceinline__ void pair_den(const PairArgs& a, uint32_t k, uint32_t b, Fe<F>& den) {
+    fe_one(den);
+    const uint32_t i0 = a.in_off[b] + 2 * (k - a.out_off[b]);
+    if (i0 + 1 >= a.in_off[b + 1]) return;
+    bool n0, n1;
+    const uint32_t* r0 = pair_row<F>(a, i0, n0);
+    const uint32_t* r1 = pair_row<F>(a, i0 + 1, n1);
+    Fe<F> x0, x1;
+    ld_words16<F::N>(x0.v, r0);
+    ld_words16<F::N>(x1.v, r1);
+    if (aff_is_inf_words<F>(x0.v) || aff_is_inf_words<F>(x1.v)) return;
+    if (!fe_eq(x0, x1)) {
+        fe_sub(den, x1, x0);
+        return;
+    }
+    Fe<F> y0, y1;
+    fe_load(y0, r0 + F::N);
+    fe_load(y1, r1 + F::N);
+    if (n0) fe_neg(y0, y0);
+    if (n1) fe_neg(y1, y1);
+    if (fe_eq(y0, y1) && !fe_is_zero(y0)) fe_dbl(den, y0);
 }
 
 template <class C>
-__global__ void __launch_bounds__(PAIR_T, 2) k_pair_level(PairArgs a) {
+__global__ void __launch_bounds__(256) k_pair_fwd(PairArgs a, uint32_t T, uint32_t* __restrict__ pre,
+                                                  uint32_t* __restrict__ tot) {
     using F = typename C::F;
-    constexpr int N = F::N;
-    constexpr int NW = PAIR_T / 32;
-    extern __shared__ __align__(16) uint32_t s_pre[];  // PAIR_J * N * PAIR_T words
-    __shared__ uint32_t s_wt[NW * N];                  // warp totals, then their inverses
-    const int warp = threadIdx.x >> 5;
-    const int t = threadIdx.x;
-    const int lane = t & 31;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
     const uint32_t total = a.out_off[a.B];
-    const uint32_t k0 = (blockIdx.x * PAIR_T + (uint32_t)t) * PAIR_J;
-    uint32_t b0 = k0 < total ? bucket_of(a.out_off, a.B, k0) : 0u;
-    // pass 1: prefix products of the denominators
+    const uint32_t k0 = t * (uint32_t)PAIR_J;
     Fe<F> run;
     fe_one(run);
-    {
-        uint32_t b = b0;
-        for (int j = 0; j < PAIR_J; ++j) {
-            const uint32_t k = k0 + (uint32_t)j;
-            if (k < total) {
-                while (a.out_off[b + 1] <= k) ++b;
-                Affine<F> P0, P1;
-                bool inf0;
-                Fe<F> den;
-                pair_setup<F>(a, k, b, P0, P1, inf0, den);
-                fe_mul(run, run, den);
-            }
-            smp_store(s_pre, j, t, run);
+    if (k0 < total) {
+        const uint32_t kend = min(k0 + (uint32_t)PAIR_J, total);
+        uint32_t b = bucket_of(a.out_off, a.B, k0);
+        for (uint32_t k = k0; k < kend; ++k) {
+            while (a.out_off[b + 1] <= k) ++b;
+            Fe<F> den;
+            pair_den<F>(a, k, b, den);
+            fe_mul(run, run, den);
+            if (k + 1 < kend) fe_store_wm(pre + (size_t)(k - k0) * F::N * T, T, t, run);
         }
     }
-    // warp: inclusive prefix P and suffix S of the thread totals
-    Fe<F> P = run, S = run, o;
-    for (int d = 1; d < 32; d <<= 1) {
-#pragma unroll
-        for (int q = 0; q < N; ++q) o.v[q] = __shfl_up_sync(0xffffffffu, P.v[q], d);
-        if (lane >= d) fe_mul(P, P, o);
-#pragma unroll
-        for (int q = 0; q < N; ++q) o.v[q] = __shfl_down_sync(0xffffffffu, S.v[q], d);
-        if (lane + d < 32) fe_mul(S, S, o);
-    }
-    // block: one inversion for all warps' totals (thread 0), then each
-    // warp's inverse by Montgomery's trick over the NW warp totals
-    if (lane == 31) fe_store(s_wt + warp * N, P);
-    __syncthreads();
-    if (t == 0) {
-        Fe<F> pre[NW], w, inv, x;
-        fe_load(pre[0], s_wt);
-        for (int q = 1; q < NW; ++q) {
-            fe_load(w, s_wt + q * N);
-            fe_mul(pre[q], pre[q - 1], w);
-        }
-        fe_inv_binary(inv, pre[NW - 1]);
-        for (int q = NW - 1; q >= 0; --q) {
-            fe_load(w, s_wt + q * N);
-            if (q > 0)
-                fe_mul(x, inv, pre[q - 1]);
-            else
-                x = inv;
-            fe_mul(inv, inv, w);
-            fe_store(s_wt + q * N, x);  // 1 / (warp q's total)
-        }
-    }
-    __syncthreads();
-    Fe<F> inv_total;
-    fe_load(inv_total, s_wt + warp * N);
-    // inverse of this thread's total: inv_total * P_{lane-1} * S_{lane+1}
-    Fe<F> inv_run = inv_total;
-#pragma unroll
-    for (int q = 0; q < N; ++q) o.v[q] = __shfl_up_sync(0xffffffffu, P.v[q], 1);
-    if (lane > 0) fe_mul(inv_run, inv_run, o);
-#pragma unroll
-    for (int q = 0; q < N; ++q) o.v[q] = __shfl_down_sync(0xffffffffu, S.v[q], 1);
-    if (lane < 31) fe_mul(inv_run, inv_run, o);
-    // pass 2 (backward): each slot's inverse, then its sum
+    fe_store_wm(tot, T, t, run);  // one for threads without slots
+}
+
+template <class C>
+__global__ void __launch_bounds__(256, 2) k_pair_bwd(PairArgs a, uint32_t T, const uint32_t* __restrict__ pre,
+                                                     const uint32_t* __restrict__ inv_tot) {
+    using F = typename C::F;
+    constexpr int N = F::N;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    const uint32_t total = a.out_off[a.B];
+    const uint32_t k0 = t * (uint32_t)PAIR_J;
     if (k0 >= total) return;
     const uint32_t kend = min(k0 + (uint32_t)PAIR_J, total);
+    Fe<F> inv_run;
+    fe_load_wm(inv_run, inv_tot, T, t);
     uint32_t bend = bucket_of(a.out_off, a.B, kend - 1);
     for (int j = (int)(kend - k0) - 1; j >= 0; --j) {
         const uint32_t k = k0 + (uint32_t)j;
@@ -519,16 +553,15 @@ __global__ void __launch_bounds__(PAIR_T, 2) k_pair_level(PairArgs a) {
         Fe<F> den, inv;
         const int kind = pair_setup<F>(a, k, bend, P0, P1, inf0, den);
         if (j > 0) {
-            Fe<F> pre;
-            smp_load(pre, s_pre, j - 1, t);
-            fe_mul(inv, inv_run, pre);
+            fe_load_wm(inv, pre + (size_t)(j - 1) * N * T, T, t);
+            fe_mul(inv, inv, inv_run);
+            fe_mul(inv_run, inv_run, den);
         } else {
             inv = inv_run;
         }
-        fe_mul(inv_run, inv_run, den);
         uint32_t* dst = a.dst + (size_t)k * 2 * N;
         if (kind == PAIR_ADD || kind == PAIR_DBL) {
-            Fe<F> lam, x3, y3;
+            Fe<F> lam, x3;
             if (kind == PAIR_ADD) {
                 fe_sub(lam, P1.y, P0.y);
             } else {
@@ -541,20 +574,118 @@ __global__ void __launch_bounds__(PAIR_T, 2) k_pair_level(PairArgs a) {
             fe_sqr(x3, lam);
             fe_sub(x3, x3, P0.x);
             fe_sub(x3, x3, P1.x);
-            fe_sub(y3, P0.x, x3);
-            fe_mul(y3, lam, y3);
-            fe_sub(y3, y3, P0.y);
-            fe_store(dst, x3);
-            fe_store(dst + N, y3);
+            fe_sub(P1.y, P0.x, x3);
+            fe_mul(P1.y, lam, P1.y);
+            fe_sub(P1.y, P1.y, P0.y);
+            pair_store<F>(dst, x3, P1.y);
         } else if (kind == PAIR_INF || (kind == PAIR_PASS0 && inf0)) {
-            for (int q = 0; q < 2 * N; ++q) dst[q] = 0;
-            dst[N - 1] = INF_FLAG;
+            Fe<F> z;
+            fe_zero(z);
+            P0.x = z;
+            P0.x.v[N - 1] = INF_FLAG;
+            pair_store<F>(dst, P0.x, z);
         } else {
             const Affine<F>& R = kind == PAIR_PASS0 ? P0 : P1;
-            fe_store(dst, R.x);
-            fe_store(dst + N, R.y);
+            pair_store<F>(dst, R.x, R.y);
         }
     }
+}
+
+// Tree level: thread t < T = ceil(M / INV_G) multiplies elements t, t + T,
+// t + 2T, ... of v (M elements, word-major), keeping the running products
+// in pre and the total in out[t].
+template <class F>
+__global__ void __launch_bounds__(256) k_inv_fwd(const uint32_t* __restrict__ v, uint32_t M, uint32_t T,
+                                                 uint32_t* __restrict__ pre, uint32_t* __restrict__ out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    Fe<F> run, x;
+    fe_load_wm(run, v, M, t);
+    for (uint32_t j = 1, e = t + T; j < (uint32_t)INV_G && e < M; ++j, e += T) {
+        fe_store_wm(pre + (size_t)(j - 1) * F::N * T, T, t, run);
+        fe_load_wm(x, v, M, e);
+        fe_mul(run, run, x);
+    }
+    fe_store_wm(out, T, t, run);
+}
+
+// Inverse of the tree level: out[t] holds the inverse of thread t's total;
+// each of its elements is replaced by its own inverse.
+template <class F>
+__global__ void __launch_bounds__(256) k_inv_bwd(uint32_t* __restrict__ v, uint32_t M, uint32_t T,
+                                                 const uint32_t* __restrict__ pre,
+                                                 const uint32_t* __restrict__ out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    const uint32_t cnt = min((uint32_t)INV_G, (M - t + T - 1) / T);
+    Fe<F> inv, x, r;
+    fe_load_wm(inv, out, T, t);
+    for (int j = (int)cnt - 1; j > 0; --j) {
+        const uint32_t e = t + (uint32_t)j * T;
+        fe_load_wm(x, v, M, e);
+        fe_load_wm(r, pre + (size_t)(j - 1) * F::N * T, T, t);
+        fe_mul(r, r, inv);
+        fe_mul(inv, inv, x);
+        fe_store_wm(v, M, e, r);
+    }
+    fe_store_wm(v, M, t, inv);
+}
+
+// The tree's root: the M <= INV_ROOT elements of v (word-major, stride M)
+// replaced by their inverses with one binary-Euclid inversion.  Elements are
+// non-zero: every denominator is a difference of distinct x, or 2y with y
+// non-zero, or one.
+template <class F>
+__global__ void __launch_bounds__(INV_ROOT) k_inv_root(uint32_t* __restrict__ v, uint32_t M) {
+    constexpr int N = F::N;
+    constexpr int NW = INV_ROOT / 32;
+    __shared__ uint32_t s_wt[NW * N];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    Fe<F> x, P, S, o;
+    if ((uint32_t)t < M)
+        fe_load_wm(x, v, M, t);
+    else
+        fe_one(x);
+    P = x;
+    S = x;
+    for (int d = 1; d < 32; d <<= 1) {  // inclusive prefix P and suffix S over the warp
+#pragma unroll
+        for (int q = 0; q < N; ++q) o.v[q] = __shfl_up_sync(0xffffffffu, P.v[q], d);
+        if (lane >= d) fe_mul(P, P, o);
+#pragma unroll
+        for (int q = 0; q < N; ++q) o.v[q] = __shfl_down_sync(0xffffffffu, S.v[q], d);
+        if (lane + d < 32) fe_mul(S, S, o);
+    }
+    if (lane == 31) fe_store(s_wt + warp * N, P);
+    __syncthreads();
+    if (t == 0) {  // Montgomery's trick over the warp totals
+        Fe<F> pre[NW], w, inv, y;
+        fe_load(pre[0], s_wt);
+        for (int q = 1; q < NW; ++q) {
+            fe_load(w, s_wt + q * N);
+            fe_mul(pre[q], pre[q - 1], w);
+        }
+        fe_inv_binary(inv, pre[NW - 1]);
+        for (int q = NW - 1; q >= 0; --q) {
+            fe_load(w, s_wt + q * N);
+            if (q > 0)
+                fe_mul(y, inv, pre[q - 1]);
+            else
+                y = inv;
+            fe_mul(inv, inv, w);
+            fe_store(s_wt + q * N, y);  // 1 / (warp q's total)
+        }
+    }
+    __syncthreads();
+    Fe<F> r;
+    fe_load(r, s_wt + warp * N);  // x^-1 = (total)^-1 * P_{lane-1} * S_{lane+1}
+#pragma unroll
+    for (int q = 0; q < N; ++q) o.v[q] = __shfl_up_sync(0xffffffffu, P.v[q], 1);
+    if (lane > 0) fe_mul(r, r, o);
+#pragma unroll
+    for (int q = 0; q < N; ++q) o.v[q] = __shfl_down_sync(0xffffffffu, S.v[q], 1);
+    if (lane < 31) fe_mul(r, r, o);
+    if ((uint32_t)t < M) fe_store_wm(v, M, t, r);
 }
 
 // Fold level l >= 2: the level's (big bucket, group) items are flattened by
@@ -902,11 +1033,45 @@ struct MsmLaunchImpl {
                                                            keys, vals);
         KB_LAUNCH_CHECK();
     }
-    static void pair_level(const PairArgs& a, unsigned grid, cudaStream_t st) {
-        if (!grid) return;
-        const size_t smem = (size_t)PAIR_J * F::N * PAIR_T * 4;
-        set_smem_attr((const void*)k_pair_level<C>, smem);
-        k_pair_level<C><<<grid, PAIR_T, smem, st>>>(a);
+    // One pairing level over T0 = ceil(slots / PAIR_J) threads; scratch holds
+    // pair_scratch_words(T0, N) words.
+    static void pair_level(const PairArgs& a, uint32_t T0, uint32_t* scratch, cudaStream_t st) {
+        if (!T0) return;
+        constexpr int N = F::N;
+        uint32_t* pre0 = scratch;
+        uint32_t* tot = pre0 + (size_t)(PAIR_J - 1) * N * T0;
+        k_pair_fwd<C><<<ceil_div_u(T0, 256), 256, 0, st>>>(a, T0, pre0, tot);
+        KB_LAUNCH_CHECK();
+        uint32_t* lv_v[16];
+        uint32_t* lv_pre[16];
+        uint32_t lv_M[16];
+        int R = 0;
+        uint32_t* cur = tot;
+        uint32_t M = T0;
+        uint32_t* next = tot + (size_t)N * T0;
+        while (M > (uint32_t)INV_ROOT) {  // M shrinks 16x per level: at most 8 levels
+            const uint32_t T = (M + INV_G - 1) / INV_G;
+            uint32_t* pre = next;
+            uint32_t* out = pre + (size_t)(INV_G - 1) * N * T;
+            next = out + (size_t)N * T;
+            k_inv_fwd<F><<<ceil_div_u(T, 256), 256, 0, st>>>(cur, M, T, pre, out);
+            KB_LAUNCH_CHECK();
+            lv_v[R] = cur;
+            lv_pre[R] = pre;
+            lv_M[R] = M;
+            ++R;
+            cur = out;
+            M = T;
+        }
+        k_inv_root<F><<<1, INV_ROOT, 0, st>>>(cur, M);
+        KB_LAUNCH_CHECK();
+        for (int r = R - 1; r >= 0; --r) {
+            const uint32_t T = (lv_M[r] + INV_G - 1) / INV_G;
+            k_inv_bwd<F><<<ceil_div_u(T, 256), 256, 0, st>>>(lv_v[r], lv_M[r], T, lv_pre[r],
+                                                            r + 1 < R ? lv_v[r + 1] : cur);
+            KB_LAUNCH_CHECK();
+        }
+        k_pair_bwd<C><<<ceil_div_u(T0, 256), 256, 0, st>>>(a, T0, pre0, tot);
         KB_LAUNCH_CHECK();
     }
     static void glv_rows(uint32_t* table, size_t n, cudaStream_t st) {

@@ -183,10 +183,12 @@ def test_glv_halves_share_a_bucket(cuda_lib):
     assert kb().gpukit_multi_pippenger(2, S, pts, n) == want
 
 
-def test_pairing_levels_bit_exact(cuda_lib):
-    """The batch-affine pairing levels (off by default, KB200_MSM_PAIR_LEVELS)
-    give the same bytes: run in a child process with two levels, on inputs
-    with long runs per bucket, repeated points and cancelling pairs."""
+@pytest.mark.parametrize("levels", [1, 4])
+def test_pairing_levels_bit_exact(cuda_lib, levels):
+    """The batch-affine pairing levels, forced (KB200_MSM_PAIR_LEVELS) on
+    inputs whose runs the planner would not pair, give the same bytes: long
+    runs in a few buckets, repeated points (doublings) and cancelling pairs
+    (infinity rows that later levels pass through)."""
     import os
     import subprocess
     import sys
@@ -210,7 +212,7 @@ for curve, n in ((2, 1 << 13), (1, 1 << 13)):
     assert kb.gpukit_multi_pippenger(curve, S, P, n) == O.msm(curve, S, P, n), curve
 print("ok")
 '''
-    env = dict(os.environ, KB200_MSM_PAIR_LEVELS="2")
+    env = dict(os.environ, KB200_MSM_PAIR_LEVELS=str(levels))
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True,
                          text=True, timeout=600)
