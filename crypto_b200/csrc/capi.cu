@@ -165,17 +165,17 @@ static int msm_host(uint32_t curve, const uint8_t* scalars, const uint8_t* point
                        c->d_b.reserve(n * pb + 16, st);
                        c->d_out.reserve(256, st);
                        c->h_out.reserve(256, st);
-                       if (n) {
-                           KB_CUDA(cudaMemcpyAsync(c->d_a.ptr, scalars, n * 32,
-                                                   cudaMemcpyHostToDevice, st));
-                           KB_CUDA(cudaMemcpyAsync(c->d_b.ptr, points, n * pb,
-                                                   cudaMemcpyHostToDevice, st));
-                       }
                        MsmOptions opt;
                        opt.ref_carry_quirk = true;
-                       msm_run_wire(c->msm_for((int)curve), c->d_a.as<uint8_t>(),
-                                    c->d_b.as<uint8_t>(), n, c->d_out.as<uint8_t>(), nullptr, st,
-                                    opt);
+                       if (n) {
+                           msm_run_host_wire(c->msm_for((int)curve), scalars, points, n,
+                                             c->d_a.as<uint8_t>(), c->d_b.as<uint8_t>(),
+                                             c->d_out.as<uint8_t>(), st, opt);
+                       } else {
+                           msm_run_wire(c->msm_for((int)curve), c->d_a.as<uint8_t>(),
+                                        c->d_b.as<uint8_t>(), n, c->d_out.as<uint8_t>(), nullptr,
+                                        st, opt);
+                       }
                        KB_CUDA(cudaMemcpyAsync(c->h_out.ptr, c->d_out.ptr, pb,
                                                cudaMemcpyDeviceToHost, st));
                        KB_CUDA(cudaStreamSynchronize(st));

@@ -455,6 +455,19 @@ class MsmEngine {
     std::map<std::tuple<size_t, bool, int, int, int, size_t, bool, size_t>, MsmBatchPlan*> single_plans;
     cudaEvent_t ev[N_STAGE_EVENTS] = {};
     bool ev_ready = false, ev_recorded = false;
+    // Host-input pipeline (msm_run_host_wire): copy and conversion streams,
+    // and events for the start, each point chunk and the finished table.
+    static constexpr int HOST_CHUNKS = 8;
+    cudaStream_t st_copy = nullptr, st_conv = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_table = nullptr, ev_chunk[HOST_CHUNKS] = {};
+    void host_streams() {
+        if (st_copy) return;
+        KB_CUDA(cudaStreamCreateWithFlags(&st_copy, cudaStreamNonBlocking));
+        KB_CUDA(cudaStreamCreateWithFlags(&st_conv, cudaStreamNonBlocking));
+        KB_CUDA(cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming));
+        KB_CUDA(cudaEventCreateWithFlags(&ev_table, cudaEventDisableTiming));
+        for (auto& c : ev_chunk) KB_CUDA(cudaEventCreateWithFlags(&c, cudaEventDisableTiming));
+    }
     void mark(int i, cudaStream_t st) {
         if (!profiling_enabled()) return;
         if (!ev_ready) {
@@ -468,9 +481,17 @@ class MsmEngine {
         for (auto& kv : single_plans) delete kv.second;
         if (ev_ready)
             for (auto& e : ev) cudaEventDestroy(e);
+        if (st_copy) {
+            cudaStreamDestroy(st_copy);
+            cudaStreamDestroy(st_conv);
+            cudaEventDestroy(ev_start);
+            cudaEventDestroy(ev_table);
+            for (auto& c : ev_chunk) cudaEventDestroy(c);
+        }
         for (DevBuf* b : {&table, &keys, &vals, &counts, &offsets, &cursor, &sorted, &rec_first,
                           &rec_last, &fold_buf, &buckets, &blk_out, &win_out, &scan_tmp, &queue,
-                          &fold_counts, &fold_prefix})
+                          &fold_counts, &fold_prefix, &pair_off[0], &pair_off[1], &pair_rows[0],
+                          &pair_rows[1], &pair_scratch})
             b->release();
     }
 };
@@ -554,14 +575,15 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
 
 void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_scalars,
                        const uint32_t* d_table, uint8_t* d_out_wire, uint8_t* d_out_comp,
-                       cudaStream_t st) {
+                       cudaStream_t st, cudaEvent_t table_ready) {
     const MsmBatchPlan& P = *p;
     const MsmLaunchers& K = msm_launchers(e->curve);
     const ItemDesc* items = P.d_items.as<ItemDesc>();
     const uint32_t nitems = (uint32_t)P.count;
     if (P.L > 0) {
         K.recode(items, nitems, P.total_scalars, reinterpret_cast<const uint32_t*>(d_scalars),
-                 d_table, e->keys.as<uint32_t>(), e->vals.as<uint32_t>(), st);
+                 table_ready ? nullptr : d_table, e->keys.as<uint32_t>(), e->vals.as<uint32_t>(),
+                 st);
     }
     e->mark(2, st);
     KB_CUDA(cudaMemsetAsync(e->counts.ptr, 0, ((size_t)P.B + 1) * 4, st));
@@ -580,6 +602,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
                                                        e->sorted.as<uint32_t>());
         KB_LAUNCH_CHECK();
     }
+    if (table_ready) KB_CUDA(cudaStreamWaitEvent(st, table_ready, 0));
     // Pairing levels: the sorted runs shrink to about half per level, the
     // accumulation then reads the last level's rows directly.
     const uint32_t* off = e->offsets.as<uint32_t>();
@@ -726,9 +749,53 @@ void msm_run_wire(MsmEngine* e, const uint8_t* d_scalars, const uint8_t* d_point
     e->table.reserve(std::max<size_t>(1, n) * (glv ? 2 : 1) * (size_t)K.table_words * 4, st);
     e->mark(0, st);
     K.wire_to_table(d_points, e->table.as<uint32_t>(), n, st);
-    if (glv) K.glv_rows(e->table.as<uint32_t>(), n, st);
+    if (glv) K.glv_rows(e->table.as<uint32_t>(), n, 0, n, st);
     e->mark(1, st);
     msm_engine_launch(e, p, d_scalars, e->table.as<uint32_t>(), d_out_wire, d_out_comp, st);
+}
+
+void msm_run_host_wire(MsmEngine* e, const uint8_t* h_scalars, const uint8_t* h_points, size_t n,
+                       uint8_t* d_scalars, uint8_t* d_points, uint8_t* d_out_wire, cudaStream_t st,
+                       const MsmOptions& opt) {
+    static const bool glv_env_off = [] {
+        const char* v = std::getenv("KB200_MSM_NO_GLV");
+        return v && *v && *v != '0';
+    }();
+    MsmOptions o2 = opt;
+    const bool glv = e->curve == 2 && opt.shift_c <= 0 && !opt.no_glv && !glv_env_off;
+    if (glv) {
+        o2.glv = true;
+        o2.glv_rows = n;
+    }
+    MsmBatchPlan* p = single_plan(e, n, o2, st);
+    msm_engine_reserve(e, p, st);
+    const MsmLaunchers& K = msm_launchers(e->curve);
+    const size_t TW = (size_t)K.table_words, WB = (size_t)K.wire_bytes;
+    e->table.reserve(std::max<size_t>(1, n) * (glv ? 2 : 1) * TW * 4, st);
+    e->host_streams();
+    uint32_t* table = e->table.as<uint32_t>();
+    // The side streams start after everything already queued on st (the
+    // staging buffers may still be read by an earlier call).
+    KB_CUDA(cudaEventRecord(e->ev_start, st));
+    KB_CUDA(cudaStreamWaitEvent(e->st_copy, e->ev_start, 0));
+    KB_CUDA(cudaStreamWaitEvent(e->st_conv, e->ev_start, 0));
+    KB_CUDA(cudaMemcpyAsync(d_scalars, h_scalars, n * 32, cudaMemcpyHostToDevice, st));
+    const size_t chunks = n >= ((size_t)1 << 16) ? (size_t)MsmEngine::HOST_CHUNKS : 1;
+    for (size_t c = 0; c < chunks; ++c) {
+        const size_t lo = n * c / chunks, hi = n * (c + 1) / chunks;
+        if (hi > lo) {
+            KB_CUDA(cudaMemcpyAsync(d_points + lo * WB, h_points + lo * WB, (hi - lo) * WB,
+                                    cudaMemcpyHostToDevice, e->st_copy));
+        }
+        KB_CUDA(cudaEventRecord(e->ev_chunk[c], e->st_copy));
+        KB_CUDA(cudaStreamWaitEvent(e->st_conv, e->ev_chunk[c], 0));
+        K.wire_to_table(d_points + lo * WB, table + lo * TW, hi - lo, e->st_conv);
+        if (glv) K.glv_rows(table, n, lo, hi - lo, e->st_conv);
+    }
+    KB_CUDA(cudaEventRecord(e->ev_table, e->st_conv));
+    e->mark(0, st);
+    e->mark(1, st);
+    msm_engine_launch(e, p, d_scalars, table, d_out_wire, nullptr, st, e->ev_table);
 }
 
 void points_wire_to_table(int curve, const uint8_t* d_wire, uint32_t* d_table, size_t n,

@@ -118,14 +118,24 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t stream
 // synchronisation after msm_engine_reserve, so it can be captured in a
 // CUDA graph.  out_wire: count * WIRE bytes; out_comp: count * 48 bytes
 // (BLS12-381 only, may be null).
+// table_ready: null, or an event after which d_table is complete; the
+// recode and sort then run without reading the table and the stream waits
+// for the event before the first stage that reads points.
 void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_scalars,
                        const uint32_t* d_table, uint8_t* d_out_wire, uint8_t* d_out_comp,
-                       cudaStream_t stream);
+                       cudaStream_t stream, cudaEvent_t table_ready = nullptr);
 
 // Convenience single-MSM entry points (plan cached per (n, options)).
 void msm_run_wire(MsmEngine* e, const uint8_t* d_scalars, const uint8_t* d_points, size_t n,
                   uint8_t* d_out_wire, uint8_t* d_out_comp, cudaStream_t stream,
                   const MsmOptions& opt);
+// From host buffers: the scalars are copied first on `stream` and the
+// recode and sort start at once, while the points arrive in chunks on a
+// copy stream and are converted to table rows chunk by chunk on a third;
+// d_scalars (n * 32 bytes) and d_points (n * WIRE bytes) are the staging.
+void msm_run_host_wire(MsmEngine* e, const uint8_t* h_scalars, const uint8_t* h_points, size_t n,
+                       uint8_t* d_scalars, uint8_t* d_points, uint8_t* d_out_wire,
+                       cudaStream_t stream, const MsmOptions& opt);
 void msm_run_table(MsmEngine* e, const uint8_t* d_scalars, const uint32_t* d_table, size_t n,
                    uint8_t* d_out_wire, uint8_t* d_out_comp, cudaStream_t stream,
                    const MsmOptions& opt);

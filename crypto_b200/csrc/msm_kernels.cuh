@@ -143,7 +143,9 @@ __global__ void k_recode(const ItemDesc* __restrict__ items, uint32_t n_items,
     if (g < it.scalar_off || g - it.scalar_off >= it.n) return;  // gap between items
     const uint32_t j = (uint32_t)(g - it.scalar_off);
     const uint32_t row = it.point_off + j;
-    const bool inf = aff_is_inf_words<F>(table + (size_t)row * 2 * F::N);
+    // Without a table (points still in flight) infinity points get entries
+    // too: every later stage skips infinity rows.
+    const bool inf = table && aff_is_inf_words<F>(table + (size_t)row * 2 * F::N);
     uint32_t s[8];
     const uint4* sp = reinterpret_cast<const uint4*>(scalars + g * 8);
     const uint4 a = sp[0], b = sp[1];
@@ -251,10 +253,11 @@ __global__ void k_recode(const ItemDesc* __restrict__ items, uint32_t n_items,
 
 // GLV rows: table[n + i] = phi(table[i]) = (beta2 x, y); infinity stays.
 template <class C>
-__global__ void k_glv_rows(uint32_t* __restrict__ table, size_t n) {
+__global__ void k_glv_rows(uint32_t* __restrict__ table, size_t n, size_t first, size_t count) {
     using F = typename C::F;
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const size_t i = first + k;
     const uint32_t* src = table + i * 2 * F::N;
     uint32_t* dst = table + (n + i) * 2 * F::N;
     if (aff_is_inf_words<F>(src)) {
@@ -440,7 +443,7 @@ __device__ __forceinline__ void pair_load(const PairArgs& a, uint32_t i, Affine<
     const uint32_t* row = pair_row<F>(a, i, neg);
     uint32_t w[2 * F::N];
     ld_words16<2 * F::N>(w, row);
-    inf = aff_is_inf_words<F>(w);  // level 0: never (the recode drops infinity entries)
+    inf = aff_is_inf_words<F>(w);
     aff_load(P, w);
     if (neg) fe_neg(P.y, P.y);
 }
@@ -1074,10 +1077,10 @@ struct MsmLaunchImpl {
         k_pair_bwd<C><<<ceil_div_u(T0, 256), 256, 0, st>>>(a, T0, pre0, tot);
         KB_LAUNCH_CHECK();
     }
-    static void glv_rows(uint32_t* table, size_t n, cudaStream_t st) {
+    static void glv_rows(uint32_t* table, size_t n, size_t first, size_t count, cudaStream_t st) {
         if constexpr (C::CURVE_ID == 2) {
-            if (!n) return;
-            k_glv_rows<C><<<ceil_div_u(n, 128), 128, 0, st>>>(table, n);
+            if (!count) return;
+            k_glv_rows<C><<<ceil_div_u(count, 128), 128, 0, st>>>(table, n, first, count);
             KB_LAUNCH_CHECK();
         }
     }

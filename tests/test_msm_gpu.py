@@ -217,3 +217,23 @@ print("ok")
     out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True,
                          text=True, timeout=600)
     assert out.returncode == 0 and "ok" in out.stdout, out.stdout + out.stderr
+
+
+@pytest.mark.parametrize("curve,logn", [(2, 20), (1, 17)])
+def test_host_pipeline_with_infinity_points(cuda_lib, curve, logn):
+    """gpukit_multi_pippenger overlaps the point copy with the recode and
+    sort (chunked copies, conversion per chunk), so infinity points reach
+    the buckets and are skipped there: one point in eight is the identity,
+    at a size with eight chunks (and, at 2^20 on BLS12-381, GLV rows and
+    pairing levels)."""
+    n = 1 << logn
+    pb = O.PB[curve]
+    pts = bytearray(rand_points(curve, n, seed=90 + curve))
+    rng = random.Random(90 + curve)
+    for i in range(0, n, 8):
+        j = i + rng.randrange(8)
+        pts[pb * j:pb * (j + 1)] = bytes(pb)
+    pts = bytes(pts)
+    S = b"".join(rng.randrange(O.FR[curve]).to_bytes(32, "little") for _ in range(n))
+    want = O.ref_msm(curve, S, pts, n, threads=16) if O.ref_available() else O.msm(curve, S, pts, n)
+    assert kb().gpukit_multi_pippenger(curve, S, pts, n) == want
