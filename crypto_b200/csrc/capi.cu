@@ -34,6 +34,18 @@ static std::atomic<bool> g_profile{false};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 bool profiling_enabled() { return g_profile.load(std::memory_order_relaxed); }
 
+bool alloc_trace_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("KB200_ALLOC_TRACE");
+        return v && *v && *v != '0';
+    }();
+    return on;
+}
+
+void alloc_trace(size_t from, size_t to, double ms) {
+    std::fprintf(stderr, "[devbuf] %zu -> %zu bytes, %.3f ms\n", from, to, ms);
+}
+
 struct DeviceCtx {
     int dev = -1;
     std::mutex mu;

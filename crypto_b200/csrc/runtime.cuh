@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstddef>
 #include <cstdint>
 #include <cstdio>
@@ -45,6 +46,11 @@ bool profiling_enabled();
 // Records the most recent failure message so the C ABI can report it.
 void set_last_error(const std::string& msg);
 
+// KB200_ALLOC_TRACE=1: every device-buffer growth logged on stderr with its
+// size and host time.
+bool alloc_trace_enabled();
+void alloc_trace(size_t from, size_t to, double ms);
+
 // A grow-only device buffer.  Growing synchronises the owning stream first,
 // because the old allocation may still be read by queued work.
 struct DevBuf {
@@ -52,6 +58,9 @@ struct DevBuf {
     size_t bytes = 0;
     void reserve(size_t need, cudaStream_t stream) {
         if (need <= bytes) return;
+        const bool tr = alloc_trace_enabled();
+        const auto t0 = std::chrono::steady_clock::now();
+        const size_t from = bytes;
         if (ptr) {
             KB_CUDA(cudaStreamSynchronize(stream));
             KB_CUDA(cudaFree(ptr));
@@ -61,6 +70,9 @@ struct DevBuf {
         size_t want = need + need / 8 + 256;
         KB_CUDA(cudaMalloc(&ptr, want));
         bytes = want;
+        if (tr)
+            alloc_trace(from, want,
+                        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
     }
     template <class T>
     T* as() const {

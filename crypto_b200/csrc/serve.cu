@@ -46,10 +46,19 @@ using Clock = std::chrono::steady_clock;
 // Pinned host slabs for request payloads, recycled by power-of-two size
 // class: a request is copied once, at submit, into page-locked memory, and
 // its batch's host-to-device copy reads it from there asynchronously.
+// Slabs are carved from one arena pinned at server creation: page-locking
+// under load (cudaHostAlloc, tens of ms for a few MiB) holds a driver lock
+// that stalls the worker's launches.  An exhausted arena falls back to
+// cudaHostAlloc.
 class PinnedPool {
    public:
     ~PinnedPool() {
         for (void* p : all_) cudaFreeHost(p);
+        if (base_) cudaFreeHost(base_);
+    }
+    void reserve_arena(size_t bytes) {
+        KB_CUDA(cudaHostAlloc(&base_, bytes, cudaHostAllocPortable));
+        cap_ = bytes;
     }
     static size_t size_class(size_t bytes) {
         size_t c = 4096;
@@ -66,9 +75,18 @@ class PinnedPool {
                 v.pop_back();
                 return static_cast<uint8_t*>(p);
             }
+            if (base_ && used_ + c <= cap_) {
+                uint8_t* p = static_cast<uint8_t*>(base_) + used_;
+                used_ += c;
+                return p;
+            }
         }
         void* p = nullptr;
+        const auto t0 = Clock::now();
         KB_CUDA(cudaHostAlloc(&p, c, cudaHostAllocPortable));
+        if (alloc_trace_enabled())
+            std::fprintf(stderr, "[pinned] %zu bytes, %.3f ms\n", c,
+                         std::chrono::duration<double, std::milli>(Clock::now() - t0).count());
         std::lock_guard<std::mutex> lk(mu_);
         all_.push_back(p);
         return static_cast<uint8_t*>(p);
@@ -83,6 +101,8 @@ class PinnedPool {
     std::mutex mu_;
     std::map<size_t, std::vector<void*>> free_;
     std::vector<void*> all_;
+    void* base_ = nullptr;
+    size_t cap_ = 0, used_ = 0;
 };
 
 struct Request {
@@ -189,12 +209,14 @@ bool KzgServer::launch_batch(Slot& s) {
     if (s.h_out.bytes < take.size() * 48) s.h_out.reserve(std::max<size_t>(max_batch, take.size()) * 48, s.stream);
     uint8_t* d_in = commit_batch_device_input(s.batcher, sizes.data(), sizes.size(), srs, srs_n,
                                               s.stream);
+    const auto t_prep = Clock::now();
     size_t off = 0;
     for (Request* r : take) {
         KB_CUDA(cudaMemcpyAsync(d_in + off * 32, r->evals, r->n * 32, cudaMemcpyHostToDevice,
                                 s.stream));
         off += r->n;
     }
+    const auto t_copy = Clock::now();
     commit_batch_device(s.batcher, sizes.data(), sizes.size(), srs, srs_n, s.stream,
                         /*use_graph=*/false);
     KB_CUDA(cudaMemcpyAsync(s.h_out.ptr, commit_batch_device_output(s.batcher), take.size() * 48,
@@ -203,11 +225,12 @@ bool KzgServer::launch_batch(Slot& s) {
     if (trace) {
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
-        std::fprintf(stderr, "[kzg_server] slot %d: %zu requests (%zu evaluations), host %.3f ms, "
-                             "queue left %zu, free %.1f GB\n",
-                     (int)(&s - slots.data()), take.size(), total,
-                     std::chrono::duration<double, std::milli>(Clock::now() - t_launch).count(),
-                     queue.size(), free_b / 1e9);
+        using ms = std::chrono::duration<double, std::milli>;
+        std::fprintf(stderr, "[kzg_server] slot %d: %zu requests (%zu evaluations), host %.3f ms "
+                             "(prepare %.3f, copies %.3f), queue left %zu, free %.1f GB\n",
+                     (int)(&s - slots.data()), take.size(), total, ms(Clock::now() - t_launch).count(),
+                     ms(t_prep - t_launch).count(), ms(t_copy - t_prep).count(), queue.size(),
+                     free_b / 1e9);
     }
     s.reqs = std::move(take);
     s.busy = true;
@@ -272,6 +295,14 @@ void* kzg_server_create(size_t max_batch, int slots, size_t mem_budget_bytes) {
         }
         s->max_batch = max_batch ? max_batch : 64;
         s->mem_budget = mem_budget_bytes;
+        {
+            // Room for eight full-size requests in flight (or many smaller
+            // ones); KB200_SERVE_PINNED_MB overrides.
+            size_t arena = (size_t)8 * s->srs_n * 32;
+            if (const char* v = std::getenv("KB200_SERVE_PINNED_MB"))
+                if (*v) arena = (size_t)std::strtoull(v, nullptr, 10) << 20;
+            if (arena) s->pool.reserve_arena(arena);
+        }
         s->slots.resize(slots > 0 ? (size_t)slots : 2);
         for (Slot& sl : s->slots) {
             KB_CUDA(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
