@@ -444,7 +444,7 @@ size_t msm_batch_plan_count(const MsmBatchPlan* p) { return p->count; }
 // Engine
 // ---------------------------------------------------------------------------
 
-constexpr int N_STAGE_EVENTS = 9;
+constexpr int N_STAGE_EVENTS = 10;
 
 class MsmEngine {
    public:
@@ -602,6 +602,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
                                                        e->sorted.as<uint32_t>());
         KB_LAUNCH_CHECK();
     }
+    e->mark(3, st);
     if (table_ready) KB_CUDA(cudaStreamWaitEvent(st, table_ready, 0));
     // Pairing levels: the sorted runs shrink to about half per level, the
     // accumulation then reads the last level's rows directly.
@@ -634,7 +635,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
                                                         big_list);
         KB_LAUNCH_CHECK();
     }
-    e->mark(3, st);
+    e->mark(4, st);
 
     AccArgs acc;
     acc.sorted = acc_sorted;
@@ -652,7 +653,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
             (unsigned)std::min<size_t>(units, (size_t)device_sms() * acc_occupancy(e->curve));
         K.accumulate(acc, std::max(1u, grid), st);
     }
-    e->mark(4, st);
+    e->mark(5, st);
 
     if (P.levels >= 1 && P.L > 0) {
         FoldArgs fa;
@@ -678,7 +679,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
             std::swap(in, out);
         }
     }
-    e->mark(5, st);
+    e->mark(6, st);
 
     RedArgs ra;
     ra.offsets = off;
@@ -693,11 +694,11 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
     ra.blk_out = e->blk_out.as<uint32_t>();
     ra.win_out = e->win_out.as<uint32_t>();
     K.reduce_blocks(ra, (unsigned)P.blks.size(), st);
-    e->mark(6, st);
-    K.reduce_windows(ra, (unsigned)P.wins.size(), st);
     e->mark(7, st);
-    K.combine(items, nitems, e->win_out.as<uint32_t>(), d_out_wire, d_out_comp, st);
+    K.reduce_windows(ra, (unsigned)P.wins.size(), st);
     e->mark(8, st);
+    K.combine(items, nitems, e->win_out.as<uint32_t>(), d_out_wire, d_out_comp, st);
+    e->mark(9, st);
 }
 
 static MsmBatchPlan* single_plan(MsmEngine* e, size_t n, const MsmOptions& opt, cudaStream_t st) {
