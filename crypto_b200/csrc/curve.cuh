@@ -325,18 +325,18 @@ KB_DEV bool xyzz_to_affine_single(Affine<F>& a, const Xyzz<F>& p) {
 
 // Memory helpers for XYZZ points stored as 4N consecutive words.
 template <class F>
-KB_DEV void xyzz_load(Xyzz<F>& p, const uint32_t* w) {
-    fe_load(p.X, w);
-    fe_load(p.Y, w + F::N);
-    fe_load(p.ZZ, w + 2 * F::N);
-    fe_load(p.ZZZ, w + 3 * F::N);
+KB_DEV void xyzz_load(Xyzz<F>& p, const uint32_t* w) {  // w 16-byte aligned
+    fe_load16(p.X, w);
+    fe_load16(p.Y, w + F::N);
+    fe_load16(p.ZZ, w + 2 * F::N);
+    fe_load16(p.ZZZ, w + 3 * F::N);
 }
 template <class F>
-KB_DEV void xyzz_store(uint32_t* w, const Xyzz<F>& p) {
-    fe_store(w, p.X);
-    fe_store(w + F::N, p.Y);
-    fe_store(w + 2 * F::N, p.ZZ);
-    fe_store(w + 3 * F::N, p.ZZZ);
+KB_DEV void xyzz_store(uint32_t* w, const Xyzz<F>& p) {  // w 16-byte aligned
+    fe_store16(w, p.X);
+    fe_store16(w + F::N, p.Y);
+    fe_store16(w + 2 * F::N, p.ZZ);
+    fe_store16(w + 3 * F::N, p.ZZZ);
 }
 
 // An XYZZ point held in shared memory, word-major over a block of STRIDE
@@ -366,9 +366,12 @@ struct SmXyzz {
 #pragma unroll
         for (int k = 0; k < 4 * F::N; ++k) base[k * STRIDE] = 0;
     }
-    KB_DEV void to_global(uint32_t* w) const {
+    KB_DEV void to_global(uint32_t* w) const {  // w 16-byte aligned
+        uint4* d = reinterpret_cast<uint4*>(w);
 #pragma unroll
-        for (int k = 0; k < 4 * F::N; ++k) w[k] = base[k * STRIDE];
+        for (int k = 0; k < F::N; ++k)
+            d[k] = make_uint4(base[(4 * k) * STRIDE], base[(4 * k + 1) * STRIDE],
+                              base[(4 * k + 2) * STRIDE], base[(4 * k + 3) * STRIDE]);
     }
 };
 
@@ -377,7 +380,7 @@ struct SmXyzz {
 template <class F>
 struct GXyzz {
     const uint32_t* w;
-    KB_DEV void get(int f, Fe<F>& r) const { fe_load(r, w + f * F::N); }
+    KB_DEV void get(int f, Fe<F>& r) const { fe_load16(r, w + f * F::N); }  // w 16-byte aligned
     KB_DEV bool is_inf() const {
         uint32_t o = 0;
 #pragma unroll

@@ -488,6 +488,30 @@ KB_DEV void fe_store(uint32_t* dst, const Fe<F>& a) {
     for (int i = 0; i < F::N; ++i) dst[i] = a.v[i];
 }
 
+// The same through 16-byte accesses: src / dst 16-byte aligned (point
+// records are 2N or 4N words and N is a multiple of 4).
+template <class F>
+KB_DEV void fe_load16(Fe<F>& r, const uint32_t* src) {
+    static_assert(F::N % 4 == 0, "16-byte field access needs N % 4 == 0");
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+#pragma unroll
+    for (int k = 0; k < F::N / 4; ++k) {
+        const uint4 v = s[k];
+        r.v[4 * k] = v.x;
+        r.v[4 * k + 1] = v.y;
+        r.v[4 * k + 2] = v.z;
+        r.v[4 * k + 3] = v.w;
+    }
+}
+template <class F>
+KB_DEV void fe_store16(uint32_t* dst, const Fe<F>& a) {
+    static_assert(F::N % 4 == 0, "16-byte field access needs N % 4 == 0");
+    uint4* d = reinterpret_cast<uint4*>(dst);
+#pragma unroll
+    for (int k = 0; k < F::N / 4; ++k)
+        d[k] = make_uint4(a.v[4 * k], a.v[4 * k + 1], a.v[4 * k + 2], a.v[4 * k + 3]);
+}
+
 // Big-endian byte string (F::BYTES long) -> little-endian words.
 template <class F>
 KB_DEV void fe_from_be_bytes(Fe<F>& r, const uint8_t* b) {

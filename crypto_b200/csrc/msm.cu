@@ -163,7 +163,11 @@ static int ceil_log2(size_t n) {
 
 MsmPlan make_msm_plan(int curve, size_t n, const MsmOptions& opt) {
     MsmPlan p;
-    int c = opt.force_c;
+    static const int env_c = [] {
+        const char* v = std::getenv("KB200_MSM_C");
+        return v && *v ? std::atoi(v) : 0;
+    }();
+    int c = opt.force_c > 0 ? opt.force_c : env_c;
     if (c <= 0) c = msm_tune_get(curve, ceil_log2(n ? n : 1));
     if (c <= 0) {
         // Cost model in accumulation-entry units: one per entry over the
@@ -173,7 +177,8 @@ MsmPlan make_msm_plan(int curve, size_t n, const MsmOptions& opt) {
         double best = 1e300;
         for (int cc = 4; cc <= 20; ++cc) {
             const double wl = (double)((255 + cc - 1) / cc);
-            const double cost = wl * (double)n + RED_COST * wl * (double)(1u << (cc - 1));
+            const double red = wl * (double)n >= PAIRED_ENTRIES ? RED_COST_PAIRED : RED_COST;
+            const double cost = wl * (double)n + red * wl * (double)(1u << (cc - 1));
             if (cost < best) {
                 best = cost;
                 c = cc;
@@ -191,13 +196,18 @@ MsmPlan make_msm_plan(int curve, size_t n, const MsmOptions& opt) {
 
 MsmPlan make_msm_plan_glv(size_t n, const MsmOptions& opt) {
     MsmPlan p;
-    int c = opt.force_c;
+    static const int env_c = [] {
+        const char* v = std::getenv("KB200_MSM_GLV_C");
+        return v && *v ? std::atoi(v) : 0;
+    }();
+    int c = opt.force_c > 0 ? opt.force_c : env_c;
     if (c <= 0) {
         // 2n points, ceil(128/c) populated windows of the 128-bit halves.
         double best = 1e300;
         for (int cc = 4; cc <= 20; ++cc) {
             const double wl = (double)((128 + cc - 1) / cc);
-            const double cost = wl * 2.0 * (double)n + RED_COST * wl * (double)(1u << (cc - 1));
+            const double red = wl * 2.0 * (double)n >= PAIRED_ENTRIES ? RED_COST_PAIRED : RED_COST;
+            const double cost = wl * 2.0 * (double)n + red * wl * (double)(1u << (cc - 1));
             if (cost < best) {
                 best = cost;
                 c = cc;

@@ -37,6 +37,14 @@ namespace kb200 {
 // a fixed per-block part, the scan and tree phases, that the per-bucket
 // model does not see; window choices were checked against measured times.)
 constexpr double RED_COST = 2.8;
+// The same weight once the batch-affine pairing levels run (from about 2^22
+// sorted entries: a level needs 2M pair sums): entries cost less than a mixed addition, so a bucket
+// weighs more.  Fitted on B200: reduction 1.0 ms + 3.0 ns per bucket against
+// 0.40 ns per sorted entry (BLS12-381 GLV at 2^22, windows 16-19: 16 wins,
+// 33.5 ms against 35.0 ms for 19; BN254 at 2^24, windows 17-21: 17 wins,
+// 64.0 / 30.8 ms uniform / skewed against 67.3 / 36.4 ms for 20).
+constexpr double RED_COST_PAIRED = 7.5;
+constexpr double PAIRED_ENTRIES = (double)(1u << 22);
 
 struct MsmPlan {
     int c = 0;          // window bits
