@@ -759,8 +759,7 @@ void msm_run_wire(MsmEngine* e, const uint8_t* d_scalars, const uint8_t* d_point
     const MsmLaunchers& K = msm_launchers(e->curve);
     e->table.reserve(std::max<size_t>(1, n) * (glv ? 2 : 1) * (size_t)K.table_words * 4, st);
     e->mark(0, st);
-    K.wire_to_table(d_points, e->table.as<uint32_t>(), n, st);
-    if (glv) K.glv_rows(e->table.as<uint32_t>(), n, 0, n, st);
+    K.wire_to_table(d_points, e->table.as<uint32_t>(), n, glv ? n : 0, st);
     e->mark(1, st);
     msm_engine_launch(e, p, d_scalars, e->table.as<uint32_t>(), d_out_wire, d_out_comp, st);
 }
@@ -800,8 +799,7 @@ void msm_run_host_wire(MsmEngine* e, const uint8_t* h_scalars, const uint8_t* h_
         }
         KB_CUDA(cudaEventRecord(e->ev_chunk[c], e->st_copy));
         KB_CUDA(cudaStreamWaitEvent(e->st_conv, e->ev_chunk[c], 0));
-        K.wire_to_table(d_points + lo * WB, table + lo * TW, hi - lo, e->st_conv);
-        if (glv) K.glv_rows(table, n, lo, hi - lo, e->st_conv);
+        K.wire_to_table(d_points + lo * WB, table + lo * TW, hi - lo, glv ? n : 0, e->st_conv);
     }
     KB_CUDA(cudaEventRecord(e->ev_table, e->st_conv));
     e->mark(0, st);
@@ -811,7 +809,7 @@ void msm_run_host_wire(MsmEngine* e, const uint8_t* h_scalars, const uint8_t* h_
 
 void points_wire_to_table(int curve, const uint8_t* d_wire, uint32_t* d_table, size_t n,
                           cudaStream_t st) {
-    msm_launchers(curve).wire_to_table(d_wire, d_table, n, st);
+    msm_launchers(curve).wire_to_table(d_wire, d_table, n, 0, st);
 }
 
 void points_table_to_wire(int curve, const uint32_t* d_table, uint8_t* d_wire, size_t n,

@@ -123,7 +123,7 @@ struct RedArgs {
 };
 
 struct MsmLaunchers {
-    void (*wire_to_table)(const uint8_t*, uint32_t*, size_t, cudaStream_t);
+    void (*wire_to_table)(const uint8_t*, uint32_t*, size_t, size_t, cudaStream_t);
     void (*table_to_wire)(const uint32_t*, uint8_t*, size_t, cudaStream_t);
     void (*recode)(const ItemDesc*, uint32_t, unsigned long long, const uint32_t*,
                    const uint32_t*, uint32_t*, uint32_t*, cudaStream_t);

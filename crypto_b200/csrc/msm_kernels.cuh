@@ -8,14 +8,6 @@
 
 namespace kb200 {
 
-template <class C>
-__global__ void k_wire_to_table(const uint8_t* __restrict__ wire, uint32_t* __restrict__ table,
-                                size_t n) {
-    using F = typename C::F;
-    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    wire_to_table<C>(table + i * 2 * F::N, wire + i * C::WIRE);
-}
 
 template <class C>
 __global__ void k_table_to_wire(const uint32_t* __restrict__ table, uint8_t* __restrict__ wire,
@@ -53,6 +45,10 @@ static __constant__ uint32_t kGlvMu[9] = {0x896c72dd, 0xda5e4f8d, 0x268bf7a3, 0x
 static __constant__ uint32_t kGlvBeta2[12] = {0x0000aaac, 0x8bfd0000, 0x4f49fffd, 0x409427eb,
                                        0x0fb85f9b, 0x897d2965, 0x89759ad4, 0xaa0d857d,
                                        0x63d4de85, 0xec024086, 0x397fe699, 0x1a0111ea};
+// beta2 in Montgomery form (beta2 * 2^384 mod p).
+static __constant__ uint32_t kGlvBeta2Mont[12] = {0x8671f071, 0xcd03c9e4, 0x1fcda5d2, 0x5dab2246,
+                                           0xd3851b95, 0x587042af, 0x01bacb9e, 0x8eb60ebe,
+                                           0x83d050d2, 0x03f97d6e, 0x54638741, 0x18f02065};
 // 2^256 mod r: the reference's dropped top carry subtracts 2^256.
 static __constant__ uint32_t kR256ModR[8] = {0xfffffffe, 0x00000001, 0x00034802, 0x5884b7fa,
                                       0xecbc4ff5, 0x998c4fef, 0xacc5056f, 0x1824b159};
@@ -251,6 +247,75 @@ __global__ void k_recode(const ItemDesc* __restrict__ items, uint32_t n_items,
     emit(s, 8, row, it.entry_base + j, (unsigned long long)it.n, neg);
 }
 
+// Wire points (big-endian x || y, all-zero = infinity) -> table rows, read
+// in 16-byte pieces when the wire base is 16-byte aligned (rows are 64 or
+// 96 bytes), byte by byte otherwise.  glv_stride: 0, or the row distance of
+// the BLS12-381 GLV rows: row i + glv_stride gets phi(P_i) = (beta2 x, y).
+template <class C, bool V16>
+__global__ void k_wire_to_table(const uint8_t* __restrict__ wire, uint32_t* __restrict__ table,
+                                size_t n, size_t glv_stride) {
+    using F = typename C::F;
+    constexpr int N = F::N;
+    static_assert(C::WIRE == 8 * N, "wire row = two N-word coordinates");
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t m[2 * N];  // the row's 4-byte groups in memory order
+    if constexpr (V16) {
+        const uint4* s = reinterpret_cast<const uint4*>(wire + i * C::WIRE);
+#pragma unroll
+        for (int k = 0; k < N / 2; ++k) {
+            const uint4 v = s[k];
+            m[4 * k] = v.x;
+            m[4 * k + 1] = v.y;
+            m[4 * k + 2] = v.z;
+            m[4 * k + 3] = v.w;
+        }
+    } else {
+        const uint8_t* w = wire + i * C::WIRE;
+#pragma unroll
+        for (int q = 0; q < 2 * N; ++q)
+            m[q] = (uint32_t)w[4 * q] | ((uint32_t)w[4 * q + 1] << 8) | ((uint32_t)w[4 * q + 2] << 16) |
+                   ((uint32_t)w[4 * q + 3] << 24);
+    }
+    uint32_t any = 0;
+#pragma unroll
+    for (int q = 0; q < 2 * N; ++q) any |= m[q];
+    uint32_t* dst = table + i * 2 * N;
+    Fe<F> x, y;
+    if (!any) {
+        fe_zero(x);
+        fe_zero(y);
+        x.v[N - 1] = INF_FLAG;
+        fe_store16(dst, x);
+        fe_store16(dst + N, y);
+        if (glv_stride) {
+            fe_store16(dst + glv_stride * 2 * N, x);
+            fe_store16(dst + glv_stride * 2 * N + N, y);
+        }
+        return;
+    }
+    // limb l (little-endian words) = the big-endian group N - 1 - l, bytes swapped
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+        x.v[l] = __byte_perm(m[N - 1 - l], 0, 0x0123);
+        y.v[l] = __byte_perm(m[2 * N - 1 - l], 0, 0x0123);
+    }
+    fe_to_mont(x, x);
+    fe_to_mont(y, y);
+    fe_store16(dst, x);
+    fe_store16(dst + N, y);
+    if constexpr (C::CURVE_ID == 2) {
+        if (glv_stride) {
+            Fe<F> b;
+#pragma unroll
+            for (int k = 0; k < N; ++k) b.v[k] = kGlvBeta2Mont[k];
+            fe_mul(x, x, b);
+            fe_store16(dst + glv_stride * 2 * N, x);
+            fe_store16(dst + glv_stride * 2 * N + N, y);
+        }
+    }
+}
+
 // GLV rows: table[n + i] = phi(table[i]) = (beta2 x, y); infinity stays.
 template <class C>
 __global__ void k_glv_rows(uint32_t* __restrict__ table, size_t n, size_t first, size_t count) {
@@ -266,8 +331,7 @@ __global__ void k_glv_rows(uint32_t* __restrict__ table, size_t n, size_t first,
     }
     Fe<F> x, b;
     fe_load(x, src);
-    for (int k = 0; k < F::N; ++k) b.v[k] = kGlvBeta2[k];
-    fe_to_mont(b, b);
+    for (int k = 0; k < F::N; ++k) b.v[k] = kGlvBeta2Mont[k];
     fe_mul(x, x, b);
     fe_store(dst, x);
     for (int k = 0; k < F::N; ++k) dst[F::N + k] = src[F::N + k];
@@ -1018,9 +1082,13 @@ __global__ void k_combine(const ItemDesc* __restrict__ items, uint32_t n_items,
 template <class C>
 struct MsmLaunchImpl {
     using F = typename C::F;
-    static void wire_to_table(const uint8_t* w, uint32_t* t, size_t n, cudaStream_t st) {
+    static void wire_to_table(const uint8_t* w, uint32_t* t, size_t n, size_t glv_stride,
+                              cudaStream_t st) {
         if (!n) return;
-        k_wire_to_table<C><<<ceil_div_u(n, 128), 128, 0, st>>>(w, t, n);
+        if (((uintptr_t)w & 15) == 0)
+            k_wire_to_table<C, true><<<ceil_div_u(n, 128), 128, 0, st>>>(w, t, n, glv_stride);
+        else
+            k_wire_to_table<C, false><<<ceil_div_u(n, 128), 128, 0, st>>>(w, t, n, glv_stride);
         KB_LAUNCH_CHECK();
     }
     static void table_to_wire(const uint32_t* t, uint8_t* w, size_t n, cudaStream_t st) {

@@ -237,3 +237,31 @@ def test_host_pipeline_with_infinity_points(cuda_lib, curve, logn):
     S = b"".join(rng.randrange(O.FR[curve]).to_bytes(32, "little") for _ in range(n))
     want = O.ref_msm(curve, S, pts, n, threads=16) if O.ref_available() else O.msm(curve, S, pts, n)
     assert kb().gpukit_multi_pippenger(curve, S, pts, n) == want
+
+
+@pytest.mark.parametrize("curve", [1, 2])
+def test_device_entry_aligned_and_unaligned_points(cuda_lib, curve):
+    """kb200_msm_device reads wire points straight from device memory: in
+    16-byte pieces from an aligned base, byte by byte from any other (here
+    one byte past an aligned allocation); both give the oracle's bytes, with
+    infinity points among the inputs."""
+    import torch
+    n = 3001
+    pb = O.PB[curve]
+    pts = bytearray(rand_points(curve, n, seed=120 + curve))
+    for j in (0, 17, n - 1):
+        pts[pb * j:pb * (j + 1)] = bytes(pb)
+    pts = bytes(pts)
+    rng = random.Random(120 + curve)
+    S = b"".join(rng.randrange(O.FR[curve]).to_bytes(32, "little") for _ in range(n))
+    want = O.msm(curve, S, pts, n)
+    d_sc = torch.frombuffer(bytearray(S), dtype=torch.uint8).cuda()
+    d_out = torch.empty(pb, dtype=torch.uint8, device="cuda")
+    for shift in (0, 1):
+        buf = torch.zeros(n * pb + 16, dtype=torch.uint8, device="cuda")
+        buf[shift:shift + n * pb] = torch.frombuffer(bytearray(pts), dtype=torch.uint8).cuda()
+        rc = kb().lib().kb200_msm_device(curve, d_sc.data_ptr(), buf.data_ptr() + shift, n,
+                                         d_out.data_ptr(), None)
+        assert rc == 0, kb().last_error()
+        torch.cuda.synchronize()
+        assert bytes(d_out.cpu().numpy().tobytes()) == want, shift
