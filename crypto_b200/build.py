@@ -26,7 +26,7 @@ CUFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
                   "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 HOSTFLAGS = ["-O2", "-std=c++17", "-fPIC"]
 
-SOURCES = ["msm.cu", "msm_bls.cu", "msm_bn.cu", "ntt.cu", "kzg.cu", "scan.cu", "capi.cu", "batch.cu", "serve.cu", "autotune.cu", "wntt.cu", "eip2537.cu", "kzg_blob.cu",
+SOURCES = ["msm.cu", "msm_bls.cu", "msm_bn.cu", "ntt.cu", "kzg.cu", "scan.cu", "capi.cu", "batch.cu", "serve.cu", "autotune.cu", "wntt.cu", "eip2537.cu", "kzg_blob.cu", "selfcheck.cu",
            "inputs.cpp"]
 
 

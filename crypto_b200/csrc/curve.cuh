@@ -306,22 +306,6 @@ KB_DEV bool xyzz_to_affine(Affine<F>& a, const Xyzz<F>& p) {
     return true;
 }
 
-// xyzz_to_affine with the binary-Euclid inversion: for one conversion on a
-// thread's critical path (an MSM result), not for bulk conversions where a
-// warp's lanes would diverge.
-template <class F>
-KB_DEV bool xyzz_to_affine_single(Affine<F>& a, const Xyzz<F>& p) {
-    if (xyzz_is_inf(p)) return false;
-    Fe<F> t, inv;
-    fe_mul(t, p.ZZ, p.ZZZ);
-    fe_inv_binary(inv, t);    // 1 / (ZZ * ZZZ)
-    Fe<F> izz, izzz;
-    fe_mul(izz, inv, p.ZZZ);  // 1 / ZZ
-    fe_mul(izzz, inv, p.ZZ);  // 1 / ZZZ
-    fe_mul(a.x, p.X, izz);
-    fe_mul(a.y, p.Y, izzz);
-    return true;
-}
 
 // Memory helpers for XYZZ points stored as 4N consecutive words.
 template <class F>

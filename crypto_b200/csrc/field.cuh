@@ -353,9 +353,11 @@ KB_HD constexpr uint32_t pm2_word(int i) {
     return w;
 }
 
-// a^(p-2) by left-to-right square-and-multiply with 4-bit fixed windows.
+// a^(p-2) by left-to-right square-and-multiply with 4-bit fixed windows:
+// the reference the binary-GCD inversion is checked against on the device
+// (kb200_field_inverse_check).
 template <class F>
-__device__ __noinline__ void fe_inv(Fe<F>& r, const Fe<F>& a) {
+__device__ __noinline__ void fe_inv_fermat(Fe<F>& r, const Fe<F>& a) {
     Fe<F> tab[16];
     fe_one(tab[0]);
     tab[1] = a;
@@ -384,96 +386,232 @@ __device__ __noinline__ void fe_inv(Fe<F>& r, const Fe<F>& a) {
     r = acc;
 }
 
-// Inverse by the binary extended Euclidean algorithm on the stored words
-// (Montgomery in, Montgomery out).  The loop is data-dependent, so this is
-// for public values only (MSM results), where its few thousand word
-// operations replace the ~N*8*1.2 products of the Fermat chain on a single
-// thread's critical path.  With u = aR: (aR)^-1 * R^2 (two products by R2)
-// is the Montgomery form of a^-1.  a must be non-zero.
+// ---- Inversion by the optimized binary GCD ---------------------------------
+// Pornin, "Optimized Binary GCD for Modular Inversion" (IACR ePrint 2020/972),
+// Algorithm 2 with 32-bit words: each outer step runs 31 divsteps on 64-bit
+// approximations of (a, b) (their low 31 bits and top 33 bits), collecting
+// the 2x2 update (f0, g0; f1, g1) with |f| + |g| <= 2^31, then applies it to
+// the full values: a <- (a f0 + b g0) / 2^31, b <- (a f1 + b g1) / 2^31 (exact
+// divisions; a negative result is negated with its row of factors).  The
+// companions u, v follow with the same factors and a Montgomery division by
+// 2^31, so a = u y and b = v y (mod p) hold throughout; starting from u =
+// R^2 the final v is (aR)^-1 R^2 = a^-1 R, the Montgomery form of the inverse.
+// ceil((2 len(p) - 1) / 31) outer steps always end with b = 1 for y != 0.
+// Fixed trip counts and a branch-free divstep: the lanes of a warp stay
+// converged, so it serves bulk conversions as well as single results.
+namespace gcd_detail {
+
 template <class F>
-__device__ __noinline__ void fe_inv_binary(Fe<F>& r, const Fe<F>& a) {
-    constexpr int N = F::N;
-    uint32_t u[N], v[N], x1[N], x2[N], p[N];
-    for (int i = 0; i < N; ++i) {
-        u[i] = a.v[i];
-        v[i] = p[i] = F::P(i);
-        x1[i] = 0;
-        x2[i] = 0;
+KB_HD constexpr int bit_length_p() {
+    int top = F::N - 1;
+    while (top > 0 && F::P(top) == 0) --top;
+    uint32_t w = F::P(top);
+    int b = 0;
+    while (w) {
+        ++b;
+        w >>= 1;
     }
-    x1[0] = 1;
-    auto is_one = [](const uint32_t* w) {
-        uint32_t o = w[0] ^ 1u;
-        for (int i = 1; i < N; ++i) o |= w[i];
-        return o == 0;
-    };
-    auto halve = [&](uint32_t* w, uint32_t* x) {  // w /= 2; x = x / 2 mod p
-        for (int i = 0; i < N - 1; ++i) w[i] = (w[i] >> 1) | (w[i + 1] << 31);
-        w[N - 1] >>= 1;
-        uint32_t carry = 0;
-        if (x[0] & 1) {  // x + p is even and below 2^(32N) since x, p < 2^(32N - 1)
-            uint64_t c = 0;
-            for (int i = 0; i < N; ++i) {
-                c += (uint64_t)x[i] + p[i];
-                x[i] = (uint32_t)c;
-                c >>= 32;
-            }
-            carry = (uint32_t)c;
-        }
-        for (int i = 0; i < N - 1; ++i) x[i] = (x[i] >> 1) | (x[i + 1] << 31);
-        x[N - 1] = (x[N - 1] >> 1) | (carry << 31);
-    };
-    auto geq = [](const uint32_t* x, const uint32_t* y) {
-        for (int i = N - 1; i >= 0; --i)
-            if (x[i] != y[i]) return x[i] > y[i];
-        return true;
-    };
-    auto sub_mod = [&](uint32_t* x, const uint32_t* y) {  // x = x - y mod p (x, y < p)
-        int64_t c = 0;
-        for (int i = 0; i < N; ++i) {
-            c += (int64_t)x[i] - y[i];
-            x[i] = (uint32_t)c;
-            c >>= 32;
-        }
-        if (c < 0) {
-            uint64_t d = 0;
-            for (int i = 0; i < N; ++i) {
-                d += (uint64_t)x[i] + p[i];
-                x[i] = (uint32_t)d;
-                d >>= 32;
-            }
-        }
-    };
-    auto sub = [](uint32_t* x, const uint32_t* y) {
-        int64_t c = 0;
-        for (int i = 0; i < N; ++i) {
-            c += (int64_t)x[i] - y[i];
-            x[i] = (uint32_t)c;
-            c >>= 32;
-        }
-    };
-    // gcd(u, v) = 1 and u, v > 0 until one reaches 1; every step either
-    // halves u or v or makes one of them even, so at most 4 * 32N steps
-    // run (the guard only bounds the loop should that reasoning fail).
-    for (int guard = 0; guard < 8 * 32 * N && !is_one(u) && !is_one(v); ++guard) {
-        if (!(u[0] & 1)) {
-            halve(u, x1);
-        } else if (!(v[0] & 1)) {
-            halve(v, x2);
-        } else if (geq(u, v)) {
-            sub(u, v);
-            sub_mod(x1, x2);
+    return 32 * top + b;
+}
+
+// r (N + 2 words, two's complement) = x f + y g for non-negative N-word x, y
+// and |f|, |g| <= 2^31.
+template <int N>
+KB_DEV void lin_comb(uint32_t (&r)[N + 2], const uint32_t (&x)[N], const uint32_t (&y)[N], int64_t f,
+                     int64_t g) {
+    const uint32_t fa = (uint32_t)(f < 0 ? -f : f), ga = (uint32_t)(g < 0 ? -g : g);
+    const uint32_t mx = f < 0 ? 0xffffffffu : 0u, my = g < 0 ? 0xffffffffu : 0u;
+    uint64_t cx = 0, cy = 0, c = (uint64_t)(mx & 1u) + (my & 1u);
+#pragma unroll
+    for (int i = 0; i <= N; ++i) {
+        uint32_t px, py;
+        if (i < N) {
+            const uint64_t tx = (uint64_t)x[i] * fa + cx;
+            const uint64_t ty = (uint64_t)y[i] * ga + cy;
+            px = (uint32_t)tx;
+            py = (uint32_t)ty;
+            cx = tx >> 32;
+            cy = ty >> 32;
         } else {
-            sub(v, u);
-            sub_mod(x2, x1);
+            px = (uint32_t)cx;
+            py = (uint32_t)cy;
+        }
+        const uint64_t s = (uint64_t)(px ^ mx) + (py ^ my) + c;
+        r[i] = (uint32_t)s;
+        c = s >> 32;
+    }
+    r[N + 1] = mx + my + (uint32_t)c;
+}
+
+// r (N + 1 words, two's complement) = t / 2^31 for a two's-complement t of
+// N + 2 words whose low 31 bits are zero.
+template <int N>
+KB_DEV void shr31(uint32_t (&r)[N + 1], const uint32_t (&t)[N + 2]) {
+#pragma unroll
+    for (int i = 0; i <= N; ++i) r[i] = (t[i] >> 31) | (t[i + 1] << 1);
+}
+
+// x (N + 1 words, two's complement) -> |x| in place; returns true if x < 0.
+template <int N>
+KB_DEV bool abs_in_place(uint32_t (&x)[N + 1]) {
+    const bool neg = (x[N] >> 31) != 0;
+    const uint32_t m = neg ? 0xffffffffu : 0u;
+    uint64_t c = neg ? 1u : 0u;
+#pragma unroll
+    for (int i = 0; i <= N; ++i) {
+        const uint64_t s = (uint64_t)(x[i] ^ m) + c;
+        x[i] = (uint32_t)s;
+        c = s >> 32;
+    }
+    return neg;
+}
+
+// (u f + v g) / 2^31 mod p for u, v in [0, p): the sum plus q p with
+// q = -sum p^-1 mod 2^31 divides exactly; the quotient lies in (-2p, 2p).
+template <class F>
+KB_DEV void mont_comb(uint32_t (&r)[F::N], const uint32_t (&u)[F::N], const uint32_t (&v)[F::N], int64_t f,
+                      int64_t g) {
+    constexpr int N = F::N;
+    uint32_t t[N + 2];
+    lin_comb<N>(t, u, v, f, g);
+    const uint32_t q = (t[0] * F::M0) & 0x7fffffffu;
+    uint64_t c = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const uint64_t s = (uint64_t)F::P(i) * q + t[i] + c;
+        t[i] = (uint32_t)s;
+        c = s >> 32;
+    }
+    {
+        const uint64_t s = (uint64_t)t[N] + c;
+        t[N] = (uint32_t)s;
+        t[N + 1] += (uint32_t)(s >> 32);
+    }
+    uint32_t w[N + 1];
+    shr31<N>(w, t);
+    // into [0, p): add p while negative (at most twice), subtract p once if >= p
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const uint32_t m = (w[N] >> 31) ? 0xffffffffu : 0u;
+        uint64_t cc = 0;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            const uint64_t s = (uint64_t)w[i] + (F::P(i) & m) + cc;
+            w[i] = (uint32_t)s;
+            cc = s >> 32;
+        }
+        w[N] += (uint32_t)cc;
+    }
+    uint32_t d[N];
+    int64_t br = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const int64_t s = (int64_t)w[i] - F::P(i) + br;
+        d[i] = (uint32_t)s;
+        br = s >> 32;
+    }
+    const bool ge = (int64_t)w[N] + br >= 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r[i] = ge ? d[i] : w[i];
+}
+
+// Bits [s, s + 33) of the N-word x, for 31 <= s <= 32 N - 33.
+template <int N>
+KB_DEV uint64_t top33(const uint32_t (&x)[N], int s) {
+    const int wi = s >> 5, sh = s & 31;
+    uint32_t w0 = 0, w1 = 0, w2 = 0;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        w0 = k == wi ? x[k] : w0;
+        w1 = k == wi + 1 ? x[k] : w1;
+        w2 = k == wi + 2 ? x[k] : w2;
+    }
+    uint64_t v = (((uint64_t)w1 << 32) | w0) >> sh;
+    if (sh) v |= (uint64_t)w2 << (64 - sh);
+    return v & ((1ull << 33) - 1);
+}
+
+}  // namespace gcd_detail
+
+template <class F>
+__device__ __noinline__ void fe_inv_gcd(Fe<F>& r, const Fe<F>& y) {
+    using namespace gcd_detail;
+    constexpr int N = F::N;
+    constexpr int STEPS = (2 * bit_length_p<F>() - 1 + 30) / 31;
+    uint32_t a[N], b[N], u[N], v[N];
+    uint32_t any = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        a[i] = y.v[i];
+        b[i] = F::P(i);
+        u[i] = F::R2(i);
+        v[i] = 0;
+        any |= y.v[i];
+    }
+#pragma unroll 1
+    for (int it = 0; it < STEPS; ++it) {
+        // n = max(len a, len b, 64); approximations from the low 31 and top 33 bits
+        int n = 64;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const uint32_t w = a[k] | b[k];
+            n = w ? max(n, 32 * k + 32 - __clz(w)) : n;
+        }
+        uint64_t ab = (a[0] & 0x7fffffffu) | (top33<N>(a, n - 33) << 31);
+        uint64_t bb = (b[0] & 0x7fffffffu) | (top33<N>(b, n - 33) << 31);
+        int64_t f0 = 1, g0 = 0, f1 = 0, g1 = 1;
+#pragma unroll 1
+        for (int j = 0; j < 31; ++j) {
+            const bool odd = (ab & 1) != 0;
+            const bool sw = odd && ab < bb;
+            const uint64_t a2 = sw ? bb : ab, b2 = sw ? ab : bb;
+            const int64_t nf0 = sw ? f1 : f0, ng0 = sw ? g1 : g0;
+            const int64_t nf1 = sw ? f0 : f1, ng1 = sw ? g0 : g1;
+            ab = odd ? a2 - b2 : a2;
+            bb = b2;
+            f0 = odd ? nf0 - nf1 : nf0;
+            g0 = odd ? ng0 - ng1 : ng0;
+            f1 = nf1;
+            g1 = ng1;
+            ab >>= 1;
+            f1 <<= 1;
+            g1 <<= 1;
+        }
+        uint32_t ta[N + 2], tb[N + 2], na[N + 1], nb[N + 1];
+        lin_comb<N>(ta, a, b, f0, g0);
+        lin_comb<N>(tb, a, b, f1, g1);
+        shr31<N>(na, ta);
+        shr31<N>(nb, tb);
+        if (abs_in_place<N>(na)) {
+            f0 = -f0;
+            g0 = -g0;
+        }
+        if (abs_in_place<N>(nb)) {
+            f1 = -f1;
+            g1 = -g1;
+        }
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            a[i] = na[i];
+            b[i] = nb[i];
+        }
+        uint32_t nu[N], nv[N];
+        mont_comb<F>(nu, u, v, f0, g0);
+        mont_comb<F>(nv, u, v, f1, g1);
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            u[i] = nu[i];
+            v[i] = nv[i];
         }
     }
-    Fe<F> y, r2;
-    for (int i = 0; i < N; ++i) {
-        y.v[i] = is_one(u) ? x1[i] : x2[i];
-        r2.v[i] = F::R2(i);
-    }
-    fe_mul<F>(y, y, r2);
-    fe_mul<F>(r, y, r2);
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.v[i] = any ? v[i] : 0u;
+}
+
+// 1/a in Montgomery form (0 for 0).
+template <class F>
+KB_DEV void fe_inv(Fe<F>& r, const Fe<F>& a) {
+    fe_inv_gcd<F>(r, a);
 }
 
 // Load / store helpers for canonical little-endian words.

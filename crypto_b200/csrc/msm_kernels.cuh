@@ -446,7 +446,7 @@ __global__ void __launch_bounds__(128, C::ACC_MIN_BLOCKS) k_accumulate(AccArgs a
 //   k_inv_fwd    tree over the totals, INV_G elements per thread (strided so
 //                loads coalesce), down to at most INV_ROOT elements;
 //   k_inv_root   one block: warp-shuffle prefix/suffix products, one
-//                binary-Euclid inversion, each element's inverse;
+//                inversion, each element's inverse;
 //   k_inv_bwd    back up the tree: every total replaced by its inverse;
 //   k_pair_bwd   per thread, backwards over its slots: the slot's inverse from
 //                its prefix, then the affine sum.
@@ -699,7 +699,7 @@ __global__ void __launch_bounds__(256) k_inv_bwd(uint32_t* __restrict__ v, uint3
 }
 
 // The tree's root: the M <= INV_ROOT elements of v (word-major, stride M)
-// replaced by their inverses with one binary-Euclid inversion.  Elements are
+// replaced by their inverses with one field inversion.  Elements are
 // non-zero: every denominator is a difference of distinct x, or 2y with y
 // non-zero, or one.
 template <class F>
@@ -732,7 +732,7 @@ __global__ void __launch_bounds__(INV_ROOT) k_inv_root(uint32_t* __restrict__ v,
             fe_load(w, s_wt + q * N);
             fe_mul(pre[q], pre[q - 1], w);
         }
-        fe_inv_binary(inv, pre[NW - 1]);
+        fe_inv(inv, pre[NW - 1]);
         for (int q = NW - 1; q >= 0; --q) {
             fe_load(w, s_wt + q * N);
             if (q > 0)
@@ -1043,7 +1043,7 @@ __global__ void k_combine(const ItemDesc* __restrict__ items, uint32_t n_items,
         }
     }
     Affine<F> af;
-    const bool fin = xyzz_to_affine_single(af, acc);
+    const bool fin = xyzz_to_affine(af, acc);
     Fe<F> x, y;
     if (fin) {
         fe_from_mont(x, af.x);

@@ -264,6 +264,12 @@ int kb200_msm_window(uint32_t curve, size_t n);
 /* Expected bucket additions of one n-point MSM through the wire path (entries
  * of non-zero digits: points x populated windows x (1 - 2^-c)). */
 double kb200_msm_entries(uint32_t curve, size_t n);
+/* Device self-check of the field inversion used throughout (binary GCD)
+ * against the Fermat chain a^(p-2), plus x * x^-1 = 1, over `count` elements
+ * (edge values, then seeded pseudo-random ones) of field 0 = BLS12-381 Fp,
+ * 1 = BLS12-381 Fr, 2 = BN254 Fp, 3 = BN254 Fr.  *mismatches receives the
+ * number of failing elements.  Diagnostic: no reference counterpart. */
+int kb200_field_inverse_check(int field, uint64_t seed, size_t count, unsigned long long* mismatches);
 /* Number of this library's kernel launches since load. */
 unsigned long long kb200_launch_count(void);
 /* Per-stage CUDA-event timing of MSMs (off by default). */
