@@ -40,6 +40,29 @@ static uint32_t pair_threads(unsigned long long slots) {
     return (uint32_t)((slots + PAIR_J - 1) / PAIR_J);
 }
 
+// Per-chunk first pairing level: sub-run (c, b) of the chunk-major sort has
+// cnt[c B + b] output slots; cntT is the same counts bucket-major.
+__global__ void k_transpose_counts(const uint32_t* __restrict__ cnt, uint32_t B, uint32_t CH,
+                                   uint32_t* __restrict__ cntT) {
+    const size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= (size_t)B * CH) return;
+    const uint32_t c = (uint32_t)(r / B), b = (uint32_t)(r % B);
+    cntT[(size_t)b * CH + c] = cnt[r];
+}
+
+// From the bucket-major exclusive scan of the sub-run counts: each sub-run's
+// first output row (dst_off, chunk-major index) and each bucket's first row
+// (in1, B + 1 entries: the runs the next level reads).
+__global__ void k_chunk_offsets(const uint32_t* __restrict__ scanT, uint32_t B, uint32_t CH,
+                                uint32_t* __restrict__ dst_off, uint32_t* __restrict__ in1) {
+    const size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < (size_t)B * CH) {
+        const uint32_t c = (uint32_t)(r / B), b = (uint32_t)(r % B);
+        dst_off[r] = scanT[(size_t)b * CH + c];
+    }
+    if (r <= B) in1[r] = scanT[(size_t)r * CH];
+}
+
 // cnt[b] = ceil(m_b / 2) for the runs of a pairing level.
 __global__ void k_pair_counts(const uint32_t* __restrict__ in_off, uint32_t B, uint32_t* __restrict__ cnt) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -238,6 +261,11 @@ class MsmBatchPlan {
     // each level's output length (level l: (len_{l-1} + B) / 2).
     int pair_levels = 0;
     std::vector<unsigned long long> pair_len;
+    // Per-chunk first pairing level (single item, host-input pipeline): the
+    // sort runs over B_sort = B * chunks keys, chunk-major; chunk_len[c]
+    // bounds chunk c's level-0 output slots.
+    uint32_t chunks = 1, B_sort = 0, chunk_rows = 0;
+    std::vector<unsigned long long> chunk_len;
     DevBuf d_items, d_wins, d_blks;
     ~MsmBatchPlan() {
         d_items.release();
@@ -303,6 +331,8 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         d.W = n ? (uint32_t)plans[i].W : 0u;
         d.glv = glv ? 1u : 0u;
         d.glv_off = glv ? (uint32_t)opt.glv_rows : 0u;
+        d.chunk_rows = 0;
+        d.chunk_stride = 0;
         const bool shifted = opt.shift_c > 0 && !glv;
         d.row_stride = shifted ? (uint32_t)opt.shift_stride : 0u;
         d.Wr = shifted ? (n ? 1u : 0u) : d.W;
@@ -371,16 +401,41 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         }();
         const int fixed = opt.pair_levels >= 0 ? opt.pair_levels : env_levels;
         const int max_levels = fixed >= 0 ? fixed : PAIR_MAX_LEVELS;
+        // per-chunk level 0 splits every run into up to CH sub-runs (one more
+        // odd remainder each)
+        const uint32_t CH = (opt.point_chunks > 1 && count == 1 && P.items[0].n >= (uint32_t)opt.point_chunks)
+                                ? (uint32_t)opt.point_chunks
+                                : 1u;
         unsigned long long len = L;
         while (P.pair_levels < max_levels && total_live > 0 &&
                (fixed >= 0 || ((double)len >= PAIR_MIN_RUN * (double)total_live &&
                                len / 2 >= PAIR_MIN_SLOTS))) {
-            len = (len + B) / 2;
+            len = (len + B * (P.pair_levels == 0 ? CH : 1u)) / 2;
             P.pair_len.push_back(len);
             ++P.pair_levels;
         }
         L = len;  // entries left for the accumulation (upper bound)
         for (int l = 0; l < P.pair_levels; ++l) max_n = (max_n + 1) / 2;
+        P.chunks = P.pair_levels > 0 ? CH : 1u;
+        P.B_sort = P.B * P.chunks;
+        P.chunk_rows = 0;
+        P.chunk_len.clear();
+        if (P.chunks > 1) {
+            ItemDesc& d = P.items[0];
+            const uint32_t S = (d.n + P.chunks - 1) / P.chunks;
+            P.chunk_rows = S;
+            d.chunk_rows = S;
+            d.chunk_stride = P.B;
+            if ((unsigned long long)P.B * P.chunks >= 0xffffffffull)
+                throw std::invalid_argument("msm: too many chunk-major sort keys");
+            const unsigned long long per_row = (unsigned long long)d.W * (d.glv ? 2u : 1u);
+            for (uint32_t c = 0; c < P.chunks; ++c) {
+                const unsigned long long lo = (unsigned long long)c * S;
+                const unsigned long long hi = std::min<unsigned long long>(lo + S, d.n);
+                const unsigned long long ent = hi > lo ? (hi - lo) * per_row : 0ull;
+                P.chunk_len.push_back((ent + P.B) / 2);
+            }
+        }
     }
     // Chunk length: long chunks amortise the per-chunk records, but there must
     // be at least two chunks per resident accumulation thread.
@@ -461,22 +516,26 @@ class MsmEngine {
     int curve = 0;
     DevBuf table, keys, vals, counts, offsets, cursor, sorted, rec_first, rec_last, fold_buf,
         buckets, blk_out, win_out, scan_tmp, queue, fold_counts, fold_prefix, pair_off[2],
-        pair_rows[2], pair_scratch;
-    std::map<std::tuple<size_t, bool, int, int, int, size_t, bool, size_t>, MsmBatchPlan*> single_plans;
+        pair_rows[2], pair_scratch, pair_cntT, pair_dst, pair_in1;
+    std::map<std::tuple<size_t, bool, int, int, int, size_t, bool, size_t, int>, MsmBatchPlan*> single_plans;
     cudaEvent_t ev[N_STAGE_EVENTS] = {};
     bool ev_ready = false, ev_recorded = false;
     // Host-input pipeline (msm_run_host_wire): copy and conversion streams,
     // and events for the start, each point chunk and the finished table.
-    static constexpr int HOST_CHUNKS = 8;
+    // Point chunks of the host pipeline: 4 (measured at 2^22: 2, 3, 4, 6, 8
+    // chunks give 36.1, 36.5, 35.8, 36.9, 38.5 ms end to end; each chunk's
+    // first pairing level pays its own inversion tree and launches).
+    static constexpr int HOST_CHUNKS_MAX = 8;
+    static constexpr int HOST_CHUNKS = 4;
     cudaStream_t st_copy = nullptr, st_conv = nullptr;
-    cudaEvent_t ev_start = nullptr, ev_table = nullptr, ev_chunk[HOST_CHUNKS] = {};
+    cudaEvent_t ev_start = nullptr, ev_chunk[HOST_CHUNKS_MAX] = {}, ev_conv[HOST_CHUNKS_MAX] = {};
     void host_streams() {
         if (st_copy) return;
         KB_CUDA(cudaStreamCreateWithFlags(&st_copy, cudaStreamNonBlocking));
         KB_CUDA(cudaStreamCreateWithFlags(&st_conv, cudaStreamNonBlocking));
         KB_CUDA(cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming));
-        KB_CUDA(cudaEventCreateWithFlags(&ev_table, cudaEventDisableTiming));
         for (auto& c : ev_chunk) KB_CUDA(cudaEventCreateWithFlags(&c, cudaEventDisableTiming));
+        for (auto& c : ev_conv) KB_CUDA(cudaEventCreateWithFlags(&c, cudaEventDisableTiming));
     }
     void mark(int i, cudaStream_t st) {
         if (!profiling_enabled()) return;
@@ -495,13 +554,13 @@ class MsmEngine {
             cudaStreamDestroy(st_copy);
             cudaStreamDestroy(st_conv);
             cudaEventDestroy(ev_start);
-            cudaEventDestroy(ev_table);
             for (auto& c : ev_chunk) cudaEventDestroy(c);
+            for (auto& c : ev_conv) cudaEventDestroy(c);
         }
         for (DevBuf* b : {&table, &keys, &vals, &counts, &offsets, &cursor, &sorted, &rec_first,
                           &rec_last, &fold_buf, &buckets, &blk_out, &win_out, &scan_tmp, &queue,
                           &fold_counts, &fold_prefix, &pair_off[0], &pair_off[1], &pair_rows[0],
-                          &pair_rows[1], &pair_scratch})
+                          &pair_rows[1], &pair_scratch, &pair_cntT, &pair_dst, &pair_in1})
             b->release();
     }
 };
@@ -559,9 +618,10 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
     e->keys.reserve(L * 4, st);
     e->vals.reserve(L * 4, st);
     e->sorted.reserve(L * 4, st);
-    e->counts.reserve(((size_t)P.B + 1) * 4, st);
-    e->offsets.reserve(((size_t)P.B + 1) * 4, st);
-    e->cursor.reserve(((size_t)P.B + 1) * 4, st);
+    const size_t BS = std::max<size_t>(P.B, P.B_sort);
+    e->counts.reserve((BS + 1) * 4, st);
+    e->offsets.reserve((BS + 1) * 4, st);
+    e->cursor.reserve((BS + 1) * 4, st);
     const size_t nch = std::max<size_t>(1, P.nchunks);
     e->rec_first.reserve(nch * PW * 4, st);
     e->rec_last.reserve(nch * PW * 4, st);
@@ -569,14 +629,19 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
     e->buckets.reserve(std::max<size_t>(1, (size_t)P.B) * PW * 4, st);
     e->blk_out.reserve(std::max<size_t>(1, P.blks.size()) * 2 * PW * 4, st);
     e->win_out.reserve(std::max<size_t>(1, P.wins.size()) * PW * 4, st);
-    e->scan_tmp.reserve(scan_tmp_words(std::max<size_t>((size_t)P.B, P.big_cap) + 1) * 4, st);
+    e->scan_tmp.reserve(scan_tmp_words(std::max<size_t>(BS, P.big_cap) + 1) * 4, st);
     e->fold_counts.reserve((P.big_cap + 1) * 4, st);
     e->fold_prefix.reserve((P.big_cap + 1) * 4, st);
     e->queue.reserve((P.big_cap + 8) * 4, st);
     if (P.pair_levels > 0) {
         const size_t TW = (size_t)msm_launchers(e->curve).table_words;
+        if (P.chunks > 1) {
+            e->pair_cntT.reserve((BS + 1) * 4, st);
+            e->pair_dst.reserve((BS + 1) * 4, st);
+            e->pair_in1.reserve(((size_t)P.B + 1) * 4, st);
+        }
         for (int k = 0; k < 2 && k < P.pair_levels; ++k) {
-            e->pair_off[k].reserve(((size_t)P.B + 1) * 4, st);
+            e->pair_off[k].reserve((BS + 1) * 4, st);
             e->pair_rows[k].reserve(std::max<unsigned long long>(1, P.pair_len[k]) * TW * 4, st);
         }
         e->pair_scratch.reserve(pair_scratch_words(pair_threads(P.pair_len[0]), (int)TW / 2) * 4, st);
@@ -585,7 +650,7 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
 
 void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_scalars,
                        const uint32_t* d_table, uint8_t* d_out_wire, uint8_t* d_out_comp,
-                       cudaStream_t st, cudaEvent_t table_ready) {
+                       cudaStream_t st, const cudaEvent_t* table_ready, int n_ready) {
     const MsmBatchPlan& P = *p;
     const MsmLaunchers& K = msm_launchers(e->curve);
     const ItemDesc* items = P.d_items.as<ItemDesc>();
@@ -596,16 +661,17 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
                  st);
     }
     e->mark(2, st);
-    KB_CUDA(cudaMemsetAsync(e->counts.ptr, 0, ((size_t)P.B + 1) * 4, st));
+    const uint32_t BS = std::max<uint32_t>(P.B, P.B_sort);  // sort keys
+    KB_CUDA(cudaMemsetAsync(e->counts.ptr, 0, ((size_t)BS + 1) * 4, st));
     if (P.L > 0) {
         k_histogram<<<ceil_div_u(P.L, 256), 256, 0, st>>>(e->keys.as<uint32_t>(), P.L,
                                                          e->counts.as<uint32_t>());
         KB_LAUNCH_CHECK();
     }
-    exclusive_scan_u32(e->counts.as<uint32_t>(), e->offsets.as<uint32_t>(), P.B, 0,
+    exclusive_scan_u32(e->counts.as<uint32_t>(), e->offsets.as<uint32_t>(), BS, 0,
                        e->scan_tmp.as<uint32_t>(), st);
     if (P.L > 0) {
-        KB_CUDA(cudaMemcpyAsync(e->cursor.ptr, e->offsets.ptr, (size_t)P.B * 4,
+        KB_CUDA(cudaMemcpyAsync(e->cursor.ptr, e->offsets.ptr, (size_t)BS * 4,
                                 cudaMemcpyDeviceToDevice, st));
         k_scatter<<<ceil_div_u(P.L, 256), 256, 0, st>>>(e->keys.as<uint32_t>(), e->vals.as<uint32_t>(),
                                                        P.L, e->cursor.as<uint32_t>(),
@@ -613,13 +679,50 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
         KB_LAUNCH_CHECK();
     }
     e->mark(3, st);
-    if (table_ready) KB_CUDA(cudaStreamWaitEvent(st, table_ready, 0));
+    const bool per_chunk = P.chunks > 1 && table_ready && n_ready == (int)P.chunks && P.L > 0;
+    if (table_ready && n_ready > 0 && !per_chunk)
+        KB_CUDA(cudaStreamWaitEvent(st, table_ready[n_ready - 1], 0));
     // Pairing levels: the sorted runs shrink to about half per level, the
     // accumulation then reads the last level's rows directly.
     const uint32_t* off = e->offsets.as<uint32_t>();
     const uint32_t* acc_sorted = e->sorted.as<uint32_t>();
     const uint32_t* acc_table = d_table;
-    for (int l = 0; l < P.pair_levels && P.L > 0; ++l) {
+    int l0 = 0;
+    if (P.chunks > 1 && P.pair_levels > 0 && P.L > 0) {
+        // Level 0 per chunk of points: sub-run (c, b) pairs only the points of
+        // chunk c, so chunk c runs as soon as its rows exist; its sums land
+        // at bucket-major rows, so level 1 reads ordinary bucket runs.
+        const uint32_t CH = P.chunks, B = P.B;
+        uint32_t* out_off = e->pair_off[0].as<uint32_t>();
+        k_pair_counts<<<ceil_div_u(BS, 256), 256, 0, st>>>(off, BS, e->counts.as<uint32_t>());
+        KB_LAUNCH_CHECK();
+        exclusive_scan_u32(e->counts.as<uint32_t>(), out_off, BS, 0, e->scan_tmp.as<uint32_t>(), st);
+        k_transpose_counts<<<ceil_div_u(BS, 256), 256, 0, st>>>(e->counts.as<uint32_t>(), B, CH,
+                                                               e->pair_cntT.as<uint32_t>());
+        KB_LAUNCH_CHECK();
+        uint32_t* scanT = e->cursor.as<uint32_t>();  // free once the scatter is done
+        exclusive_scan_u32(e->pair_cntT.as<uint32_t>(), scanT, BS, 0, e->scan_tmp.as<uint32_t>(), st);
+        k_chunk_offsets<<<ceil_div_u((size_t)BS + 1, 256), 256, 0, st>>>(
+            scanT, B, CH, e->pair_dst.as<uint32_t>(), e->pair_in1.as<uint32_t>());
+        KB_LAUNCH_CHECK();
+        for (uint32_t c = 0; c < CH; ++c) {
+            if (per_chunk) KB_CUDA(cudaStreamWaitEvent(st, table_ready[c], 0));
+            PairArgs pa;
+            pa.in_off = off + (size_t)c * B;
+            pa.out_off = out_off + (size_t)c * B;
+            pa.B = B;
+            pa.sorted = acc_sorted;
+            pa.src = acc_table;
+            pa.dst = e->pair_rows[0].as<uint32_t>();
+            pa.dst_off = e->pair_dst.as<uint32_t>() + (size_t)c * B;
+            K.pair_level(pa, pair_threads(P.chunk_len[c]), e->pair_scratch.as<uint32_t>(), st);
+        }
+        off = e->pair_in1.as<uint32_t>();
+        acc_sorted = nullptr;
+        acc_table = e->pair_rows[0].as<uint32_t>();
+        l0 = 1;
+    }
+    for (int l = l0; l < P.pair_levels && P.L > 0; ++l) {
         uint32_t* out_off = e->pair_off[l & 1].as<uint32_t>();
         k_pair_counts<<<ceil_div_u(P.B, 256), 256, 0, st>>>(off, P.B, e->counts.as<uint32_t>());
         KB_LAUNCH_CHECK();
@@ -631,6 +734,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
         pa.sorted = acc_sorted;
         pa.src = acc_table;
         pa.dst = e->pair_rows[l & 1].as<uint32_t>();
+        pa.dst_off = nullptr;
         const unsigned long long slots = P.pair_len[l];
         K.pair_level(pa, pair_threads(slots), e->pair_scratch.as<uint32_t>(), st);
         off = out_off;
@@ -713,7 +817,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
 
 static MsmBatchPlan* single_plan(MsmEngine* e, size_t n, const MsmOptions& opt, cudaStream_t st) {
     auto key = std::make_tuple(n, opt.ref_carry_quirk, opt.force_c, opt.force_K, opt.shift_c,
-                               opt.shift_stride, opt.glv, opt.glv_rows);
+                               opt.shift_stride, opt.glv, opt.glv_rows, opt.point_chunks);
     auto it = e->single_plans.find(key);
     if (it != e->single_plans.end()) return it->second;
     MsmItem item{0, n, 0};
@@ -777,6 +881,14 @@ void msm_run_host_wire(MsmEngine* e, const uint8_t* h_scalars, const uint8_t* h_
         o2.glv = true;
         o2.glv_rows = n;
     }
+    // KB200_MSM_HOST_CHUNKS: point chunks of the host pipeline (1 .. HOST_CHUNKS_MAX)
+    static const int env_chunks = [] {
+        const char* v = std::getenv("KB200_MSM_HOST_CHUNKS");
+        return v && *v ? std::atoi(v) : 0;
+    }();
+    size_t chunks = n >= ((size_t)1 << 16) ? (size_t)MsmEngine::HOST_CHUNKS : 1;
+    if (env_chunks > 0) chunks = std::min<size_t>((size_t)env_chunks, (size_t)MsmEngine::HOST_CHUNKS_MAX);
+    o2.point_chunks = (int)chunks;
     MsmBatchPlan* p = single_plan(e, n, o2, st);
     msm_engine_reserve(e, p, st);
     const MsmLaunchers& K = msm_launchers(e->curve);
@@ -790,9 +902,11 @@ void msm_run_host_wire(MsmEngine* e, const uint8_t* h_scalars, const uint8_t* h_
     KB_CUDA(cudaStreamWaitEvent(e->st_copy, e->ev_start, 0));
     KB_CUDA(cudaStreamWaitEvent(e->st_conv, e->ev_start, 0));
     KB_CUDA(cudaMemcpyAsync(d_scalars, h_scalars, n * 32, cudaMemcpyHostToDevice, st));
-    const size_t chunks = n >= ((size_t)1 << 16) ? (size_t)MsmEngine::HOST_CHUNKS : 1;
+    // chunk c = rows [c S, (c + 1) S), S = ceil(n / chunks): the rows the
+    // plan's chunk-major sort keys (when it pairs per chunk) assign to c
+    const size_t S = (n + chunks - 1) / chunks;
     for (size_t c = 0; c < chunks; ++c) {
-        const size_t lo = n * c / chunks, hi = n * (c + 1) / chunks;
+        const size_t lo = std::min(n, c * S), hi = std::min(n, lo + S);
         if (hi > lo) {
             KB_CUDA(cudaMemcpyAsync(d_points + lo * WB, h_points + lo * WB, (hi - lo) * WB,
                                     cudaMemcpyHostToDevice, e->st_copy));
@@ -800,11 +914,11 @@ void msm_run_host_wire(MsmEngine* e, const uint8_t* h_scalars, const uint8_t* h_
         KB_CUDA(cudaEventRecord(e->ev_chunk[c], e->st_copy));
         KB_CUDA(cudaStreamWaitEvent(e->st_conv, e->ev_chunk[c], 0));
         K.wire_to_table(d_points + lo * WB, table + lo * TW, hi - lo, glv ? n : 0, e->st_conv);
+        KB_CUDA(cudaEventRecord(e->ev_conv[c], e->st_conv));
     }
-    KB_CUDA(cudaEventRecord(e->ev_table, e->st_conv));
     e->mark(0, st);
     e->mark(1, st);
-    msm_engine_launch(e, p, d_scalars, table, d_out_wire, nullptr, st, e->ev_table);
+    msm_engine_launch(e, p, d_scalars, table, d_out_wire, nullptr, st, e->ev_conv, (int)chunks);
 }
 
 void points_wire_to_table(int curve, const uint8_t* d_wire, uint32_t* d_table, size_t n,

@@ -77,6 +77,10 @@ struct MsmOptions {
     size_t glv_rows = 0;
     bool no_glv = false;  // msm_run_wire: keep the plain 256-bit windows
     int pair_levels = -1; // batch-affine pairing levels (-1: planner's choice or KB200_MSM_PAIR_LEVELS)
+    // Host-input pipeline: the first pairing level runs per chunk of point
+    // rows as the chunks arrive (sort keys chunk-major).  Single items only;
+    // ignored when the planner runs no pairing level.
+    int point_chunks = 1;
 };
 
 // Average entries per live bucket from which a batch-affine pairing level
@@ -126,12 +130,15 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t stream
 // synchronisation after msm_engine_reserve, so it can be captured in a
 // CUDA graph.  out_wire: count * WIRE bytes; out_comp: count * 48 bytes
 // (BLS12-381 only, may be null).
-// table_ready: null, or an event after which d_table is complete; the
-// recode and sort then run without reading the table and the stream waits
-// for the event before the first stage that reads points.
+// table_ready: null, or n_ready events recorded in order on one stream, the
+// last when d_table is complete (event c: the rows of point chunk c, when
+// the plan sorts by chunk).  The recode and sort then run without reading
+// the table; the stream waits for chunk c before its first pairing level,
+// or for the last event before the first stage that reads points.
 void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_scalars,
                        const uint32_t* d_table, uint8_t* d_out_wire, uint8_t* d_out_comp,
-                       cudaStream_t stream, cudaEvent_t table_ready = nullptr);
+                       cudaStream_t stream, const cudaEvent_t* table_ready = nullptr,
+                       int n_ready = 0);
 
 // Convenience single-MSM entry points (plan cached per (n, options)).
 void msm_run_wire(MsmEngine* e, const uint8_t* d_scalars, const uint8_t* d_points, size_t n,

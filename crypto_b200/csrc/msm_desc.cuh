@@ -26,6 +26,8 @@ struct ItemDesc {
     uint32_t out_index;             // result slot in the output arrays
     uint32_t glv;                   // 1: GLV split (BLS12-381), 2 W n entries
     uint32_t glv_off;               // row offset of the phi(P) rows in the table
+    uint32_t chunk_rows;            // >0: sort key (chunk of the point) * chunk_stride + bucket,
+    uint32_t chunk_stride;          //     chunk = point index / chunk_rows (per-chunk level 0)
 };
 
 // One window of one item.
@@ -86,6 +88,8 @@ struct PairArgs {
     const uint32_t* sorted;   // level 0: table rows | sign << 31; later levels: null
     const uint32_t* src;      // level 0: the point table; later: previous level's rows
     uint32_t* dst;            // output rows (affine, 2N words, infinity flagged)
+    const uint32_t* dst_off;  // null: slot k writes row k; else run r's slots go to rows
+                              // dst_off[r] + (k - out_off[r]) (per-chunk level 0)
 };
 
 // Pairing-level geometry: slots per thread of the pair passes, elements per

@@ -190,6 +190,10 @@ __global__ void k_recode(const ItemDesc* __restrict__ items, uint32_t n_items,
             const unsigned long long slot = slot0 + (unsigned long long)w * wstride;
             if (d == 0 || inf) {
                 keys[slot] = KEY_SENTINEL;
+            } else if (it.chunk_rows) {
+                keys[slot] = (j / it.chunk_rows) * it.chunk_stride + it.bucket_base +
+                             (uint32_t)w * M + (d - 1);
+                vals[slot] = prow | ((sign ^ negbit) << 31);
             } else if (it.row_stride) {
                 // shifted table: level w holds 2^(c*w) times the point, so every
                 // window feeds the same buckets
@@ -580,8 +584,8 @@ __global__ void __launch_bounds__(256) k_pair_fwd(PairArgs a, uint32_t T, uint32
     using F = typename C::F;
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
-    const uint32_t total = a.out_off[a.B];
-    const uint32_t k0 = t * (uint32_t)PAIR_J;
+    const uint32_t total = a.out_off[a.B];  // slots out_off[0] .. out_off[B]
+    const uint32_t k0 = a.out_off[0] + t * (uint32_t)PAIR_J;
     Fe<F> run;
     fe_one(run);
     if (k0 < total) {
@@ -606,7 +610,7 @@ __global__ void __launch_bounds__(256, 2) k_pair_bwd(PairArgs a, uint32_t T, con
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
     const uint32_t total = a.out_off[a.B];
-    const uint32_t k0 = t * (uint32_t)PAIR_J;
+    const uint32_t k0 = a.out_off[0] + t * (uint32_t)PAIR_J;
     if (k0 >= total) return;
     const uint32_t kend = min(k0 + (uint32_t)PAIR_J, total);
     Fe<F> inv_run;
@@ -626,7 +630,8 @@ __global__ void __launch_bounds__(256, 2) k_pair_bwd(PairArgs a, uint32_t T, con
         } else {
             inv = inv_run;
         }
-        uint32_t* dst = a.dst + (size_t)k * 2 * N;
+        const uint32_t row = a.dst_off ? a.dst_off[bend] + (k - a.out_off[bend]) : k;
+        uint32_t* dst = a.dst + (size_t)row * 2 * N;
         if (kind == PAIR_ADD || kind == PAIR_DBL) {
             Fe<F> lam, x3;
             if (kind == PAIR_ADD) {

@@ -219,7 +219,7 @@ print("ok")
     assert out.returncode == 0 and "ok" in out.stdout, out.stdout + out.stderr
 
 
-@pytest.mark.parametrize("curve,logn", [(2, 20), (1, 17)])
+@pytest.mark.parametrize("curve,logn", [(2, 20), (1, 17), (1, 20)])
 def test_host_pipeline_with_infinity_points(cuda_lib, curve, logn):
     """gpukit_multi_pippenger overlaps the point copy with the recode and
     sort (chunked copies, conversion per chunk), so infinity points reach
