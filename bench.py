@@ -118,9 +118,12 @@ def setup_dist():
     if ws > 1:
         import torch.distributed as dist
         import datetime
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:  # host-side rank logic without a GPU (tests)
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
     else:
         if torch.cuda.is_available():
             torch.cuda.set_device(local)
@@ -138,7 +141,8 @@ def max_over_ranks(ws, v: float) -> float:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
