@@ -178,6 +178,18 @@ static uint32_t top_buckets(int c, int W, int scalar_bits = 256) {
     return 1u << bits;
 }
 
+// Live buckets of the top window of a GLV half.  Both halves are below
+// max(lambda - 1, (r - 1) / lambda) = 0xac45a4010001a402_0000000100000000;
+// the top window is unsigned (its digit is the raw bits plus the carry from
+// below, never negated), so nothing carries beyond it and the halves need
+// ceil(128 / c) windows.  For c = 4, 8, 16 its digit exceeds 2^(c-1).
+static uint32_t glv_top_buckets(int c, int W) {
+    const unsigned __int128 bound =
+        ((unsigned __int128)0xac45a4010001a402ull << 64) | (unsigned __int128)0x0000000100000000ull;
+    const int sh = c * (W - 1);
+    return (uint32_t)(sh >= 128 ? 0 : (bound >> sh)) + 1u;
+}
+
 static int ceil_log2(size_t n) {
     int l = 0;
     while (((size_t)1 << l) < n) ++l;
@@ -240,9 +252,9 @@ MsmPlan make_msm_plan_glv(size_t n, const MsmOptions& opt) {
     if (c < 2) c = 2;
     if (c > 22) c = 22;
     p.c = c;
-    p.W = (129 + c - 1) / c;
+    p.W = (128 + c - 1) / c;
     p.M = 1u << (c - 1);
-    p.M_top = top_buckets(c, p.W, 128);
+    p.M_top = glv_top_buckets(c, p.W);
     return p;
 }
 
@@ -344,7 +356,9 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         d.entry_base = L;
         d.bucket_base = (uint32_t)B;
         L += (unsigned long long)d.W * n * (glv ? 2u : 1u);
-        B += (unsigned long long)d.Wr * d.M;
+        // the GLV top window may hold more than M buckets (unsigned digit)
+        B += (glv && d.W) ? (unsigned long long)(d.W - 1) * d.M + std::max(d.M, plans[i].M_top)
+                          : (unsigned long long)d.Wr * d.M;
         tot_sc = std::max<unsigned long long>(tot_sc, d.scalar_off + n);
     }
     if (B >= 0xffffffffull || L >= 0xffffffffull)

@@ -180,7 +180,8 @@ __global__ void k_recode(const ItemDesc* __restrict__ items, uint32_t n_items,
             }
             uint32_t d = raw + carry;
             uint32_t sign = 0;
-            if (d > M) {
+            // a GLV half's top window stays unsigned: nothing carries past it
+            if (d > M && !(it.glv && w == (int)it.W - 1)) {
                 d = (1u << c) - d;
                 sign = 1;
                 carry = 1;
