@@ -97,11 +97,13 @@ struct PairArgs {
 // inverts.
 constexpr int PAIR_J = 16;
 constexpr int INV_G = 16;
-constexpr int INV_ROOT = 256;
+constexpr int INV_ROOT_T = 512;               // threads of the root block
+constexpr int INV_ROOT = INV_ROOT_T * INV_G;  // elements the root block inverts
 
 // Scratch words of one pairing level with T0 pair threads and N-word field
 // elements: the pair prefixes and totals, then each tree level's prefixes
-// and totals (the layout pair_level carves).
+// and totals, then the root block's running products (the layout
+// pair_level carves).
 inline size_t pair_scratch_words(size_t T0, int N) {
     size_t w = (size_t)PAIR_J * N * T0;
     for (size_t M = T0; M > (size_t)INV_ROOT;) {
@@ -109,7 +111,7 @@ inline size_t pair_scratch_words(size_t T0, int N) {
         w += (size_t)INV_G * N * T;
         M = T;
     }
-    return w;
+    return w + (size_t)INV_G * N * INV_ROOT_T;  // the root block's running products
 }
 
 struct RedArgs {

@@ -450,7 +450,8 @@ __global__ void __launch_bounds__(128, C::ACC_MIN_BLOCKS) k_accumulate(AccArgs a
 //                products of its denominators (prefixes to HBM), total to tot[t];
 //   k_inv_fwd    tree over the totals, INV_G elements per thread (strided so
 //                loads coalesce), down to at most INV_ROOT elements;
-//   k_inv_root   one block: warp-shuffle prefix/suffix products, one
+//   k_inv_root   one block: INV_G-element chains per thread, warp-shuffle
+//                prefix/suffix products over threads and over warps, one
 //                inversion, each element's inverse;
 //   k_inv_bwd    back up the tree: every total replaced by its inverse;
 //   k_pair_bwd   per thread, backwards over its slots: the slot's inverse from
@@ -704,61 +705,92 @@ __global__ void __launch_bounds__(256) k_inv_bwd(uint32_t* __restrict__ v, uint3
     fe_store_wm(v, M, t, inv);
 }
 
-// The tree's root: the M <= INV_ROOT elements of v (word-major, stride M)
-// replaced by their inverses with one field inversion.  Elements are
-// non-zero: every denominator is a difference of distinct x, or 2y with y
-// non-zero, or one.
+// The tree's root in one block: the M <= INV_ROOT elements of v (word-major,
+// stride M) replaced by their inverses.  Thread t chains elements t, t + T,
+// t + 2T, ... (T = INV_ROOT_T; running products in pre, word-major with
+// stride T), then the thread totals combine by warp-shuffle prefix and
+// suffix products; warp 0 repeats that over the warp totals and its lane 0
+// inverts the grand total, so every thread recovers the inverse of its own
+// total and walks its chain back.  Elements are non-zero: every denominator
+// is a difference of distinct x, or 2y with y non-zero, or one.
 template <class F>
-__global__ void __launch_bounds__(INV_ROOT) k_inv_root(uint32_t* __restrict__ v, uint32_t M) {
-    constexpr int N = F::N;
-    constexpr int NW = INV_ROOT / 32;
-    __shared__ uint32_t s_wt[NW * N];
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    Fe<F> x, P, S, o;
-    if ((uint32_t)t < M)
-        fe_load_wm(x, v, M, t);
-    else
-        fe_one(x);
-    P = x;
-    S = x;
+__device__ __forceinline__ void warp_prefix_suffix(Fe<F>& P, Fe<F>& S, int lane) {
+    Fe<F> o;
     for (int d = 1; d < 32; d <<= 1) {  // inclusive prefix P and suffix S over the warp
 #pragma unroll
-        for (int q = 0; q < N; ++q) o.v[q] = __shfl_up_sync(0xffffffffu, P.v[q], d);
+        for (int q = 0; q < F::N; ++q) o.v[q] = __shfl_up_sync(0xffffffffu, P.v[q], d);
         if (lane >= d) fe_mul(P, P, o);
 #pragma unroll
-        for (int q = 0; q < N; ++q) o.v[q] = __shfl_down_sync(0xffffffffu, S.v[q], d);
+        for (int q = 0; q < F::N; ++q) o.v[q] = __shfl_down_sync(0xffffffffu, S.v[q], d);
         if (lane + d < 32) fe_mul(S, S, o);
     }
+}
+
+// r *= P_{lane-1} * S_{lane+1}: the product of the warp's other lanes' values.
+template <class F>
+__device__ __forceinline__ void warp_exclude_self(Fe<F>& r, const Fe<F>& P, const Fe<F>& S, int lane) {
+    Fe<F> o;
+#pragma unroll
+    for (int q = 0; q < F::N; ++q) o.v[q] = __shfl_up_sync(0xffffffffu, P.v[q], 1);
+    if (lane > 0) fe_mul(r, r, o);
+#pragma unroll
+    for (int q = 0; q < F::N; ++q) o.v[q] = __shfl_down_sync(0xffffffffu, S.v[q], 1);
+    if (lane < 31) fe_mul(r, r, o);
+}
+
+template <class F>
+__global__ void __launch_bounds__(INV_ROOT_T) k_inv_root(uint32_t* __restrict__ v, uint32_t M,
+                                                         uint32_t* __restrict__ pre) {
+    constexpr int N = F::N;
+    constexpr int NW = INV_ROOT_T / 32;
+    constexpr uint32_t T = INV_ROOT_T;
+    __shared__ uint32_t s_wt[NW * N];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    Fe<F> run, x;
+    fe_one(run);
+    uint32_t cnt = 0;
+    for (uint32_t e = (uint32_t)t; cnt < (uint32_t)INV_G && e < M; ++cnt, e += T) {
+        if (cnt) fe_store_wm(pre + (size_t)(cnt - 1) * N * T, T, (size_t)t, run);
+        fe_load_wm(x, v, M, e);
+        fe_mul(run, run, x);
+    }
+    Fe<F> P = run, S = run;
+    warp_prefix_suffix(P, S, lane);
     if (lane == 31) fe_store(s_wt + warp * N, P);
     __syncthreads();
-    if (t == 0) {  // Montgomery's trick over the warp totals
-        Fe<F> pre[NW], w, inv, y;
-        fe_load(pre[0], s_wt);
-        for (int q = 1; q < NW; ++q) {
-            fe_load(w, s_wt + q * N);
-            fe_mul(pre[q], pre[q - 1], w);
-        }
-        fe_inv(inv, pre[NW - 1]);
-        for (int q = NW - 1; q >= 0; --q) {
-            fe_load(w, s_wt + q * N);
-            if (q > 0)
-                fe_mul(y, inv, pre[q - 1]);
-            else
-                y = inv;
-            fe_mul(inv, inv, w);
-            fe_store(s_wt + q * N, y);  // 1 / (warp q's total)
-        }
+    if (warp == 0) {
+        Fe<F> w, P2, S2, inv;
+        if (lane < NW)
+            fe_load(w, s_wt + lane * N);
+        else
+            fe_one(w);
+        P2 = w;
+        S2 = w;
+        warp_prefix_suffix(P2, S2, lane);
+        Fe<F> tot;
+#pragma unroll
+        for (int q = 0; q < N; ++q) tot.v[q] = __shfl_sync(0xffffffffu, P2.v[q], 31);
+        if (lane == 0) fe_inv(inv, tot);
+#pragma unroll
+        for (int q = 0; q < N; ++q) inv.v[q] = __shfl_sync(0xffffffffu, inv.v[q], 0);
+        warp_exclude_self(inv, P2, S2, lane);  // 1 / (warp lane's total)
+        __syncwarp();
+        if (lane < NW) fe_store(s_wt + lane * N, inv);
     }
     __syncthreads();
     Fe<F> r;
-    fe_load(r, s_wt + warp * N);  // x^-1 = (total)^-1 * P_{lane-1} * S_{lane+1}
-#pragma unroll
-    for (int q = 0; q < N; ++q) o.v[q] = __shfl_up_sync(0xffffffffu, P.v[q], 1);
-    if (lane > 0) fe_mul(r, r, o);
-#pragma unroll
-    for (int q = 0; q < N; ++q) o.v[q] = __shfl_down_sync(0xffffffffu, S.v[q], 1);
-    if (lane < 31) fe_mul(r, r, o);
-    if ((uint32_t)t < M) fe_store_wm(v, M, t, r);
+    fe_load(r, s_wt + warp * N);
+    warp_exclude_self(r, P, S, lane);  // 1 / run
+    for (int j = (int)cnt - 1; j > 0; --j) {
+        const uint32_t e = (uint32_t)t + (uint32_t)j * T;
+        Fe<F> p;
+        fe_load_wm(x, v, M, e);
+        fe_load_wm(p, pre + (size_t)(j - 1) * N * T, T, (size_t)t);
+        fe_mul(p, p, r);  // 1 / x_j
+        fe_mul(r, r, x);
+        fe_store_wm(v, M, e, p);
+    }
+    if (cnt) fe_store_wm(v, M, (size_t)t, r);
 }
 
 // Fold level l >= 2: the level's (big bucket, group) items are flattened by
@@ -1126,7 +1158,7 @@ struct MsmLaunchImpl {
         uint32_t* cur = tot;
         uint32_t M = T0;
         uint32_t* next = tot + (size_t)N * T0;
-        while (M > (uint32_t)INV_ROOT) {  // M shrinks 16x per level: at most 8 levels
+        while (M > (uint32_t)INV_ROOT) {  // M shrinks 16x per level: at most 6 levels
             const uint32_t T = (M + INV_G - 1) / INV_G;
             uint32_t* pre = next;
             uint32_t* out = pre + (size_t)(INV_G - 1) * N * T;
@@ -1140,7 +1172,7 @@ struct MsmLaunchImpl {
             cur = out;
             M = T;
         }
-        k_inv_root<F><<<1, INV_ROOT, 0, st>>>(cur, M);
+        k_inv_root<F><<<1, INV_ROOT_T, 0, st>>>(cur, M, next);  // next: INV_G N INV_ROOT_T words
         KB_LAUNCH_CHECK();
         for (int r = R - 1; r >= 0; --r) {
             const uint32_t T = (lv_M[r] + INV_G - 1) / INV_G;
