@@ -69,21 +69,15 @@ __global__ void k_pair_counts(const uint32_t* __restrict__ in_off, uint32_t B, u
     if (b < B) cnt[b] = (in_off[b + 1] - in_off[b] + 1) >> 1;
 }
 
-__global__ void k_histogram(const uint32_t* __restrict__ keys, unsigned long long total,
-                            uint32_t* __restrict__ counts) {
-    const unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total) return;
-    const uint32_t key = keys[t];
-    const unsigned mask = __activemask();
-    const unsigned peers = __match_any_sync(mask, key);
-    const int leader = __ffs(peers) - 1;
-    if ((int)(threadIdx.x & 31) == leader && key != KEY_SENTINEL)
-        atomicAdd(&counts[key], (uint32_t)__popc(peers));
-}
-
-__global__ void k_scatter(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
-                          unsigned long long total, uint32_t* __restrict__ cursor,
-                          uint32_t* __restrict__ sorted) {
+// Counting sort of the (key, val) entries in two passes.  Pass 1 counts the
+// keys and gives every entry its rank among the entries of its key: a warp's
+// lanes with equal keys (match_any) take one atomicAdd for all of them, and
+// each lane's rank is that base plus the number of its peers below it.
+// Pass 2, after the scan of the counts, writes val to offsets[key] + rank:
+// no atomics.  The order inside a bucket is whatever order the atomics
+// granted; bucket sums do not depend on it.
+__global__ void k_rank(const uint32_t* __restrict__ keys, unsigned long long total,
+                       uint32_t* __restrict__ counts, uint32_t* __restrict__ ranks) {
     const unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= total) return;
     const uint32_t key = keys[t];
@@ -92,11 +86,19 @@ __global__ void k_scatter(const uint32_t* __restrict__ keys, const uint32_t* __r
     const int lane = threadIdx.x & 31;
     const int leader = __ffs(peers) - 1;
     uint32_t base = 0;
-    if (lane == leader && key != KEY_SENTINEL) base = atomicAdd(&cursor[key], (uint32_t)__popc(peers));
+    if (lane == leader && key != KEY_SENTINEL) base = atomicAdd(&counts[key], (uint32_t)__popc(peers));
     base = __shfl_sync(peers, base, leader);
+    ranks[t] = base + __popc(peers & ((1u << lane) - 1u));
+}
+
+__global__ void k_scatter(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                          const uint32_t* __restrict__ ranks, unsigned long long total,
+                          const uint32_t* __restrict__ offsets, uint32_t* __restrict__ sorted) {
+    const unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const uint32_t key = keys[t];
     if (key == KEY_SENTINEL) return;
-    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
-    sorted[base + rank] = vals[t];
+    sorted[offsets[key] + ranks[t]] = vals[t];
 }
 
 // Lists buckets spanning more than K2 + 1 chunks (list = {count, ids});
@@ -529,7 +531,7 @@ class MsmEngine {
    public:
     int curve = 0;
     DevBuf table, keys, vals, counts, offsets, cursor, sorted, rec_first, rec_last, fold_buf,
-        buckets, blk_out, win_out, scan_tmp, queue, fold_counts, fold_prefix, pair_off[2],
+        buckets, blk_out, win_out, scan_tmp, queue, fold_counts, fold_prefix, ranks, pair_off[2],
         pair_rows[2], pair_scratch, pair_cntT, pair_dst, pair_in1;
     std::map<std::tuple<size_t, bool, int, int, int, size_t, bool, size_t, int>, MsmBatchPlan*> single_plans;
     cudaEvent_t ev[N_STAGE_EVENTS] = {};
@@ -573,7 +575,7 @@ class MsmEngine {
         }
         for (DevBuf* b : {&table, &keys, &vals, &counts, &offsets, &cursor, &sorted, &rec_first,
                           &rec_last, &fold_buf, &buckets, &blk_out, &win_out, &scan_tmp, &queue,
-                          &fold_counts, &fold_prefix, &pair_off[0], &pair_off[1], &pair_rows[0],
+                          &fold_counts, &fold_prefix, &ranks, &pair_off[0], &pair_off[1], &pair_rows[0],
                           &pair_rows[1], &pair_scratch, &pair_cntT, &pair_dst, &pair_in1})
             b->release();
     }
@@ -601,13 +603,13 @@ static size_t pair_item_bytes(size_t TW, size_t L, size_t B) {
 
 // Upper bounds without building a plan (admission control calls these per
 // request).  Per item, with its plain-table window plan: keys, vals and the
-// sorted list (4 B per entry each), three 4 B bucket arrays and the bucket
+// sorted list and the ranks (4 B per entry each), three 4 B bucket arrays and the bucket
 // accumulators (per bucket), and the reduction blocks of its windows.
 size_t msm_item_scratch_bytes(int curve, size_t n) {
     const size_t PW = (size_t)(curve == 2 ? 48 : 32) * 4;
     const MsmPlan p = make_msm_plan(curve, n, MsmOptions());
     const size_t L = (size_t)p.W * n, B = (size_t)p.W * p.M;
-    return 12 * L + 12 * (B + 1) + B * PW + (size_t)p.W * (2 * RED_THREADS + 1) * PW +
+    return 16 * L + 12 * (B + 1) + B * PW + (size_t)p.W * (2 * RED_THREADS + 1) * PW +
            (L / 64 + 1) * (3 * PW + 4) +  // chunk records once lists are long (K = 64)
            pair_item_bytes(PW / 2, L, B);
 }
@@ -632,6 +634,7 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
     e->keys.reserve(L * 4, st);
     e->vals.reserve(L * 4, st);
     e->sorted.reserve(L * 4, st);
+    e->ranks.reserve(L * 4, st);
     const size_t BS = std::max<size_t>(P.B, P.B_sort);
     e->counts.reserve((BS + 1) * 4, st);
     e->offsets.reserve((BS + 1) * 4, st);
@@ -678,17 +681,16 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
     const uint32_t BS = std::max<uint32_t>(P.B, P.B_sort);  // sort keys
     KB_CUDA(cudaMemsetAsync(e->counts.ptr, 0, ((size_t)BS + 1) * 4, st));
     if (P.L > 0) {
-        k_histogram<<<ceil_div_u(P.L, 256), 256, 0, st>>>(e->keys.as<uint32_t>(), P.L,
-                                                         e->counts.as<uint32_t>());
+        k_rank<<<ceil_div_u(P.L, 256), 256, 0, st>>>(e->keys.as<uint32_t>(), P.L,
+                                                    e->counts.as<uint32_t>(), e->ranks.as<uint32_t>());
         KB_LAUNCH_CHECK();
     }
     exclusive_scan_u32(e->counts.as<uint32_t>(), e->offsets.as<uint32_t>(), BS, 0,
                        e->scan_tmp.as<uint32_t>(), st);
     if (P.L > 0) {
-        KB_CUDA(cudaMemcpyAsync(e->cursor.ptr, e->offsets.ptr, (size_t)BS * 4,
-                                cudaMemcpyDeviceToDevice, st));
         k_scatter<<<ceil_div_u(P.L, 256), 256, 0, st>>>(e->keys.as<uint32_t>(), e->vals.as<uint32_t>(),
-                                                       P.L, e->cursor.as<uint32_t>(),
+                                                       e->ranks.as<uint32_t>(), P.L,
+                                                       e->offsets.as<uint32_t>(),
                                                        e->sorted.as<uint32_t>());
         KB_LAUNCH_CHECK();
     }
