@@ -6,6 +6,9 @@
 #include "runtime.cuh"
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -186,16 +189,29 @@ static Prepared* prepare(CommitBatcher* B, const size_t* sizes, size_t count,
 
 // The device work of one batch: grouped inverse NTTs then the batched MSM.
 static void enqueue(CommitBatcher* B, Prepared* P, const uint32_t* srs, cudaStream_t st) {
+    static const bool trace = std::getenv("KB200_SERVE_TRACE") != nullptr;
+    using Clk = std::chrono::steady_clock;
+    auto t0 = Clk::now();
+    auto lap = [&](const char* what, size_t arg) {
+        if (!trace) return;
+        const auto t1 = Clk::now();
+        const double ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        if (ms > 2.0) std::fprintf(stderr, "[batcher] enqueue %s (%zu): %.3f ms\n", what, arg, ms);
+        t0 = t1;
+    };
     for (size_t k = 0; k < P->classes.size(); ++k) {
         const size_t n = P->classes[k].first, cnt = P->classes[k].second;
         ntt_run_list(B->ntt, B->evals.as<uint32_t>(), n, /*inverse=*/1, /*coset=*/0, cnt,
                      P->d_vec_off.as<unsigned long long>() + P->class_off[k],
                      B->scratch.as<uint32_t>(), st);
+        lap("ntt", n);
     }
     (void)srs;
-    for (size_t k = 0; k < P->ngroups; ++k)
+    for (size_t k = 0; k < P->ngroups; ++k) {
         msm_engine_launch(B->msm, P->groups[k].plan, B->evals.as<uint8_t>(), P->groups[k].table,
                           B->out_wire.as<uint8_t>(), B->out_comp.as<uint8_t>(), st);
+        lap("msm group", k);
+    }
 }
 
 static void run(CommitBatcher* B, Prepared* P, const uint32_t* srs, cudaStream_t st,

@@ -672,12 +672,22 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
     const MsmLaunchers& K = msm_launchers(e->curve);
     const ItemDesc* items = P.d_items.as<ItemDesc>();
     const uint32_t nitems = (uint32_t)P.count;
+    static const bool trace = std::getenv("KB200_SERVE_TRACE") != nullptr;
+    auto tt = std::chrono::steady_clock::now();
+    auto lap = [&](int where) {
+        if (!trace) return;
+        const auto t1 = std::chrono::steady_clock::now();
+        const double ms = std::chrono::duration<double, std::milli>(t1 - tt).count();
+        if (ms > 2.0) std::fprintf(stderr, "[msm] launch step %d: %.3f ms\n", where, ms);
+        tt = t1;
+    };
     if (P.L > 0) {
         K.recode(items, nitems, P.total_scalars, reinterpret_cast<const uint32_t*>(d_scalars),
                  table_ready ? nullptr : d_table, e->keys.as<uint32_t>(), e->vals.as<uint32_t>(),
                  st);
     }
     e->mark(2, st);
+    lap(2);
     const uint32_t BS = std::max<uint32_t>(P.B, P.B_sort);  // sort keys
     KB_CUDA(cudaMemsetAsync(e->counts.ptr, 0, ((size_t)BS + 1) * 4, st));
     if (P.L > 0) {
@@ -695,6 +705,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
         KB_LAUNCH_CHECK();
     }
     e->mark(3, st);
+    lap(3);
     const bool per_chunk = P.chunks > 1 && table_ready && n_ready == (int)P.chunks && P.L > 0;
     if (table_ready && n_ready > 0 && !per_chunk)
         KB_CUDA(cudaStreamWaitEvent(st, table_ready[n_ready - 1], 0));
@@ -766,6 +777,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
         KB_LAUNCH_CHECK();
     }
     e->mark(4, st);
+    lap(4);
 
     AccArgs acc;
     acc.sorted = acc_sorted;
@@ -784,6 +796,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
         K.accumulate(acc, std::max(1u, grid), st);
     }
     e->mark(5, st);
+    lap(5);
 
     if (P.levels >= 1 && P.L > 0) {
         FoldArgs fa;
@@ -810,6 +823,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
         }
     }
     e->mark(6, st);
+    lap(6);
 
     RedArgs ra;
     ra.offsets = off;
@@ -825,10 +839,13 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
     ra.win_out = e->win_out.as<uint32_t>();
     K.reduce_blocks(ra, (unsigned)P.blks.size(), st);
     e->mark(7, st);
+    lap(7);
     K.reduce_windows(ra, (unsigned)P.wins.size(), st);
     e->mark(8, st);
+    lap(8);
     K.combine(items, nitems, e->win_out.as<uint32_t>(), d_out_wire, d_out_comp, st);
     e->mark(9, st);
+    lap(9);
 }
 
 static MsmBatchPlan* single_plan(MsmEngine* e, size_t n, const MsmOptions& opt, cudaStream_t st) {

@@ -888,29 +888,33 @@ __device__ __forceinline__ void sm_store(uint32_t* sm, int t, const Xyzz<F>& p) 
     }
 }
 
-// In-place suffix scan over the RED_THREADS slots of sm:
+// In-place suffix scan over the first `width` slots of sm (a power of two
+// <= RED_THREADS; every thread of the block calls it):
 // afterwards slot t = sum_{t' >= t} old slot t'.
 template <class F>
-__device__ __forceinline__ void smem_suffix_scan(uint32_t* sm) {
+__device__ __forceinline__ void smem_suffix_scan(uint32_t* sm, int width = RED_THREADS) {
     const int t = threadIdx.x;
-    for (int d = 1; d < RED_THREADS; d <<= 1) {
+    for (int d = 1; d < width; d <<= 1) {
         Xyzz<F> y, o;
-        sm_load(y, sm, t);
-        if (t + d < RED_THREADS) {
-            sm_load(o, sm, t + d);
-            xyzz_add(y, o);
+        if (t < width) {
+            sm_load(y, sm, t);
+            if (t + d < width) {
+                sm_load(o, sm, t + d);
+                xyzz_add(y, o);
+            }
         }
         __syncthreads();
-        sm_store(sm, t, y);
+        if (t < width) sm_store(sm, t, y);
         __syncthreads();
     }
 }
 
-// In-place tree sum over the RED_THREADS slots of sm: afterwards slot 0 = sum.
+// In-place tree sum over the first `width` slots of sm (a power of two <=
+// RED_THREADS; every thread of the block calls it): afterwards slot 0 = sum.
 template <class F>
-__device__ __forceinline__ void smem_tree_sum(uint32_t* sm) {
+__device__ __forceinline__ void smem_tree_sum(uint32_t* sm, int width = RED_THREADS) {
     const int t = threadIdx.x;
-    for (int d = RED_THREADS >> 1; d >= 1; d >>= 1) {
+    for (int d = width >> 1; d >= 1; d >>= 1) {
         if (t < d) {
             Xyzz<F> y, o;
             sm_load(y, sm, t);
@@ -1024,7 +1028,11 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_windows(RedArgs a) {
         sm_store(sB, (int)t, Fb);
     }
     __syncthreads();
-    smem_suffix_scan<F>(sA);
+    // slots nb .. RED_THREADS-1 hold infinity: scan and sum only the power of
+    // two that covers the window's stage-1 blocks
+    int width = 1;
+    while (width < (int)wd.nb) width <<= 1;
+    smem_suffix_scan<F>(sA, width);
     Xyzz<F> Y0;
     if (t == 0) {
         sm_load(Y0, sA, 0);
@@ -1033,8 +1041,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_windows(RedArgs a) {
         sm_store(sA, 0, inf);
     }
     __syncthreads();
-    smem_tree_sum<F>(sA);
-    smem_tree_sum<F>(sB);
+    smem_tree_sum<F>(sA, width);
+    smem_tree_sum<F>(sB, width);
     // Warp 0 finishes: V = [blk] (sum over b >= 1 of Y_b) + sum Fb + Y_0,
     // then the window weight 2^(c*w).  The doubling chains run with their
     // products spread over the warp's lanes (three product latencies per

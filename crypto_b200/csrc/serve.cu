@@ -149,6 +149,27 @@ class KzgServer {
     std::string error;
     std::thread worker;
 
+    // Free device memory for admission.  cudaMemGetInfo is queried only while
+    // no batch of this server is in flight, at most once a second: measured
+    // on B200, calls made while large kernels ran stalled the worker thread
+    // for tens of milliseconds, which showed up as p99 latency.
+    size_t free_snapshot = 0;
+    Clock::time_point free_at{};
+    size_t device_free() {
+        bool busy = false;
+        for (const Slot& sl : slots) busy |= sl.busy;
+        const auto now = Clock::now();
+        if (free_snapshot == 0 || (!busy && now - free_at > std::chrono::seconds(1))) {
+            size_t f = 0, t = 0;
+            if (cudaMemGetInfo(&f, &t) != cudaSuccess) {
+                cudaGetLastError();
+                f = 0;
+            }
+            free_snapshot = f;
+            free_at = now;
+        }
+        return free_snapshot;
+    }
     void loop();
     bool launch_batch(Slot& s);
     void finish(Slot& s);
@@ -181,11 +202,7 @@ bool KzgServer::launch_batch(Slot& s) {
     std::vector<size_t> sizes;
     {
         std::lock_guard<std::mutex> lk(mu);
-        size_t free_b = 0, total_b = 0;
-        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
-            cudaGetLastError();
-            free_b = 0;
-        }
+        const size_t free_b = device_free();
         const size_t headroom = (size_t)256 << 20;
         const size_t avail = free_b > headroom ? free_b - headroom : 0;
         const size_t cap = mem_budget ? std::min(mem_budget, avail + 0) : avail;
@@ -223,8 +240,7 @@ bool KzgServer::launch_batch(Slot& s) {
                             cudaMemcpyDeviceToHost, s.stream));
     KB_CUDA(cudaEventRecord(s.done, s.stream));
     if (trace) {
-        size_t free_b = 0, total_b = 0;
-        cudaMemGetInfo(&free_b, &total_b);
+        const size_t free_b = free_snapshot;
         using ms = std::chrono::duration<double, std::milli>;
         std::fprintf(stderr, "[kzg_server] slot %d: %zu requests (%zu evaluations), host %.3f ms "
                              "(prepare %.3f, copies %.3f), queue left %zu, free %.1f GB\n",
@@ -338,6 +354,7 @@ void* kzg_server_create(size_t max_batch, int slots, size_t mem_budget_bytes) {
                 KB_CUDA(cudaStreamSynchronize(sl.stream));
             }
         }
+        s->device_free();  // first admission snapshot, device idle after the warm-up
         s->worker = std::thread([s] { s->loop(); });
         return s;
     } catch (const std::exception& e) {
