@@ -116,13 +116,17 @@ __global__ void k_list_big(const uint32_t* __restrict__ offsets, uint32_t B, uin
     }
 }
 
-// Group counts of fold level `level`, one per listed big bucket (zero past
-// the list's end); an exclusive scan of these flattens the level's work.
-__global__ void k_fold_counts(const uint32_t* __restrict__ offsets, uint32_t K, int FK, int level,
+// Group counts of every fold level at once: counts[(level - 2) big_cap + k]
+// for listed big bucket k (zero past the list's end).  One exclusive scan
+// of the whole array flattens each level's work; level l reads its slice
+// relative to the slice's first value.
+__global__ void k_fold_counts(const uint32_t* __restrict__ offsets, uint32_t K, int FK, int levels,
                               const uint32_t* __restrict__ big_list, uint32_t big_cap,
                               uint32_t* __restrict__ counts) {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= big_cap) return;
+    const size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= (size_t)levels * big_cap) return;
+    const int level = 2 + (int)(r / big_cap);
+    const uint32_t k = (uint32_t)(r % big_cap);
     uint32_t n = 0;
     if (k < min(big_list[0], big_cap)) {
         const uint32_t g = big_list[1 + k];
@@ -130,7 +134,7 @@ __global__ void k_fold_counts(const uint32_t* __restrict__ offsets, uint32_t K, 
         uint32_t t0, np;
         fold_sizes(o, c, K, FK, level, t0, np, n);
     }
-    counts[k] = n;
+    counts[r] = n;
 }
 
 // ---------------------------------------------------------------------------
@@ -646,9 +650,11 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
     e->buckets.reserve(std::max<size_t>(1, (size_t)P.B) * PW * 4, st);
     e->blk_out.reserve(std::max<size_t>(1, P.blks.size()) * 2 * PW * 4, st);
     e->win_out.reserve(std::max<size_t>(1, P.wins.size()) * PW * 4, st);
-    e->scan_tmp.reserve(scan_tmp_words(std::max<size_t>(BS, P.big_cap) + 1) * 4, st);
-    e->fold_counts.reserve((P.big_cap + 1) * 4, st);
-    e->fold_prefix.reserve((P.big_cap + 1) * 4, st);
+    e->scan_tmp.reserve(
+        scan_tmp_words(std::max<size_t>(BS, (size_t)std::max(1, P.levels) * P.big_cap) + 1) * 4, st);
+    const size_t fold_all = (size_t)std::max(1, P.levels) * P.big_cap;
+    e->fold_counts.reserve((fold_all + 1) * 4, st);
+    e->fold_prefix.reserve((fold_all + 1) * 4, st);
     e->queue.reserve((P.big_cap + 8) * 4, st);
     if (P.pair_levels > 0) {
         const size_t TW = (size_t)msm_launchers(e->curve).table_words;
@@ -811,13 +817,15 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
         fa.rec_first = e->rec_first.as<uint32_t>();
         uint32_t* in = e->rec_first.as<uint32_t>();
         uint32_t* out = e->fold_buf.as<uint32_t>();
+        const size_t all = (size_t)P.levels * P.big_cap;
+        k_fold_counts<<<ceil_div_u(all, 256), 256, 0, st>>>(off, (uint32_t)P.K, P.FK, P.levels, big_list,
+                                                           (uint32_t)P.big_cap,
+                                                           e->fold_counts.as<uint32_t>());
+        KB_LAUNCH_CHECK();
+        exclusive_scan_u32(e->fold_counts.as<uint32_t>(), e->fold_prefix.as<uint32_t>(), all, 0,
+                           e->scan_tmp.as<uint32_t>(), st);
         for (int l = 2; l <= P.levels + 1; ++l) {
-            k_fold_counts<<<ceil_div_u(P.big_cap, 256), 256, 0, st>>>(
-                off, (uint32_t)P.K, P.FK, l, big_list, (uint32_t)P.big_cap,
-                e->fold_counts.as<uint32_t>());
-            KB_LAUNCH_CHECK();
-            exclusive_scan_u32(e->fold_counts.as<uint32_t>(), e->fold_prefix.as<uint32_t>(),
-                               P.big_cap, 0, e->scan_tmp.as<uint32_t>(), st);
+            fa.prefix = e->fold_prefix.as<uint32_t>() + (size_t)(l - 2) * P.big_cap;
             K.fold(fa, l, in, out, (unsigned)device_sms() * 8, st);
             std::swap(in, out);
         }

@@ -74,7 +74,8 @@ struct FoldArgs {
     int FK;
     const uint32_t* big_list;
     uint32_t big_cap;
-    const uint32_t* prefix;  // per level: exclusive prefix of group counts (big_cap + 1)
+    const uint32_t* prefix;  // the level's slice (big_cap + 1) of the exclusive prefix of
+                             // all levels' group counts; relative to prefix[0]
     uint32_t* rec_first;
 };
 

@@ -803,19 +803,20 @@ __global__ void __launch_bounds__(128) k_fold(FoldArgs a, int level, const uint3
                                               uint32_t* __restrict__ out) {
     using F = typename C::F;
     constexpr int PW = 4 * F::N;
-    const uint32_t total = a.prefix[a.big_cap];
+    const uint32_t base = a.prefix[0];  // the level's slice of the all-levels scan
+    const uint32_t total = a.prefix[a.big_cap] - base;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total;
          i += gridDim.x * blockDim.x) {
-        uint32_t lo_k = 0, hi_k = a.big_cap;  // largest k with prefix[k] <= i
+        uint32_t lo_k = 0, hi_k = a.big_cap;  // largest k with prefix[k] - base <= i
         while (hi_k - lo_k > 1) {
             const uint32_t mid = (lo_k + hi_k) >> 1;
-            if (a.prefix[mid] <= i)
+            if (a.prefix[mid] - base <= i)
                 lo_k = mid;
             else
                 hi_k = mid;
         }
         const uint32_t g = a.big_list[1 + lo_k];
-        const uint32_t q = i - a.prefix[lo_k];
+        const uint32_t q = i - (a.prefix[lo_k] - base);
         const uint32_t o = a.offsets[g], c = a.offsets[g + 1] - o;
         uint32_t t0, n_prev, n_cur;
         fold_sizes(o, c, a.K, a.FK, level, t0, n_prev, n_cur);
