@@ -604,7 +604,7 @@ __global__ void __launch_bounds__(256) k_pair_fwd(PairArgs a, uint32_t T, uint32
     fe_store_wm(tot, T, t, run);  // one for threads without slots
 }
 
-template <class C>
+template <class C, bool DST_OFF>
 __global__ void __launch_bounds__(256, 2) k_pair_bwd(PairArgs a, uint32_t T, const uint32_t* __restrict__ pre,
                                                      const uint32_t* __restrict__ inv_tot) {
     using F = typename C::F;
@@ -632,7 +632,8 @@ __global__ void __launch_bounds__(256, 2) k_pair_bwd(PairArgs a, uint32_t T, con
         } else {
             inv = inv_run;
         }
-        const uint32_t row = a.dst_off ? a.dst_off[bend] + (k - a.out_off[bend]) : k;
+        uint32_t row = k;
+        if constexpr (DST_OFF) row = a.dst_off[bend] + (k - a.out_off[bend]);
         uint32_t* dst = a.dst + (size_t)row * 2 * N;
         if (kind == PAIR_ADD || kind == PAIR_DBL) {
             Fe<F> lam, x3;
@@ -1189,7 +1190,10 @@ struct MsmLaunchImpl {
                                                             r + 1 < R ? lv_v[r + 1] : cur);
             KB_LAUNCH_CHECK();
         }
-        k_pair_bwd<C><<<ceil_div_u(T0, 256), 256, 0, st>>>(a, T0, pre0, tot);
+        if (a.dst_off)
+            k_pair_bwd<C, true><<<ceil_div_u(T0, 256), 256, 0, st>>>(a, T0, pre0, tot);
+        else
+            k_pair_bwd<C, false><<<ceil_div_u(T0, 256), 256, 0, st>>>(a, T0, pre0, tot);
         KB_LAUNCH_CHECK();
     }
     static void glv_rows(uint32_t* table, size_t n, size_t first, size_t count, cudaStream_t st) {
