@@ -82,8 +82,18 @@ __global__ void k_rank(const uint32_t* __restrict__ keys, unsigned long long tot
     if (t >= total) return;
     const uint32_t key = keys[t];
     const unsigned mask = __activemask();
-    const unsigned peers = __match_any_sync(mask, key);
     const int lane = threadIdx.x & 31;
+    // Repeated keys (skewed scalars, where one bucket can take millions of
+    // entries) show up between neighbouring lanes; only then group the warp
+    // by key.  Without that, one atomic per lane: every atomicAdd returns a
+    // distinct rank, so both paths are exact.
+    const uint32_t up = __shfl_down_sync(mask, key, 1);
+    const bool dup = (lane < 31) && ((mask >> (lane + 1)) & 1u) && up == key && key != KEY_SENTINEL;
+    if (!__any_sync(mask, dup)) {
+        ranks[t] = key != KEY_SENTINEL ? atomicAdd(&counts[key], 1u) : 0u;
+        return;
+    }
+    const unsigned peers = __match_any_sync(mask, key);
     const int leader = __ffs(peers) - 1;
     uint32_t base = 0;
     if (lane == leader && key != KEY_SENTINEL) base = atomicAdd(&counts[key], (uint32_t)__popc(peers));
