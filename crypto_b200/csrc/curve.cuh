@@ -172,6 +172,77 @@ KB_DEV void xyzz_dbl_warp(Xyzz<F>& p) {
     fe_sub(p.Y, Ya, WY);  // Y3 = M(S - X3) - W Y
 }
 
+// Broadcast from lane k (0..3) of this thread's quad (lanes 4i .. 4i+3) to
+// the quad's four lanes; only the quad's lanes take part.
+template <class F>
+KB_DEV void fe_qbcast(Fe<F>& r, const Fe<F>& a, int k) {
+    const unsigned qm = 0xFu << (threadIdx.x & 28);
+#pragma unroll
+    for (int i = 0; i < F::N; ++i) r.v[i] = __shfl_sync(qm, a.v[i], k, 4);
+}
+
+// p += q (add-2008-s) with the products spread over the four lanes of a
+// quad: the 14 products fall into four dependent levels of at most four
+// independent ones, so the critical path is four product latencies instead
+// of fourteen.  All four lanes hold the same p and q on entry and the sum on
+// return (so every branch is uniform across the quad).  For latency-bound
+// reductions with spare lanes.
+template <class F>
+KB_DEV void xyzz_add_quad(Xyzz<F>& p, const Xyzz<F>& q) {
+    if (xyzz_is_inf(q)) return;
+    if (xyzz_is_inf(p)) {
+        p = q;
+        return;
+    }
+    const int ql = threadIdx.x & 3;
+    Fe<F> a, b, r;
+    // level 1: U1 = X1 ZZ2, U2 = X2 ZZ1, S1 = Y1 ZZZ2, S2 = Y2 ZZZ1
+    a = ql == 0 ? p.X : (ql == 1 ? q.X : (ql == 2 ? p.Y : q.Y));
+    b = ql == 0 ? q.ZZ : (ql == 1 ? p.ZZ : (ql == 2 ? q.ZZZ : p.ZZZ));
+    fe_mul(r, a, b);
+    Fe<F> U1, P, S1, R;
+    fe_qbcast(U1, r, 0);
+    fe_qbcast(P, r, 1);
+    fe_qbcast(S1, r, 2);
+    fe_qbcast(R, r, 3);
+    fe_sub(P, P, U1);  // P = U2 - U1
+    fe_sub(R, R, S1);  // R = S2 - S1
+    if (fe_is_zero(P)) {
+        if (fe_is_zero(R))
+            xyzz_dbl(p, p);
+        else
+            xyzz_set_inf(p);
+        return;
+    }
+    // level 2: PP = P^2, RR = R^2, ZZ1 ZZ2, ZZZ1 ZZZ2
+    a = ql == 0 ? P : (ql == 1 ? R : (ql == 2 ? p.ZZ : p.ZZZ));
+    b = ql == 0 ? P : (ql == 1 ? R : (ql == 2 ? q.ZZ : q.ZZZ));
+    fe_mul(r, a, b);
+    Fe<F> PP, RR;
+    fe_qbcast(PP, r, 0);
+    fe_qbcast(RR, r, 1);
+    fe_qbcast(p.ZZ, r, 2);   // ZZ1 ZZ2 for now
+    fe_qbcast(p.ZZZ, r, 3);  // ZZZ1 ZZZ2 for now
+    // level 3: PPP = P PP, Q = U1 PP, ZZ3 = ZZ1 ZZ2 PP
+    a = ql == 0 ? P : (ql == 1 ? U1 : p.ZZ);
+    fe_mul(r, a, PP);
+    fe_qbcast(P, r, 0);      // P <- PPP
+    fe_qbcast(U1, r, 1);     // U1 <- Q
+    fe_qbcast(p.ZZ, r, 2);
+    fe_sub(p.X, RR, P);
+    fe_sub(p.X, p.X, U1);
+    fe_sub(p.X, p.X, U1);    // X3 = R^2 - PPP - 2Q
+    fe_sub(U1, U1, p.X);     // Q - X3
+    // level 4: R (Q - X3), S1 PPP, ZZZ3 = ZZZ1 ZZZ2 PPP
+    a = ql == 0 ? R : (ql == 1 ? S1 : p.ZZZ);
+    b = ql == 0 ? U1 : P;
+    fe_mul(r, a, b);
+    fe_qbcast(R, r, 0);
+    fe_qbcast(S1, r, 1);
+    fe_qbcast(p.ZZZ, r, 2);
+    fe_sub(p.Y, R, S1);      // Y3 = R(Q - X3) - S1 PPP
+}
+
 // V = [k] V for a small k >= 0 by double-and-add, the doublings spread over
 // the warp (xyzz_dbl_warp); every lane holds the same point and performs the
 // same additions.  All 32 lanes must call it.

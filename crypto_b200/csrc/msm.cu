@@ -293,6 +293,7 @@ class MsmBatchPlan {
     // sort runs over B_sort = B * chunks keys, chunk-major; chunk_len[c]
     // bounds chunk c's level-0 output slots.
     uint32_t chunks = 1, B_sort = 0, chunk_rows = 0;
+    bool red_quad = false;  // stage-1 reduction by quads of lanes (k_reduce_blocks_quad)
     std::vector<unsigned long long> chunk_len;
     DevBuf d_items, d_wins, d_blks;
     ~MsmBatchPlan() {
@@ -394,6 +395,16 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
     const size_t per_wave = (size_t)2 * device_sms() * RED_THREADS;
     const uint32_t S0 = (uint32_t)std::min<size_t>(
         64, std::max<size_t>(1, (total_live + per_wave - 1) / per_wave));
+    // Few buckets (KZG commits up to 2^16, blobs): the reduction is bound by
+    // the latency of its serial additions, not by throughput, so it runs one
+    // quad of lanes per slot with the quad addition (k_reduce_blocks_quad),
+    // RED_QSLOTS slots per block and at most RED_QSLOTS blocks per window.
+    // KB200_MSM_RED_QUAD=0/1 forces the choice.
+    static const int env_quad = [] {
+        const char* v = std::getenv("KB200_MSM_RED_QUAD");
+        return v && *v ? std::atoi(v) : -1;
+    }();
+    P.red_quad = env_quad >= 0 ? env_quad != 0 : total_live <= RED_QUAD_MAX_LIVE;
     for (size_t i = 0; i < count; ++i) {
         ItemDesc& d = P.items[i];
         d.win_base = (uint32_t)P.wins.size();
@@ -404,8 +415,14 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
             const uint32_t per_block_min =
                 (uint32_t)(((size_t)wd.Mw + (size_t)RED_THREADS * RED_THREADS - 1) /
                            ((size_t)RED_THREADS * RED_THREADS));
-            wd.S = std::max<uint32_t>(S0, std::max<uint32_t>(1, per_block_min));
-            wd.blk = (uint32_t)RED_THREADS * wd.S;
+            if (P.red_quad) {
+                constexpr size_t QQ = (size_t)RED_QSLOTS * RED_QSLOTS;
+                wd.S = (uint32_t)std::max<size_t>(1, ((size_t)wd.Mw + QQ - 1) / QQ);
+                wd.blk = (uint32_t)RED_QSLOTS * wd.S;
+            } else {
+                wd.S = std::max<uint32_t>(S0, std::max<uint32_t>(1, per_block_min));
+                wd.blk = (uint32_t)RED_THREADS * wd.S;
+            }
             wd.nb = (wd.Mw + wd.blk - 1) / wd.blk;
             wd.shift = d.row_stride ? 0u : d.c * w;
             wd.blk_base = (uint32_t)P.blks.size();
@@ -855,7 +872,10 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
     ra.blks = P.d_blks.as<BlkDesc>();
     ra.blk_out = e->blk_out.as<uint32_t>();
     ra.win_out = e->win_out.as<uint32_t>();
-    K.reduce_blocks(ra, (unsigned)P.blks.size(), st);
+    if (P.red_quad)
+        K.reduce_blocks_quad(ra, (unsigned)P.blks.size(), st);
+    else
+        K.reduce_blocks(ra, (unsigned)P.blks.size(), st);
     e->mark(7, st);
     lap(7);
     K.reduce_windows(ra, (unsigned)P.wins.size(), st);

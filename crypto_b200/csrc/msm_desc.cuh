@@ -10,6 +10,8 @@ namespace kb200 {
 
 constexpr uint32_t KEY_SENTINEL = 0xffffffffu;
 constexpr int RED_THREADS = 256;
+constexpr int RED_QSLOTS = RED_THREADS / 4;       // slots of a quad-lane reduction block
+constexpr size_t RED_QUAD_MAX_LIVE = 16384;      // live buckets up to which the quads run
 
 // One MSM of a batch.
 struct ItemDesc {
@@ -139,6 +141,7 @@ struct MsmLaunchers {
     void (*glv_rows)(uint32_t*, size_t, size_t, size_t, cudaStream_t);
     void (*fold)(const FoldArgs&, int, const uint32_t*, uint32_t*, unsigned, cudaStream_t);
     void (*reduce_blocks)(const RedArgs&, unsigned, cudaStream_t);
+    void (*reduce_blocks_quad)(const RedArgs&, unsigned, cudaStream_t);
     void (*reduce_windows)(const RedArgs&, unsigned, cudaStream_t);
     void (*combine)(const ItemDesc*, uint32_t, const uint32_t*, uint8_t*, uint8_t*, cudaStream_t);
     int (*accumulate_occupancy)();

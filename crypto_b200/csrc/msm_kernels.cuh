@@ -867,6 +867,33 @@ __device__ __forceinline__ void bucket_add(const SmXyzz<F, RED_THREADS>& R, cons
     }
 }
 
+// bucket_add for a quad: R is held (identically) by the quad's four lanes
+// and every piece joins with the quad addition.
+template <class F>
+__device__ __forceinline__ void bucket_add_quad(Xyzz<F>& R, const RedArgs& a, uint32_t g) {
+    constexpr int PW = 4 * F::N;
+    const uint32_t o = a.offsets[g], c = a.offsets[g + 1] - o;
+    if (c == 0) return;
+    const uint32_t t0 = o / a.K, t1 = (o + c - 1) / a.K;
+    const uint32_t* first;
+    uint32_t npieces;
+    if (t0 == t1) {
+        const uint32_t e0 = t0 * a.K, e1 = min(e0 + a.K, a.offsets[a.B]);
+        first = (o == e0) ? a.rec_first + (size_t)t0 * PW
+                : (o + c == e1) ? a.rec_last + (size_t)t0 * PW
+                                : a.buckets + (size_t)g * PW;
+        npieces = 1;
+    } else {
+        first = ((o == t0 * a.K) ? a.rec_first : a.rec_last) + (size_t)t0 * PW;
+        npieces = 1 + ((t1 - t0 > (uint32_t)a.K2) ? 1u : (t1 - t0));
+    }
+    for (uint32_t k = 0; k < npieces; ++k) {
+        Xyzz<F> x;
+        xyzz_load(x, (k == 0) ? first : a.rec_first + (size_t)(t0 + k) * PW);
+        xyzz_add_quad(R, x);
+    }
+}
+
 // Shared-memory XYZZ arrays are word-major: word i of slot t lives at
 // sm[i * RED_THREADS + t], so a warp touching its 32 slots hits 32 banks.
 template <class F>
@@ -925,6 +952,99 @@ __device__ __forceinline__ void smem_tree_sum(uint32_t* sm, int width = RED_THRE
             sm_store(sm, t, y);
         }
         __syncthreads();
+    }
+}
+
+// The same scans over width <= RED_THREADS / 4 slots with one quad of lanes
+// per slot (slot = threadIdx.x / 4) and the quad addition: a quarter of the
+// depth in product latencies.  Every thread of the block calls them.
+template <class F>
+__device__ __forceinline__ void smem_suffix_scan_quad(uint32_t* sm, int width) {
+    const int sl = threadIdx.x >> 2;
+    for (int d = 1; d < width; d <<= 1) {
+        Xyzz<F> y, o;
+        if (sl < width) {
+            sm_load(y, sm, sl);
+            if (sl + d < width) {
+                sm_load(o, sm, sl + d);
+                xyzz_add_quad(y, o);
+            }
+        }
+        __syncthreads();
+        if (sl < width && (threadIdx.x & 3) == 0) sm_store(sm, sl, y);
+        __syncthreads();
+    }
+}
+
+template <class F>
+__device__ __forceinline__ void smem_tree_sum_quad(uint32_t* sm, int width) {
+    const int sl = threadIdx.x >> 2;
+    for (int d = width >> 1; d >= 1; d >>= 1) {
+        Xyzz<F> y, o;
+        if (sl < d) {
+            sm_load(y, sm, sl);
+            sm_load(o, sm, sl + d);
+            xyzz_add_quad(y, o);
+        }
+        __syncthreads();
+        if (sl < d && (threadIdx.x & 3) == 0) sm_store(sm, sl, y);
+        __syncthreads();
+    }
+}
+
+// Reduction stage 1 for small bucket counts (latency-bound: few blocks),
+// one quad per slot, RED_QSLOTS slots of S buckets per block, the quad
+// addition throughout; the same outputs as k_reduce_blocks (Fb, Sb per
+// block, with blk = RED_QSLOTS * S buckets per block).
+template <class C>
+__global__ void __launch_bounds__(RED_THREADS) k_reduce_blocks_quad(RedArgs a) {
+    using F = typename C::F;
+    constexpr int PW = 4 * F::N;
+    extern __shared__ __align__(16) uint32_t smr[];
+    uint32_t* sA = smr;
+    uint32_t* sB = smr + RED_THREADS * PW;
+    const BlkDesc bd = a.blks[blockIdx.x];
+    const WinDesc wd = a.wins[bd.win];
+    const uint32_t S = wd.S;
+    const int sl = threadIdx.x >> 2;
+    const uint32_t first = bd.b * wd.blk + (uint32_t)sl * S;
+    {
+        Xyzz<F> R, T;
+        xyzz_set_inf(R);
+        xyzz_set_inf(T);
+        for (int j = (int)S - 1; j >= 0; --j) {
+            if (first + (uint32_t)j < wd.Mw) bucket_add_quad(R, a, wd.bucket_base + first + (uint32_t)j);
+            if (j > 0) xyzz_add_quad(T, R);
+        }
+        if ((threadIdx.x & 3) == 0) {
+            sm_store(sA, sl, R);
+            sm_store(sB, sl, T);
+        }
+    }
+    __syncthreads();
+    smem_tree_sum_quad<F>(sB, RED_QSLOTS);    // sum of T: slot 0 of sB
+    smem_suffix_scan_quad<F>(sA, RED_QSLOTS); // Y_t = sum_{t' >= t} R_t'
+    Xyzz<F> Y0;
+    if (threadIdx.x < 32) sm_load(Y0, sA, 0);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Xyzz<F> inf;
+        xyzz_set_inf(inf);
+        sm_store(sA, 0, inf);
+    }
+    __syncthreads();
+    smem_tree_sum_quad<F>(sA, RED_QSLOTS);    // sum of Y_t, t >= 1
+    if (threadIdx.x < 32) {
+        // Fb = [S] (sum of Y_t, t >= 1) + sum of T_t; Sb = Y_0
+        Xyzz<F> V, u;
+        sm_load(V, sA, 0);
+        xyzz_mul_small_warp(V, S);
+        if (threadIdx.x == 0) {
+            sm_load(u, sB, 0);
+            xyzz_add(V, u);
+            xyzz_store(a.blk_out + ((size_t)blockIdx.x * 2) * PW, V);
+            xyzz_store(a.blk_out + ((size_t)blockIdx.x * 2 + 1) * PW, Y0);
+        }
     }
 }
 
@@ -1034,7 +1154,11 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_windows(RedArgs a) {
     // two that covers the window's stage-1 blocks
     int width = 1;
     while (width < (int)wd.nb) width <<= 1;
-    smem_suffix_scan<F>(sA, width);
+    const bool quad = width <= RED_QSLOTS;
+    if (quad)
+        smem_suffix_scan_quad<F>(sA, width);
+    else
+        smem_suffix_scan<F>(sA, width);
     Xyzz<F> Y0;
     if (t == 0) {
         sm_load(Y0, sA, 0);
@@ -1043,8 +1167,13 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_windows(RedArgs a) {
         sm_store(sA, 0, inf);
     }
     __syncthreads();
-    smem_tree_sum<F>(sA, width);
-    smem_tree_sum<F>(sB, width);
+    if (quad) {
+        smem_tree_sum_quad<F>(sA, width);
+        smem_tree_sum_quad<F>(sB, width);
+    } else {
+        smem_tree_sum<F>(sA, width);
+        smem_tree_sum<F>(sB, width);
+    }
     // Warp 0 finishes: V = [blk] (sum over b >= 1 of Y_b) + sum Fb + Y_0,
     // then the window weight 2^(c*w).  The doubling chains run with their
     // products spread over the warp's lanes (three product latencies per
@@ -1220,6 +1349,12 @@ struct MsmLaunchImpl {
         k_reduce_blocks<C><<<nblk, RED_THREADS, red_blocks_smem(), st>>>(a);
         KB_LAUNCH_CHECK();
     }
+    static void reduce_blocks_quad(const RedArgs& a, unsigned nblk, cudaStream_t st) {
+        if (!nblk) return;
+        set_smem_attr((const void*)k_reduce_blocks_quad<C>, red_smem());
+        k_reduce_blocks_quad<C><<<nblk, RED_THREADS, red_smem(), st>>>(a);
+        KB_LAUNCH_CHECK();
+    }
     static void reduce_windows(const RedArgs& a, unsigned nwin, cudaStream_t st) {
         if (!nwin) return;
         set_smem_attr((const void*)k_reduce_windows<C>, red_smem());
@@ -1247,6 +1382,7 @@ struct MsmLaunchImpl {
         L.pair_level = &pair_level;
         L.fold = &fold;
         L.reduce_blocks = &reduce_blocks;
+        L.reduce_blocks_quad = &reduce_blocks_quad;
         L.reduce_windows = &reduce_windows;
         L.combine = &combine;
         L.accumulate_occupancy = &accumulate_occupancy;

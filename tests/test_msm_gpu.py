@@ -265,3 +265,33 @@ def test_device_entry_aligned_and_unaligned_points(cuda_lib, curve):
         assert rc == 0, kb().last_error()
         torch.cuda.synchronize()
         assert bytes(d_out.cpu().numpy().tobytes()) == want, shift
+
+
+@pytest.mark.parametrize("quad,curve,logn", [(1, 2, 20), (1, 1, 17), (0, 2, 12), (0, 1, 14)])
+def test_reduction_modes_bit_exact(cuda_lib, quad, curve, logn):
+    """The bucket reduction has a quad-lane form for few buckets and the
+    per-thread form for many; forcing each where the planner picks the other
+    (KB200_MSM_RED_QUAD) gives the oracle's bytes: the quad form with several
+    buckets per slot over many windows, the per-thread form at small sizes."""
+    import os
+    import subprocess
+    import sys
+    code = r'''
+import random, sys
+sys.path.insert(0, "tests")
+import crypto_b200 as kb, _oracle as O
+from test_msm_gpu import rand_points
+curve, logn = %d, %d
+n = 1 << logn
+pts = rand_points(curve, n, seed=140 + logn)
+rng = random.Random(140 + logn)
+S = b"".join(rng.randrange(O.FR[curve]).to_bytes(32, "little") for _ in range(n))
+want = O.ref_msm(curve, S, pts, n, threads=16) if O.ref_available() else O.msm(curve, S, pts, n)
+assert kb.gpukit_multi_pippenger(curve, S, pts, n) == want
+print("ok")
+''' % (curve, logn)
+    env = dict(os.environ, KB200_MSM_RED_QUAD=str(quad))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True,
+                         text=True, timeout=900)
+    assert out.returncode == 0 and "ok" in out.stdout, out.stdout + out.stderr
