@@ -138,7 +138,6 @@ struct MsmLaunchers {
                    const uint32_t*, uint32_t*, uint32_t*, cudaStream_t);
     void (*accumulate)(const AccArgs&, unsigned, cudaStream_t);
     void (*pair_level)(const PairArgs&, uint32_t, uint32_t*, cudaStream_t);
-    void (*glv_rows)(uint32_t*, size_t, size_t, size_t, cudaStream_t);
     void (*fold)(const FoldArgs&, int, const uint32_t*, uint32_t*, unsigned, cudaStream_t);
     void (*reduce_blocks)(const RedArgs&, unsigned, cudaStream_t);
     void (*reduce_blocks_quad)(const RedArgs&, unsigned, cudaStream_t);

@@ -321,26 +321,6 @@ __global__ void k_wire_to_table(const uint8_t* __restrict__ wire, uint32_t* __re
     }
 }
 
-// GLV rows: table[n + i] = phi(table[i]) = (beta2 x, y); infinity stays.
-template <class C>
-__global__ void k_glv_rows(uint32_t* __restrict__ table, size_t n, size_t first, size_t count) {
-    using F = typename C::F;
-    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= count) return;
-    const size_t i = first + k;
-    const uint32_t* src = table + i * 2 * F::N;
-    uint32_t* dst = table + (n + i) * 2 * F::N;
-    if (aff_is_inf_words<F>(src)) {
-        for (int k = 0; k < 2 * F::N; ++k) dst[k] = src[k];
-        return;
-    }
-    Fe<F> x, b;
-    fe_load(x, src);
-    for (int k = 0; k < F::N; ++k) b.v[k] = kGlvBeta2Mont[k];
-    fe_mul(x, x, b);
-    fe_store(dst, x);
-    for (int k = 0; k < F::N; ++k) dst[F::N + k] = src[F::N + k];
-}
 
 template <class F>
 __device__ __forceinline__ void load_table_point(Affine<F>& a, const uint32_t* table, uint32_t idx) {
@@ -1325,13 +1305,6 @@ struct MsmLaunchImpl {
             k_pair_bwd<C, false><<<ceil_div_u(T0, 256), 256, 0, st>>>(a, T0, pre0, tot);
         KB_LAUNCH_CHECK();
     }
-    static void glv_rows(uint32_t* table, size_t n, size_t first, size_t count, cudaStream_t st) {
-        if constexpr (C::CURVE_ID == 2) {
-            if (!count) return;
-            k_glv_rows<C><<<ceil_div_u(count, 128), 128, 0, st>>>(table, n, first, count);
-            KB_LAUNCH_CHECK();
-        }
-    }
     static void accumulate(const AccArgs& a, unsigned grid, cudaStream_t st) {
         k_accumulate<C><<<grid, 128, 0, st>>>(a);
         KB_LAUNCH_CHECK();
@@ -1378,7 +1351,6 @@ struct MsmLaunchImpl {
         L.table_to_wire = &table_to_wire;
         L.recode = &recode;
         L.accumulate = &accumulate;
-        L.glv_rows = &glv_rows;
         L.pair_level = &pair_level;
         L.fold = &fold;
         L.reduce_blocks = &reduce_blocks;
