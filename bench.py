@@ -75,10 +75,20 @@ class ClockSampler:
                  "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.proc = None
+        # the sampler must be running before the timed region starts: wait for
+        # its first row (nvidia-smi takes a few hundred ms to start)
+        self.first_rows = 0
+        deadline = time.time() + 5.0
+        while self.proc and time.time() < deadline:
+            with open(self.path) as f:
+                self.first_rows = sum(1 for line in f if line.count(",") >= 7)
+            if self.first_rows:
+                break
+            time.sleep(0.02)
         return self
 
     def __exit__(self, *a):
@@ -93,7 +103,11 @@ class ClockSampler:
         if not self.path or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         rows = []
-        for line in open(self.path):
+        lines = [line for line in open(self.path) if line.count(",") >= 7]
+        # rows written during the timed region; if it was too short for one,
+        # the row taken just before it
+        during = lines[self.first_rows:] or lines[max(0, self.first_rows - 1):self.first_rows]
+        for line in during:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 8:
                 continue
@@ -107,7 +121,8 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v == "Active"})
         return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows),
+                "samples_in_timed_region": len(lines) - self.first_rows}
 
 
 def setup_dist():
