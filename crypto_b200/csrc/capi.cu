@@ -261,7 +261,7 @@ static int g1_msm_eip2537_host(uint8_t* rx, uint8_t* ry, const uint8_t* xycs, si
         std::lock_guard<std::mutex> lk(c->mu);
         cudaStream_t st = c->stream;
         c->d_e_in.reserve(size + 16, st);
-        c->d_e_tab.reserve(n * (size_t)table_words(2) * 4 + 16, st);
+        c->d_e_tab.reserve(2 * n * (size_t)table_words(2) * 4 + 16, st);  // + GLV rows
         c->d_e_sc.reserve(n * 32 + 16, st);
         c->d_e_out.reserve(256, st);
         c->h_out.reserve(256, st);
@@ -585,7 +585,7 @@ int kb200_bls12_381_g1_msm_device(const void* d_xycs, size_t size, void* d_out_w
                        DeviceCtx* c = get_ctx();
                        std::lock_guard<std::mutex> lk(c->mu);
                        cudaStream_t st = (cudaStream_t)stream;
-                       c->d_e_tab.reserve(n * (size_t)table_words(2) * 4 + 16, st);
+                       c->d_e_tab.reserve(2 * n * (size_t)table_words(2) * 4 + 16, st);  // + GLV rows
                        c->d_e_sc.reserve(n * 32 + 16, st);
                        g1_msm_eip2537_device(c->msm_for(2), (const uint8_t*)d_xycs, n,
                                              c->d_e_tab.as<uint32_t>(), c->d_e_sc.as<uint8_t>(),

@@ -30,6 +30,13 @@ struct G1BLS {
     static constexpr int CURVE_ID = 2;
     static constexpr int ACC_MIN_BLOCKS = KB_ACC_MIN_BLOCKS_BLS;
 };
+// GLV endomorphism of BLS12-381 G1: phi(x, y) = (beta2 x, y) = [lambda](x, y)
+// for lambda = u^2 - 1, with beta2 = 0x1a0111ea397fe699ec024086...0000aaac
+// (a cube root of unity mod p), here in Montgomery form (beta2 * 2^384 mod p).
+static __constant__ uint32_t kGlvBeta2Mont[12] = {0x8671f071, 0xcd03c9e4, 0x1fcda5d2, 0x5dab2246,
+                                                  0xd3851b95, 0x587042af, 0x01bacb9e, 0x8eb60ebe,
+                                                  0x83d050d2, 0x03f97d6e, 0x54638741, 0x18f02065};
+
 struct G1BN {
     using F = FpBN;
     static constexpr uint32_t B = 3;

@@ -57,12 +57,24 @@ __global__ void __launch_bounds__(128) k_g1msm_unpack(const uint8_t* __restrict_
             fe_store(row + F::N, a.y);
         }
     }
+    // GLV row n + i: phi(P) = (beta2 x, y) = [lambda]P, valid because every
+    // accepted point is in G1 (the subgroup check above)
+    uint32_t* grow = row + (size_t)n * 2 * F::N;
     if (!ok) atomicOr(flag, 1u);
     if (!ok || inf) {
-        for (int k = 0; k < 2 * F::N; ++k) row[k] = 0;
-        row[F::N - 1] = INF_FLAG;
+        for (int k = 0; k < 2 * F::N; ++k) row[k] = grow[k] = 0;
+        row[F::N - 1] = grow[F::N - 1] = INF_FLAG;
         for (int k = 0; k < 8; ++k) sc[k] = 0;
         return;
+    }
+    {
+        Fe<F> bx, b, yy;
+        fe_load(bx, row);
+        fe_load(yy, row + F::N);
+        for (int k = 0; k < F::N; ++k) b.v[k] = kGlvBeta2Mont[k];
+        fe_mul(bx, bx, b);
+        fe_store(grow, bx);
+        fe_store(grow + F::N, yy);
     }
     Fe<FR> s;
     fe_from_be_bytes(s, e + 128);
@@ -89,6 +101,8 @@ void g1_msm_eip2537_device(MsmEngine* eng, const uint8_t* d_xycs, size_t n, uint
         KB_LAUNCH_CHECK();
     }
     MsmOptions opt;
+    opt.glv = true;  // d_table holds the phi rows from row n on
+    opt.glv_rows = n;
     msm_run_table(eng, d_scalars, d_table, n, d_out_wire, nullptr, st, opt);
 }
 

@@ -12,7 +12,8 @@ namespace kb200 {
 
 // Validates and unpacks n entries of 160 bytes (x[64] || y[64] || c[32], big
 // endian) into the affine table and reduced little-endian scalars, then runs
-// the MSM.  d_table: n * 24 words, d_scalars: n * 32 bytes, d_flag: one word,
+// the MSM with the GLV split.  d_table: 2n * 24 words (rows n.. hold
+// phi(P) = (beta2 x, y)), d_scalars: n * 32 bytes, d_flag: one word,
 // set to 1 if any entry is invalid (coordinate >= p or top 16 bytes non-zero,
 // off the curve, or outside G1); d_out_wire: 96 bytes (x || y, 48 B BE each,
 // zeros for infinity).  Queued on `st`, nothing synchronised.

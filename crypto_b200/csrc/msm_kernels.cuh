@@ -42,13 +42,6 @@ __global__ void k_table_to_wire(const uint32_t* __restrict__ table, uint8_t* __r
 static __constant__ uint32_t kGlvLambda[4] = {0xffffffff, 0x00000000, 0x0001a402, 0xac45a401};
 static __constant__ uint32_t kGlvMu[9] = {0x896c72dd, 0xda5e4f8d, 0x268bf7a3, 0x389f49a7, 0xf6cfee30,
                                    0x63f6e522, 0xe01faadd, 0x7c6becf1, 0x00000001};
-static __constant__ uint32_t kGlvBeta2[12] = {0x0000aaac, 0x8bfd0000, 0x4f49fffd, 0x409427eb,
-                                       0x0fb85f9b, 0x897d2965, 0x89759ad4, 0xaa0d857d,
-                                       0x63d4de85, 0xec024086, 0x397fe699, 0x1a0111ea};
-// beta2 in Montgomery form (beta2 * 2^384 mod p).
-static __constant__ uint32_t kGlvBeta2Mont[12] = {0x8671f071, 0xcd03c9e4, 0x1fcda5d2, 0x5dab2246,
-                                           0xd3851b95, 0x587042af, 0x01bacb9e, 0x8eb60ebe,
-                                           0x83d050d2, 0x03f97d6e, 0x54638741, 0x18f02065};
 // 2^256 mod r: the reference's dropped top carry subtracts 2^256.
 static __constant__ uint32_t kR256ModR[8] = {0xfffffffe, 0x00000001, 0x00034802, 0x5884b7fa,
                                       0xecbc4ff5, 0x998c4fef, 0xacc5056f, 0x1824b159};
