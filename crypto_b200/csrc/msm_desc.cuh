@@ -95,26 +95,34 @@ struct PairArgs {
                               // dst_off[r] + (k - out_off[r]) (per-chunk level 0)
 };
 
-// Pairing-level geometry: slots per thread of the pair passes, elements per
-// thread of the batch-inversion tree, and the size the tree's root block
-// inverts.
+// Pairing-level geometry: slots per thread of the pair passes; the
+// batch inversion of the level's per-thread totals runs as one grid of
+// INV_T-thread blocks, each thread chaining up to INV_G elements and each
+// block inverting its own product.  G is the smallest chain length that keeps
+// the grid at about INV_FILL threads (two 256-thread blocks on each of 148
+// SMs), so large levels stay throughput-bound and small ones short.
 constexpr int PAIR_J = 16;
 constexpr int INV_G = 16;
-constexpr int INV_ROOT_T = 512;               // threads of the root block
-constexpr int INV_ROOT = INV_ROOT_T * INV_G;  // elements the root block inverts
+constexpr int INV_T = 256;
+constexpr size_t INV_FILL = (size_t)2 * 148 * INV_T;
+
+struct InvGeom {
+    uint32_t G;   // elements per thread
+    uint32_t nb;  // blocks
+};
+inline InvGeom inv_geom(size_t M) {
+    size_t G = (M + INV_FILL - 1) / INV_FILL;
+    G = G < 1 ? 1 : (G > (size_t)INV_G ? (size_t)INV_G : G);
+    const size_t per_block = (size_t)INV_T * G;
+    return {(uint32_t)G, (uint32_t)((M + per_block - 1) / per_block)};
+}
 
 // Scratch words of one pairing level with T0 pair threads and N-word field
-// elements: the pair prefixes and totals, then each tree level's prefixes
-// and totals, then the root block's running products (the layout
-// pair_level carves).
+// elements: the pair prefixes and totals, then the inversion's running
+// products (the layout pair_level carves).
 inline size_t pair_scratch_words(size_t T0, int N) {
-    size_t w = (size_t)PAIR_J * N * T0;
-    for (size_t M = T0; M > (size_t)INV_ROOT;) {
-        const size_t T = (M + INV_G - 1) / INV_G;
-        w += (size_t)INV_G * N * T;
-        M = T;
-    }
-    return w + (size_t)INV_G * N * INV_ROOT_T;  // the root block's running products
+    const InvGeom g = inv_geom(T0);
+    return (size_t)PAIR_J * N * T0 + (size_t)(g.G - 1) * N * g.nb * INV_T;
 }
 
 struct RedArgs {

@@ -417,20 +417,19 @@ __global__ void __launch_bounds__(128, C::ACC_MIN_BLOCKS) k_accumulate(AccArgs a
 // affine coordinates,
 //   lambda = (y1 - y0) / (x1 - x0)  (or 3 x0^2 / 2 y0 when the points are
 //   equal), x3 = lambda^2 - x0 - x1, y3 = lambda (x0 - x3) - y0,
-// with infinity where they cancel.  All denominators of a level share ONE
-// inversion (Montgomery's trick over the whole grid):
+// with infinity where they cancel.  The denominators are inverted together
+// (Montgomery's trick, one field inversion per block of k_inv_wide):
 //   k_pair_fwd   thread t owns slots [PAIR_J t, PAIR_J t + PAIR_J): running
 //                products of its denominators (prefixes to HBM), total to tot[t];
-//   k_inv_fwd    tree over the totals, INV_G elements per thread (strided so
-//                loads coalesce), down to at most INV_ROOT elements;
-//   k_inv_root   one block: INV_G-element chains per thread, warp-shuffle
+//   k_inv_wide   every total replaced by its inverse: blocks of INV_T
+//                threads, each thread chaining up to INV_G totals, warp-shuffle
 //                prefix/suffix products over threads and over warps, one
-//                inversion, each element's inverse;
-//   k_inv_bwd    back up the tree: every total replaced by its inverse;
+//                inversion per block;
 //   k_pair_bwd   per thread, backwards over its slots: the slot's inverse from
 //                its prefix, then the affine sum.
 // Per addition: 1 product forward, 2 to recover the inverse, 3 for the sum,
-// plus 3/PAIR_J for the tree, against 10 for a mixed XYZZ addition.  Field
+// plus about 4/PAIR_J for the totals' inversion, against 10 for a mixed XYZZ
+// addition.  Field
 // elements in the scratch arrays are stored word-major (word q of element e
 // at q * stride + e) so that consecutive threads touch consecutive words.
 enum PairCase : int { PAIR_PASS0 = 0, PAIR_PASS1 = 1, PAIR_INF = 2, PAIR_ADD = 3, PAIR_DBL = 4 };
@@ -639,54 +638,7 @@ __global__ void __launch_bounds__(256, 2) k_pair_bwd(PairArgs a, uint32_t T, con
     }
 }
 
-// Tree level: thread t < T = ceil(M / INV_G) multiplies elements t, t + T,
-// t + 2T, ... of v (M elements, word-major), keeping the running products
-// in pre and the total in out[t].
-template <class F>
-__global__ void __launch_bounds__(256) k_inv_fwd(const uint32_t* __restrict__ v, uint32_t M, uint32_t T,
-                                                 uint32_t* __restrict__ pre, uint32_t* __restrict__ out) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= T) return;
-    Fe<F> run, x;
-    fe_load_wm(run, v, M, t);
-    for (uint32_t j = 1, e = t + T; j < (uint32_t)INV_G && e < M; ++j, e += T) {
-        fe_store_wm(pre + (size_t)(j - 1) * F::N * T, T, t, run);
-        fe_load_wm(x, v, M, e);
-        fe_mul(run, run, x);
-    }
-    fe_store_wm(out, T, t, run);
-}
-
-// Inverse of the tree level: out[t] holds the inverse of thread t's total;
-// each of its elements is replaced by its own inverse.
-template <class F>
-__global__ void __launch_bounds__(256) k_inv_bwd(uint32_t* __restrict__ v, uint32_t M, uint32_t T,
-                                                 const uint32_t* __restrict__ pre,
-                                                 const uint32_t* __restrict__ out) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= T) return;
-    const uint32_t cnt = min((uint32_t)INV_G, (M - t + T - 1) / T);
-    Fe<F> inv, x, r;
-    fe_load_wm(inv, out, T, t);
-    for (int j = (int)cnt - 1; j > 0; --j) {
-        const uint32_t e = t + (uint32_t)j * T;
-        fe_load_wm(x, v, M, e);
-        fe_load_wm(r, pre + (size_t)(j - 1) * F::N * T, T, t);
-        fe_mul(r, r, inv);
-        fe_mul(inv, inv, x);
-        fe_store_wm(v, M, e, r);
-    }
-    fe_store_wm(v, M, t, inv);
-}
-
-// The tree's root in one block: the M <= INV_ROOT elements of v (word-major,
-// stride M) replaced by their inverses.  Thread t chains elements t, t + T,
-// t + 2T, ... (T = INV_ROOT_T; running products in pre, word-major with
-// stride T), then the thread totals combine by warp-shuffle prefix and
-// suffix products; warp 0 repeats that over the warp totals and its lane 0
-// inverts the grand total, so every thread recovers the inverse of its own
-// total and walks its chain back.  Elements are non-zero: every denominator
-// is a difference of distinct x, or 2y with y non-zero, or one.
+// Inclusive prefix P and suffix S products of the warp's values.
 template <class F>
 __device__ __forceinline__ void warp_prefix_suffix(Fe<F>& P, Fe<F>& S, int lane) {
     Fe<F> o;
@@ -712,19 +664,30 @@ __device__ __forceinline__ void warp_exclude_self(Fe<F>& r, const Fe<F>& P, cons
     if (lane < 31) fe_mul(r, r, o);
 }
 
+// The M elements of v (word-major, stride M) replaced by their inverses.
+// Block b owns elements [b G INV_T, (b + 1) G INV_T); its thread t chains
+// elements base + j INV_T (j < G, base = b G INV_T + t; running products in
+// pre, word-major with stride TT = gridDim.x INV_T), the thread products
+// combine by warp-shuffle prefix and suffix products, warp 0 repeats that over
+// the warp products and its lane 0 inverts the block's product, so every
+// thread recovers the inverse of its own product and walks its chain back.
+// Elements are non-zero: every denominator is a difference of distinct x, or
+// 2y with y non-zero, or one.
 template <class F>
-__global__ void __launch_bounds__(INV_ROOT_T) k_inv_root(uint32_t* __restrict__ v, uint32_t M,
-                                                         uint32_t* __restrict__ pre) {
+__global__ void __launch_bounds__(INV_T, 2) k_inv_wide(uint32_t* __restrict__ v, uint32_t M, uint32_t G,
+                                                       uint32_t* __restrict__ pre) {
     constexpr int N = F::N;
-    constexpr int NW = INV_ROOT_T / 32;
-    constexpr uint32_t T = INV_ROOT_T;
+    constexpr int NW = INV_T / 32;
     __shared__ uint32_t s_wt[NW * N];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const size_t TT = (size_t)gridDim.x * INV_T;
+    const size_t gt = (size_t)blockIdx.x * INV_T + (size_t)t;
+    const size_t base = (size_t)blockIdx.x * INV_T * G + (size_t)t;
     Fe<F> run, x;
     fe_one(run);
     uint32_t cnt = 0;
-    for (uint32_t e = (uint32_t)t; cnt < (uint32_t)INV_G && e < M; ++cnt, e += T) {
-        if (cnt) fe_store_wm(pre + (size_t)(cnt - 1) * N * T, T, (size_t)t, run);
+    for (size_t e = base; cnt < G && e < M; ++cnt, e += INV_T) {
+        if (cnt) fe_store_wm(pre + (size_t)(cnt - 1) * N * TT, TT, gt, run);
         fe_load_wm(x, v, M, e);
         fe_mul(run, run, x);
     }
@@ -747,7 +710,7 @@ __global__ void __launch_bounds__(INV_ROOT_T) k_inv_root(uint32_t* __restrict__ 
         if (lane == 0) fe_inv(inv, tot);
 #pragma unroll
         for (int q = 0; q < N; ++q) inv.v[q] = __shfl_sync(0xffffffffu, inv.v[q], 0);
-        warp_exclude_self(inv, P2, S2, lane);  // 1 / (warp lane's total)
+        warp_exclude_self(inv, P2, S2, lane);  // 1 / (warp lane's product)
         __syncwarp();
         if (lane < NW) fe_store(s_wt + lane * N, inv);
     }
@@ -756,15 +719,15 @@ __global__ void __launch_bounds__(INV_ROOT_T) k_inv_root(uint32_t* __restrict__ 
     fe_load(r, s_wt + warp * N);
     warp_exclude_self(r, P, S, lane);  // 1 / run
     for (int j = (int)cnt - 1; j > 0; --j) {
-        const uint32_t e = (uint32_t)t + (uint32_t)j * T;
+        const size_t e = base + (size_t)j * INV_T;
         Fe<F> p;
         fe_load_wm(x, v, M, e);
-        fe_load_wm(p, pre + (size_t)(j - 1) * N * T, T, (size_t)t);
+        fe_load_wm(p, pre + (size_t)(j - 1) * N * TT, TT, gt);
         fe_mul(p, p, r);  // 1 / x_j
         fe_mul(r, r, x);
         fe_store_wm(v, M, e, p);
     }
-    if (cnt) fe_store_wm(v, M, (size_t)t, r);
+    if (cnt) fe_store_wm(v, M, base, r);
 }
 
 // Fold level l >= 2: the level's (big bucket, group) items are flattened by
@@ -1263,35 +1226,9 @@ struct MsmLaunchImpl {
         uint32_t* tot = pre0 + (size_t)(PAIR_J - 1) * N * T0;
         k_pair_fwd<C><<<ceil_div_u(T0, 256), 256, 0, st>>>(a, T0, pre0, tot);
         KB_LAUNCH_CHECK();
-        uint32_t* lv_v[16];
-        uint32_t* lv_pre[16];
-        uint32_t lv_M[16];
-        int R = 0;
-        uint32_t* cur = tot;
-        uint32_t M = T0;
-        uint32_t* next = tot + (size_t)N * T0;
-        while (M > (uint32_t)INV_ROOT) {  // M shrinks 16x per level: at most 6 levels
-            const uint32_t T = (M + INV_G - 1) / INV_G;
-            uint32_t* pre = next;
-            uint32_t* out = pre + (size_t)(INV_G - 1) * N * T;
-            next = out + (size_t)N * T;
-            k_inv_fwd<F><<<ceil_div_u(T, 256), 256, 0, st>>>(cur, M, T, pre, out);
-            KB_LAUNCH_CHECK();
-            lv_v[R] = cur;
-            lv_pre[R] = pre;
-            lv_M[R] = M;
-            ++R;
-            cur = out;
-            M = T;
-        }
-        k_inv_root<F><<<1, INV_ROOT_T, 0, st>>>(cur, M, next);  // next: INV_G N INV_ROOT_T words
+        const InvGeom g = inv_geom(T0);
+        k_inv_wide<F><<<g.nb, INV_T, 0, st>>>(tot, T0, g.G, tot + (size_t)N * T0);
         KB_LAUNCH_CHECK();
-        for (int r = R - 1; r >= 0; --r) {
-            const uint32_t T = (lv_M[r] + INV_G - 1) / INV_G;
-            k_inv_bwd<F><<<ceil_div_u(T, 256), 256, 0, st>>>(lv_v[r], lv_M[r], T, lv_pre[r],
-                                                            r + 1 < R ? lv_v[r + 1] : cur);
-            KB_LAUNCH_CHECK();
-        }
         if (a.dst_off)
             k_pair_bwd<C, true><<<ceil_div_u(T0, 256), 256, 0, st>>>(a, T0, pre0, tot);
         else
