@@ -560,7 +560,7 @@ def run_ours(args, ws, rank, local):
     sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
     peak_imad = SM_COUNT * IMAD_PER_CLK_SM * sm_mhz * 1e6
     # dominant phase: the bucket accumulation, i.e. the batch-affine pairing
-    # levels (k_pair_fwd, k_inv_*, k_pair_bwd) and the XYZZ accumulation of
+    # levels (k_pair_fwd, k_inv_wide, k_pair_bwd) and the XYZZ accumulation of
     # what they leave (k_accumulate), timed by the stage events around both
     plan_c = kb.msm_window(CURVE, n)
     entries = kb.lib().kb200_msm_entries(CURVE, n)
@@ -570,7 +570,7 @@ def run_ours(args, ws, rank, local):
     if acc_ms and acc_ms > 0:
         ach = acc_imad / (acc_ms / 1e3)
         roofline = {"bound": "int",
-                    "kernel": "bucket accumulation: pairing levels (k_pair_fwd, k_inv_*, k_pair_bwd) "
+                    "kernel": "bucket accumulation: pairing levels (k_pair_fwd, k_inv_wide, k_pair_bwd) "
                               "+ k_accumulate",
                     "achieved": ach / 1e12,
                     "peak": peak_imad / 1e12, "unit": "TIMAD/s", "frac": ach / peak_imad,

@@ -387,14 +387,18 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
     P.L = L;
     P.B = (uint32_t)B;
     P.total_scalars = tot_sc;
-    // Reduction granularity: buckets per thread S (any integer) so that
-    // stage 1 fills one wave of two resident 256-thread blocks per SM as
-    // evenly as the bucket count allows, up to 64 buckets per thread (past
-    // that, more waves of shorter serial chains run faster: BN254 at 2^24),
-    // and every window has at most RED_THREADS stage-1 blocks.
-    const size_t per_wave = (size_t)2 * device_sms() * RED_THREADS;
-    const uint32_t S0 = (uint32_t)std::min<size_t>(
-        64, std::max<size_t>(1, (total_live + per_wave - 1) / per_wave));
+    // Reduction granularity: buckets per thread S (any integer).  A stage-1
+    // block costs 2S serial additions plus a fixed 24 levels of scan and
+    // trees, so S is the smallest that gives about one 256-thread block per
+    // SM; when that is under 4 buckets per thread (few buckets), two blocks
+    // per SM instead.  At most 64 buckets per thread, and every window has
+    // at most RED_THREADS stage-1 blocks.  Measured stage-1 times, one block
+    // per SM against two: BLS12-381 2^22 (273 K buckets) 1.43 / 1.75 ms,
+    // BN254 2^24 1.43 / 1.53 ms; 2^18 (41 K buckets) 1.15 / 0.99 ms.
+    const size_t per_sm = (size_t)device_sms() * RED_THREADS;
+    size_t s_one = (total_live + per_sm - 1) / per_sm;
+    if (s_one < 4) s_one = (total_live + 2 * per_sm - 1) / (2 * per_sm);
+    const uint32_t S0 = (uint32_t)std::min<size_t>(64, std::max<size_t>(1, s_one));
     // Few buckets (KZG commits up to 2^16, blobs): the reduction is bound by
     // the latency of its serial additions, not by throughput, so it runs one
     // quad of lanes per slot with the quad addition (k_reduce_blocks_quad),

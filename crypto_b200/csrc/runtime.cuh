@@ -51,8 +51,24 @@ void set_last_error(const std::string& msg);
 bool alloc_trace_enabled();
 void alloc_trace(size_t from, size_t to, double ms);
 
+// Deferred frees for a thread that owns every stream its buffers are used
+// on (the commit server's worker): a buffer that grows on such a thread keeps
+// its old allocation in a per-thread list instead of freeing it, because
+// cudaFree waits for the whole device (another slot's batch included); the
+// thread frees the list with devbuf_free_retired() once its streams are idle.
+inline thread_local bool t_devbuf_defer = false;
+inline thread_local std::vector<void*> t_devbuf_retired;
+inline void devbuf_defer_frees(bool on) { t_devbuf_defer = on; }
+inline bool devbuf_have_retired() { return !t_devbuf_retired.empty(); }
+inline void devbuf_free_retired() {
+    for (void* p : t_devbuf_retired) cudaFree(p);
+    t_devbuf_retired.clear();
+}
+
 // A grow-only device buffer.  Growing synchronises the owning stream first,
-// because the old allocation may still be read by queued work.
+// because the old allocation may still be read by queued work (or, on a
+// thread with deferred frees, keeps the old allocation until that thread's
+// streams are idle).
 struct DevBuf {
     void* ptr = nullptr;
     size_t bytes = 0;
@@ -62,8 +78,12 @@ struct DevBuf {
         const auto t0 = std::chrono::steady_clock::now();
         const size_t from = bytes;
         if (ptr) {
-            KB_CUDA(cudaStreamSynchronize(stream));
-            KB_CUDA(cudaFree(ptr));
+            if (t_devbuf_defer) {
+                t_devbuf_retired.push_back(ptr);
+            } else {
+                KB_CUDA(cudaStreamSynchronize(stream));
+                KB_CUDA(cudaFree(ptr));
+            }
             ptr = nullptr;
             bytes = 0;
         }

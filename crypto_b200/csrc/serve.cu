@@ -255,6 +255,9 @@ bool KzgServer::launch_batch(Slot& s) {
 }
 
 void KzgServer::loop() {
+    // Buffers that grow under load keep their old allocations until both
+    // slots are idle (a free would wait for the other slot's batch).
+    devbuf_defer_frees(true);
     try {
         KB_CUDA(cudaSetDevice(device));
         while (!stop.load()) {
@@ -274,6 +277,9 @@ void KzgServer::loop() {
                 if (!s.busy && launch_batch(s)) progressed = true;
             }
             if (!progressed) {
+                bool idle = true;
+                for (Slot& s : slots) idle &= !s.busy;
+                if (idle && devbuf_have_retired()) devbuf_free_retired();
                 std::unique_lock<std::mutex> lk(mu);
                 bool any_busy = false;
                 for (Slot& s : slots) any_busy |= s.busy;
@@ -291,6 +297,8 @@ void KzgServer::loop() {
             if (kv.second->status == 1) kv.second->status = KB200_CRYPTO_ERR_BACKEND;
         cv_done.notify_all();
     }
+    for (Slot& s : slots) cudaStreamSynchronize(s.stream);
+    devbuf_free_retired();
 }
 
 }  // namespace kb200
