@@ -54,15 +54,24 @@ void alloc_trace(size_t from, size_t to, double ms);
 // Deferred frees for a thread that owns every stream its buffers are used
 // on (the commit server's worker): a buffer that grows on such a thread keeps
 // its old allocation in a per-thread list instead of freeing it, because
-// cudaFree waits for the whole device (another slot's batch included); the
-// thread frees the list with devbuf_free_retired() once its streams are idle.
+// cudaFree waits for the whole device (another slot's batch included) and,
+// measured under load, sometimes for hundreds of milliseconds more.  The
+// thread frees the list with devbuf_free_retired() once its streams are idle
+// and the list holds more than a set number of bytes, and when it exits.
 inline thread_local bool t_devbuf_defer = false;
 inline thread_local std::vector<void*> t_devbuf_retired;
+inline thread_local size_t t_devbuf_retired_bytes = 0;
 inline void devbuf_defer_frees(bool on) { t_devbuf_defer = on; }
-inline bool devbuf_have_retired() { return !t_devbuf_retired.empty(); }
+inline size_t devbuf_retired_bytes() { return t_devbuf_retired_bytes; }
 inline void devbuf_free_retired() {
+    const auto t0 = std::chrono::steady_clock::now();
     for (void* p : t_devbuf_retired) cudaFree(p);
+    if (alloc_trace_enabled() && !t_devbuf_retired.empty())
+        std::fprintf(stderr, "[devbuf] freed %zu retired buffers (%zu bytes), %.3f ms\n",
+                     t_devbuf_retired.size(), t_devbuf_retired_bytes,
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
     t_devbuf_retired.clear();
+    t_devbuf_retired_bytes = 0;
 }
 
 // A grow-only device buffer.  Growing synchronises the owning stream first,
@@ -80,6 +89,7 @@ struct DevBuf {
         if (ptr) {
             if (t_devbuf_defer) {
                 t_devbuf_retired.push_back(ptr);
+                t_devbuf_retired_bytes += bytes;
             } else {
                 KB_CUDA(cudaStreamSynchronize(stream));
                 KB_CUDA(cudaFree(ptr));

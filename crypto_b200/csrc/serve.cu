@@ -255,8 +255,9 @@ bool KzgServer::launch_batch(Slot& s) {
 }
 
 void KzgServer::loop() {
-    // Buffers that grow under load keep their old allocations until both
-    // slots are idle (a free would wait for the other slot's batch).
+    // Buffers that grow under load keep their old allocations (a free waits
+    // for the other slot's batch, and at times far longer); they are freed
+    // while both slots are idle once they pass 1 GiB, and at exit.
     devbuf_defer_frees(true);
     try {
         KB_CUDA(cudaSetDevice(device));
@@ -279,7 +280,7 @@ void KzgServer::loop() {
             if (!progressed) {
                 bool idle = true;
                 for (Slot& s : slots) idle &= !s.busy;
-                if (idle && devbuf_have_retired()) devbuf_free_retired();
+                if (idle && devbuf_retired_bytes() > ((size_t)1 << 30)) devbuf_free_retired();
                 std::unique_lock<std::mutex> lk(mu);
                 bool any_busy = false;
                 for (Slot& s : slots) any_busy |= s.busy;
