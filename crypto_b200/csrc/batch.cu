@@ -41,6 +41,7 @@ struct Prepared {
     DevBuf d_vec_off;                                // element offsets grouped by class
     size_t total = 0;                                // evaluations
     cudaGraphExec_t graph = nullptr;
+    unsigned long long graph_moves = 0;  // devbuf_moves() when the graph was captured
     ~Prepared() {
         if (graph) cudaGraphExecDestroy(graph);
         for (MsmGroup& g : groups) msm_batch_plan_destroy(g.plan);
@@ -220,6 +221,12 @@ static void run(CommitBatcher* B, Prepared* P, const uint32_t* srs, cudaStream_t
         enqueue(B, P, srs, st);
         return;
     }
+    if (P->graph && P->graph_moves != devbuf_moves()) {
+        // a buffer the graph addresses may have moved since the capture
+        // (another batch shape grew the engine): capture again
+        cudaGraphExecDestroy(P->graph);
+        P->graph = nullptr;
+    }
     if (!P->graph) {
         cudaGraph_t g = nullptr;
         KB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -234,6 +241,7 @@ static void run(CommitBatcher* B, Prepared* P, const uint32_t* srs, cudaStream_t
         const cudaError_t err = cudaGraphInstantiate(&P->graph, g, 0);
         cudaGraphDestroy(g);
         KB_CUDA(err);
+        P->graph_moves = devbuf_moves();
         ++B->graph_captures;
     }
     KB_CUDA(cudaGraphLaunch(P->graph, st));

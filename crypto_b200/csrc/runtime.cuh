@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <chrono>
 #include <cstddef>
 #include <cstdint>
@@ -74,6 +75,13 @@ inline void devbuf_free_retired() {
     t_devbuf_retired_bytes = 0;
 }
 
+// Process-wide count of device allocations replaced or released by DevBuf.
+// Work captured into a CUDA graph holds raw device addresses; a graph
+// captured when this count had another value may name freed memory and must
+// be captured again.
+inline std::atomic<unsigned long long> g_devbuf_moves{0};
+inline unsigned long long devbuf_moves() { return g_devbuf_moves.load(std::memory_order_acquire); }
+
 // A grow-only device buffer.  Growing synchronises the owning stream first,
 // because the old allocation may still be read by queued work (or, on a
 // thread with deferred frees, keeps the old allocation until that thread's
@@ -94,6 +102,7 @@ struct DevBuf {
                 KB_CUDA(cudaStreamSynchronize(stream));
                 KB_CUDA(cudaFree(ptr));
             }
+            g_devbuf_moves.fetch_add(1, std::memory_order_acq_rel);
             ptr = nullptr;
             bytes = 0;
         }
@@ -109,7 +118,10 @@ struct DevBuf {
         return static_cast<T*>(ptr);
     }
     void release() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) {
+            cudaFree(ptr);
+            g_devbuf_moves.fetch_add(1, std::memory_order_acq_rel);
+        }
         ptr = nullptr;
         bytes = 0;
     }

@@ -69,6 +69,24 @@ def test_batch_equals_single(cuda_lib):
         assert kb().kzg_commit(e) == c
 
 
+def test_batch_graph_after_engine_growth(cuda_lib):
+    """A batch shape is captured into a CUDA graph on first use; a later,
+    larger shape grows the shared engine and batch buffers, so replaying the
+    first shape must not reuse addresses from before the growth."""
+    rng = random.Random(21)
+    tau = rng.randrange(O.FR[2])
+    kb().kzg_srs_generate(tau.to_bytes(32, "little"), 1 << 16)
+    small = [256, 1024, 256]
+    large = [1 << 16] * 4 + [1 << 12]
+    ev_s = [kb().gen_scalars(2, 900 + i, s) for i, s in enumerate(small)]
+    ev_l = [kb().gen_scalars(2, 950 + i, s) for i, s in enumerate(large)]
+    want_s = [kb().kzg_commit(e) for e in ev_s]
+    want_l = [kb().kzg_commit(e) for e in ev_l]
+    for shape, evs, want in [(small, ev_s, want_s), (large, ev_l, want_l), (small, ev_s, want_s),
+                             (large, ev_l, want_l), (small, ev_s, want_s)]:
+        assert kb().kzg_commit_batch(b"".join(evs), shape) == want
+
+
 def test_commit_errors(cuda_lib):
     import ctypes
     L = kb().lib()
