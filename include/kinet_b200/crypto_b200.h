@@ -150,7 +150,10 @@ int ntt_fr_inverse(int curve, uint8_t* coeffs32le, size_t n, int coset);
 
 /* Load n monomial-basis SRS points [tau^i]G1 (96 B BE each) into device
  * memory, replacing any resident SRS.  The reference loads its setup once
- * per process (kzg/cpp/kzg_blob.cpp:23-65); this is the resident analogue. */
+ * per process (kzg/cpp/kzg_blob.cpp:23-65); this is the resident analogue.
+ * Both SRS calls also build the shifted tables commits select and size the
+ * per-call commit buffers (one commit of zeros per power of two up to n), so
+ * later kzg_commit_fr calls allocate nothing. */
 int kzg_srs_load_g1(const uint8_t* points96be, size_t n);
 /* Build the synthetic SRS [tau^i]G1, i < n, on the device from a 32-byte LE
  * tau (reduced mod r).  For tests and benchmarks. */
