@@ -393,7 +393,7 @@ static void commit_on_device(DeviceCtx* c, uint32_t* d_evals, size_t n, uint8_t*
 // up to srs_n evaluations selects, and run one commit of zeros per power of
 // two, so the per-call engines reach their working size here.  Without it the
 // first commit of each size class paid for its table build and for engine
-// growth (allocations that took up to ~90 ms on this pool), which set
+// growth (single allocations took up to ~90 ms on a B200), which set
 // per-call throughput anywhere from 280 to 990 commits/s between runs.
 static void srs_prepare_commits(DeviceCtx* c, cudaStream_t st) {
     const size_t n = c->srs_n;
