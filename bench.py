@@ -35,6 +35,30 @@ PB = 96
 N_LIMBS = 12
 SM_COUNT = 148
 IMAD_PER_CLK_SM = 64
+# The headline workload's seeds: scalars s_i from stream 1, points k_i * G1
+# with k_i from stream 1001 (uniform Fr, xorshift64* with rejection).
+SCALAR_SEED = 1
+POINT_SEED = 1001
+# One step of the reference arm: a 2^20-point quarter of the 2^22 workload.
+REF_BLOCK_LOG = 20
+GOLDEN_LARGE = ROOT / "tests" / "golden" / "large.json"
+
+
+def headline_config(logn: int) -> dict:
+    """The workload both arms time (identical in both JSON lines)."""
+    return {"workload": f"BLS12-381 G1 MSM n=2^{logn}: sum of s_i * P_i, s_i uniform Fr "
+                        f"(seed {SCALAR_SEED}), P_i = k_i * G1 with k_i uniform Fr (seed {POINT_SEED})",
+            "curve": "BLS12-381", "n": 1 << logn}
+
+
+def golden_expected(label: str):
+    """Expected result bytes (hex) of a full-size golden case, or None."""
+    if not GOLDEN_LARGE.exists():
+        return None
+    for c in json.loads(GOLDEN_LARGE.read_text())["msm"]:
+        if c["label"] == label:
+            return c["expected"]
+    return None
 
 
 def mont_imad(nlimbs: int) -> int:
@@ -162,19 +186,46 @@ def max_over_ranks(ws, v: float) -> float:
     return float(t.item())
 
 
-def cpu_reference_msm(pts: bytes, scs: bytes, n: int, threads: int) -> float:
-    """Seconds for the reference CPU MSM (composed over `threads` slices)."""
-    sys.path.insert(0, str(ROOT / "tests"))
+def ref_threads() -> int:
+    """Host threads for the reference CPU MSM: all cores, at most 16, so each
+    slice of a 2^20-point step keeps >= 2^16 points and the reference picks
+    the 12-bit window it uses for the whole 2^22 call."""
+    return max(1, min(os.cpu_count() or 1, 16))
+
+
+def cpu_workload(n: int):
+    """The headline workload built on the CPU by the oracle's restated input
+    generators (no GPU and no CUDA library involved)."""
     import _oracle as O
+    scs = O.gen_scalars(CURVE, SCALAR_SEED, n)
+    pts = O.fixed_base_points(CURVE, O.gen_scalars(CURVE, POINT_SEED, n))
+    return scs, pts
+
+
+def ref_block(scs: bytes, pts: bytes, n: int, block: int, threads: int):
+    """The reference's own gpukit_multi_pippenger_cpu on one 2^REF_BLOCK_LOG
+    block of the workload, split into `threads` contiguous slices run in
+    parallel and summed with the reference g1_add.  Returns (seconds, sum)."""
+    import _oracle as O
+    m = min(n, 1 << REF_BLOCK_LOG)
+    lo = (block * m) % n
     out = ctypes.create_string_buffer(PB)
     t0 = time.perf_counter()
-    if threads <= 1:
-        rc = O.ref().ref_msm(CURVE, scs, pts, n, out)
-    else:
-        rc = O.ref().ref_msm_parallel(CURVE, scs, pts, n, out, threads)
+    rc = O.ref().ref_msm_parallel(CURVE, scs[32 * lo:32 * (lo + m)], pts[PB * lo:PB * (lo + m)], m,
+                                  out, threads)
     dt = time.perf_counter() - t0
-    assert rc == 0
-    return dt
+    assert rc == 0, rc
+    return dt, out.raw
+
+
+def ref_sample_text(n: int, threads: int) -> str:
+    m = min(n, 1 << REF_BLOCK_LOG)
+    return (f"each step: the reference gpukit_multi_pippenger_cpu (built unmodified from its sources) on "
+            f"one 2^{m.bit_length() - 1}-point block of the 2^{n.bit_length() - 1} workload (blocks in turn), "
+            f"split into {threads} contiguous slices of {m // threads} points on {threads} threads and "
+            f"summed with the reference g1_add; the slices use the 12-bit window the reference "
+            f"picks for the whole call (its bucket overhead per point is 2^12/{m // threads} against "
+            f"2^12/2^{n.bit_length() - 1})")
 
 
 def make_inputs(n: int, seed: int):
@@ -182,7 +233,7 @@ def make_inputs(n: int, seed: int):
     import torch
     import crypto_b200 as kb
     sc = kb.gen_scalars(CURVE, seed, n)
-    ks = kb.gen_scalars(CURVE, seed + 1000, n)
+    ks = kb.gen_scalars(CURVE, seed + POINT_SEED - SCALAR_SEED, n)
     d_sc = torch.frombuffer(bytearray(sc), dtype=torch.uint8).cuda()
     d_ks = torch.frombuffer(bytearray(ks), dtype=torch.uint8).cuda()
     d_pts = torch.empty(n * PB, dtype=torch.uint8, device="cuda")
@@ -466,140 +517,269 @@ def bench_served_commits(args) -> dict:
 
 
 def run_reference(args, ws, rank):
-    n_sample = 1 << args.ref_logn
-    threads = os.cpu_count() or 1
+    """The reference arm: the reference's own CPU MSM on the headline
+    workload, built and run on the host (rank 0 only; other ranks exit
+    without work).  Never loads the CUDA library."""
     if rank != 0:
         return
-    import crypto_b200 as kb
-    d_sc, d_pts = make_inputs(n_sample, seed=1)
-    pts = d_pts.cpu().numpy().tobytes()
-    scs = d_sc.cpu().numpy().tobytes()
-    for _ in range(args.warmup and 1):
-        cpu_reference_msm(pts, scs, n_sample, threads)
-    times = [cpu_reference_msm(pts, scs, n_sample, threads) for _ in range(args.steps)]
+    import _oracle as O
+    n = 1 << args.logn
+    threads = ref_threads()
+    scs, pts = cpu_workload(n)
+    nblocks = max(1, n >> REF_BLOCK_LOG)
+    for i in range(args.warmup):
+        ref_block(scs, pts, n, i, threads)
+    times, sums = [], {}
+    for i in range(args.steps):
+        dt, r = ref_block(scs, pts, n, args.warmup + i, threads)
+        times.append(dt)
+        sums[(args.warmup + i) % nblocks] = r
     t = sum(times) / len(times)
-    v = n_sample / t / 1e6
+    m = min(n, 1 << REF_BLOCK_LOG)
+    v = m / t / 1e6
+    check = None
+    want = golden_expected(f"msm_bls12_381_2^{args.logn}")
+    if want and len(sums) == nblocks:
+        acc = bytes(PB)
+        for b in range(nblocks):
+            acc = O.g1_add(CURVE, acc, sums[b])
+        check = acc.hex() == want
     line = {
         "impl": "reference", "metric": "G1 MSM Mpts/s @2^22", "value": v, "unit": "Mpts/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"BLS12-381 G1 MSM, bounded sample n=2^{args.ref_logn} of the "
-                               "2^22 workload (uniform Fr scalars, seeded points)",
-                   "curve": "BLS12-381", "n": n_sample},
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": headline_config(args.logn),
         "cpu_baseline": {"value": v, "unit": "Mpts/s", "cores": threads, "kind": "reference",
-                         "sample": f"gpukit_multi_pippenger_cpu on {threads} contiguous slices of "
-                                   f"n=2^{args.ref_logn}, slice results summed with the reference g1_add"},
+                         "sample": ref_sample_text(n, threads)},
         "e2e": {"value": v, "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "block_sums_match_golden": check,
     }
     print(json.dumps(line), flush=True)
+
+
+def cpu_baselines(args) -> dict:
+    """The CPU baselines of the other configurations, timed on this host:
+    the restated Fr NTT (the reference has none), the plain KZG commit
+    (restated iNTT -> the reference MSM -> restated encoder), and the batched
+    and served commit mixes spread over all host cores.  Each is a bounded
+    sample, said in its entry."""
+    import random
+    import concurrent.futures as cf
+    import _oracle as O
+    cores = ref_threads()
+    out = {}
+    # Fr NTT 2^24 forward, BLS12-381 (restated radix-2, one core)
+    n = 1 << 24
+    x = O.gen_scalars(CURVE, 5 + 24, n)
+    buf = ctypes.create_string_buffer(x, len(x))
+    t0 = time.perf_counter()
+    assert O.orc().orc_ntt(CURVE, buf, n, 0, 0) == 0
+    t = time.perf_counter() - t0
+    out["fr_ntt_bls12_381_2^24"] = {"ms_forward": t * 1e3, "cores": 1, "kind": "port",
+                                    "sample": "one forward transform (oracle orc_ntt, radix-2 restatement)"}
+    del buf, x
+
+    # KZG commit kernels shared by the commit baselines: SRS [tau^i]G1
+    tau = bytes(O.gen_scalars(CURVE, 7, 1))
+    srs = O.fixed_base_points(CURVE, O.fr_powers(CURVE, tau, 1 << 16))
+
+    def commit(ev: bytes) -> bytes:
+        m = len(ev) // 32
+        coeffs = O.ntt(CURVE, ev, inverse=True)
+        return O.compress(O.ref_msm(CURVE, coeffs, srs[:96 * m], m))
+
+    ev = O.gen_scalars(CURVE, 4096, 4096)
+    commit(ev)
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        commit(ev)
+    t = (time.perf_counter() - t0) / reps
+    out["kzg_commit_4096"] = {"ms": t * 1e3, "commits_per_s": 1 / t, "cores": 1, "kind": "reference",
+                              "sample": "restated iNTT -> reference gpukit_multi_pippenger_cpu -> restated "
+                                        "compressed encoder, one commit of 4096 evaluations, 3 repetitions"}
+
+    # 512 uneven commits (2^8..2^16): every 8th commit of the benchmark's size
+    # list, spread over all cores (ctypes calls release the GIL)
+    rng = random.Random(4096)
+    sizes = [1 << rng.randint(8, 16) for _ in range(args.commits)][::8]
+    evs = [O.gen_scalars(CURVE, 100000 + 8 * i, m) for i, m in enumerate(sizes)]
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(cores) as ex:
+        list(ex.map(commit, evs))
+    t = time.perf_counter() - t0
+    out["kzg_batched_uneven"] = {"commits_per_s": len(sizes) / t, "cores": cores, "kind": "reference",
+                                 "sample": f"{len(sizes)} of the 512 commits (every 8th of the same size "
+                                           f"list), one commit per core at a time"}
+
+    # served mix (70% 4096, 25% 2^16, 5% 2^20): service time per class
+    lat = {}
+    for m in (4096, 1 << 16):
+        e = O.gen_scalars(CURVE, 200000 + m, m)
+        t0 = time.perf_counter()
+        commit(e)
+        lat[m] = time.perf_counter() - t0
+    m = 1 << 20
+    big_srs = O.fixed_base_points(CURVE, O.fr_powers(CURVE, tau, m))
+    e = O.gen_scalars(CURVE, 200000 + m, m)
+    t0 = time.perf_counter()
+    coeffs = O.ntt(CURVE, e, inverse=True)
+    O.compress(O.ref_msm(CURVE, coeffs, big_srs, m, threads=cores))
+    t_big = time.perf_counter() - t0
+    mean_1core = 0.70 * lat[4096] + 0.25 * lat[1 << 16] + 0.05 * t_big * cores
+    out["kzg_served_mix"] = {
+        "service_ms": {"4096 (1 core)": lat[4096] * 1e3, "65536 (1 core)": lat[1 << 16] * 1e3,
+                       f"1048576 ({cores} cores)": t_big * 1e3},
+        "commits_per_s_all_cores": cores / mean_1core, "cores": cores, "kind": "reference",
+        "sample": "one commit per size class; the mix's throughput on all cores is derived as "
+                  "cores / mean single-core service time, the 2^20 class counted as its all-core "
+                  "time x cores"}
+    return out
 
 
 def run_ours(args, ws, rank, local):
     import torch
     import crypto_b200 as kb
     n = 1 << args.logn
-    d_sc, d_pts = make_inputs(n, seed=1 + rank)
+    d_sc, d_pts = make_inputs(n, seed=SCALAR_SEED + rank)
     d_out = torch.empty(PB, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
     sp = ctypes.c_void_p(stream.cuda_stream)
     L = kb.lib()
+    # The drop-in path (exact for every curve point: 256-bit windows on
+    # BLS12-381) and the G1-promise path (GLV split), both on device buffers.
+    dev_fn = {"plain": L.kb200_msm_device, "subgroup": L.kb200_msm_device_subgroup}
+    host_fn = {"plain": L.gpukit_multi_pippenger, "subgroup": L.gpukit_multi_pippenger_subgroup}
+    head = args.path
+    other = "subgroup" if head == "plain" else "plain"
 
-    def step():
-        rc = L.kb200_msm_device(CURVE, d_sc.data_ptr(), d_pts.data_ptr(), n, d_out.data_ptr(), sp)
+    def run(path):
+        rc = dev_fn[path](CURVE, d_sc.data_ptr(), d_pts.data_ptr(), n, d_out.data_ptr(), sp)
         assert rc == 0, kb.last_error()
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    # correctness spot check of the device path against the C ABI drop-in
+    # warm-up of both paths; their sums against the reference's (the golden
+    # sum of the same workload from the reference CPU MSM) and each other
+    want = golden_expected(f"msm_bls12_381_2^{args.logn}") if rank == 0 else None
+    sums = {}
+    for path in (other, head):
+        for _ in range(args.warmup):
+            run(path)
+        torch.cuda.synchronize()
+        sums[path] = d_out.cpu().numpy().tobytes()
+    assert sums["plain"] == sums["subgroup"], "the two MSM paths disagree"
+    parity = {"reference_sum_equal": (sums[head].hex() == want) if want else None,
+              "against": "reference CPU MSM of this workload (tests/golden/large.json)"}
+    if want:
+        assert sums[head].hex() == want, "MSM differs from the reference's sum"
     host_sc = d_sc.cpu().numpy().tobytes()
     host_pts = d_pts.cpu().numpy().tobytes()
-    want = kb.gpukit_multi_pippenger(CURVE, host_sc, host_pts, n)
-    assert d_out.cpu().numpy().tobytes() == want, "device path differs from C ABI path"
 
-    kb.profile_enable(True)
-    barrier(ws)
-    torch.cuda.synchronize()
-    launches0 = kb.launch_count()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(torch.cuda.current_device()) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            step()
-        ev1.record(stream)
+    def timed(path, steps, sample_clocks):
+        kb.profile_enable(True)
+        barrier(ws)
         torch.cuda.synchronize()
-    launches = kb.launch_count() - launches0
-    barrier(ws)
-    stage = kb.msm_stage_ms(CURVE)
-    kb.profile_enable(False)
-    ms = ev0.elapsed_time(ev1) / args.steps
-    ms = max_over_ranks(ws, ms)
+        launches0 = kb.launch_count()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        clk = ClockSampler(torch.cuda.current_device()) if sample_clocks else None
+        if clk:
+            clk.__enter__()
+        try:
+            ev0.record(stream)
+            for _ in range(steps):
+                run(path)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        finally:
+            if clk:
+                clk.__exit__()
+        launches = kb.launch_count() - launches0
+        barrier(ws)
+        stage = kb.msm_stage_ms(CURVE)
+        kb.profile_enable(False)
+        ms = max_over_ranks(ws, ev0.elapsed_time(ev1) / steps)
+        return ms, launches, stage, (clk.summary() if clk else None)
+
+    ms, launches, stage, clocks = timed(head, args.steps, True)
     value = n * ws / (ms / 1e3) / 1e6
 
-    # e2e through the drop-in C ABI with pinned host buffers
+    # e2e through the C ABI with pinned host buffers (copies in the timed region)
     h_sc = torch.frombuffer(bytearray(host_sc), dtype=torch.uint8).pin_memory()
     h_pts = torch.frombuffer(bytearray(host_pts), dtype=torch.uint8).pin_memory()
     out = ctypes.create_string_buffer(PB)
-    e2e_steps = max(1, min(args.steps, 5))
-    L.gpukit_multi_pippenger(CURVE, ctypes.c_char_p(h_sc.data_ptr()),
-                             ctypes.c_char_p(h_pts.data_ptr()), n, out)
-    barrier(ws)
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        rc = L.gpukit_multi_pippenger(CURVE, ctypes.c_char_p(h_sc.data_ptr()),
-                                      ctypes.c_char_p(h_pts.data_ptr()), n, out)
-        assert rc == 0, kb.last_error()
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
-    e2e_ms = max_over_ranks(ws, e2e_ms)
-    assert out.raw == want
+
+    def e2e(path):
+        f = host_fn[path]
+        steps = max(1, min(args.steps, 5))
+        assert f(CURVE, ctypes.c_char_p(h_sc.data_ptr()), ctypes.c_char_p(h_pts.data_ptr()), n, out) == 0
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            rc = f(CURVE, ctypes.c_char_p(h_sc.data_ptr()), ctypes.c_char_p(h_pts.data_ptr()), n, out)
+            assert rc == 0, kb.last_error()
+        e_ms = max_over_ranks(ws, (time.perf_counter() - t0) * 1e3 / steps)
+        assert out.raw == sums[path]
+        return e_ms
+
+    e2e_ms = e2e(head)
 
     peaks = load_peaks()
-    clocks = clk.summary()
     sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
     peak_imad = SM_COUNT * IMAD_PER_CLK_SM * sm_mhz * 1e6
-    # dominant phase: the bucket accumulation, i.e. the batch-affine pairing
-    # levels (k_pair_fwd, k_inv_wide, k_pair_bwd) and the XYZZ accumulation of
-    # what they leave (k_accumulate), timed by the stage events around both
-    plan_c = kb.msm_window(CURVE, n)
-    entries = kb.lib().kb200_msm_entries(CURVE, n)
-    acc_ms = (stage.get("pair") or 0.0) + (stage.get("accumulate") or 0.0)
-    acc_imad = entries * 6 * mont_imad(N_LIMBS)
-    roofline = None
-    if acc_ms and acc_ms > 0:
-        ach = acc_imad / (acc_ms / 1e3)
-        roofline = {"bound": "int",
+
+    def rooflines(path, stage_ms, step_ms):
+        # dominant phase: the bucket accumulation, i.e. the batch-affine pairing
+        # levels (k_pair_fwd, k_inv_wide, k_pair_bwd) and the XYZZ accumulation of
+        # what they leave (k_accumulate), timed by the stage events around both
+        entries = (L.kb200_msm_entries_subgroup if path == "subgroup" else L.kb200_msm_entries)(CURVE, n)
+        acc_ms = (stage_ms.get("pair") or 0.0) + (stage_ms.get("accumulate") or 0.0)
+        roof = None
+        if acc_ms > 0:
+            ach = entries * 6 * mont_imad(N_LIMBS) / (acc_ms / 1e3)
+            roof = {"bound": "int",
                     "kernel": "bucket accumulation: pairing levels (k_pair_fwd, k_inv_wide, k_pair_bwd) "
                               "+ k_accumulate",
-                    "achieved": ach / 1e12,
-                    "peak": peak_imad / 1e12, "unit": "TIMAD/s", "frac": ach / peak_imad,
-                    "traffic": bucket_traffic(entries),
+                    "achieved": ach / 1e12, "peak": peak_imad / 1e12, "unit": "TIMAD/s",
+                    "frac": ach / peak_imad, "traffic": bucket_traffic(path, entries),
                     "peak_source": f"derived: {SM_COUNT} SMs x {IMAD_PER_CLK_SM} IMAD/clk x "
-                                   f"{sm_mhz:.0f} MHz (MEASURED_PEAKS sm_max_mhz)",
+                                   f"{sm_mhz:.0f} MHz (MEASURED_PEAKS sm_max_mhz, else the B200 maximum)",
                     "work_per_launch": f"{entries:.3e} bucket additions x 6 x {mont_imad(N_LIMBS)} IMAD"}
-    msm_w = w_msm(n, N_LIMBS)
-    msm_roof = {"achieved": msm_w / (ms / 1e3) / 1e12, "peak": peak_imad / 1e12, "unit": "TIMAD/s",
-                "frac": msm_w / (ms / 1e3) / peak_imad, "work": f"W_msm(2^{args.logn}) = {msm_w:.3e} IMAD"}
+        msm_w = w_msm(n, N_LIMBS)
+        whole = {"achieved": msm_w / (step_ms / 1e3) / 1e12, "peak": peak_imad / 1e12, "unit": "TIMAD/s",
+                 "frac": msm_w / (step_ms / 1e3) / peak_imad,
+                 "work": f"W_msm(2^{args.logn}) = {msm_w:.3e} IMAD"}
+        return roof, whole
+
+    roofline, msm_roof = rooflines(head, stage, ms)
+    # the other path, same protocol (device time, then e2e)
+    o_ms, _, o_stage, _ = timed(other, args.steps, False)
+    o_e2e = e2e(other)
+    o_roof, o_whole = rooflines(other, o_stage, o_ms)
+    other_line = {"path": other, "value": n * ws / (o_ms / 1e3) / 1e6, "unit": "Mpts/s", "ms_per_step": o_ms,
+                  "window_bits": kb.msm_window(CURVE, n, subgroup=(other == "subgroup")),
+                  "e2e": {"value": n * ws / (o_e2e / 1e3) / 1e6, "unit": "Mpts/s", "ms_per_step": o_e2e,
+                          "api": host_fn[other].__name__},
+                  "roofline_frac": o_roof["frac"] if o_roof else None, "msm_roofline_frac": o_whole["frac"],
+                  "stage_ms": o_stage}
 
     extra = None
     if rank == 0 and not args.no_extra:
-        extra = bench_extra(args, SM_COUNT * IMAD_PER_CLK_SM * float(load_peaks().get("sm_max_mhz", 1965.0)) * 1e6)
+        extra = bench_extra(args, peak_imad)
 
     kzg_batched = kzg_served = None
     if rank == 0 and not args.no_kzg:
         kzg_batched = bench_batched_commits(args)
         kzg_served = bench_served_commits(args)
 
-    cpu = None
+    cpu = cpu_more = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        import _oracle as O  # noqa: F401  (tests/ on sys.path inside cpu_reference_msm)
-        ns = 1 << args.ref_logn
-        threads = os.cpu_count() or 1
-        t = cpu_reference_msm(host_pts[:PB * ns], host_sc[:32 * ns], ns, threads)
-        cpu = {"value": ns / t / 1e6, "unit": "Mpts/s", "cores": threads, "kind": "reference",
-               "sample": f"gpukit_multi_pippenger_cpu on {threads} slices of n=2^{args.ref_logn} "
-                         "(first 2^%d inputs of the workload), summed with the reference g1_add" % args.ref_logn}
+        threads = ref_threads()
+        t, _ = ref_block(host_sc, host_pts, n, 0, threads)
+        m = min(n, 1 << REF_BLOCK_LOG)
+        cpu = {"value": m / t / 1e6, "unit": "Mpts/s", "cores": threads, "kind": "reference",
+               "sample": "one step of the reference arm: " + ref_sample_text(n, threads)}
+        cpu_more = cpu_baselines(args)
 
     if rank == 0:
         line = {
@@ -607,35 +787,44 @@ def run_ours(args, ws, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic",
-            "config": {"workload": f"BLS12-381 G1 MSM n=2^{args.logn}, uniform Fr scalars, "
-                                   "points s_i*G1 with seeded s_i (fixed-base on device)",
-                       "curve": "BLS12-381", "n": n, "window_bits": plan_c,
-                       "l2": "inputs 512 MiB > L2 (no flush)", "parallelism": f"replicas x{ws}"},
+            "config": headline_config(args.logn),
+            "path": {"plain": "kb200_msm_device / gpukit_multi_pippenger: exact for every curve point "
+                              "(256-bit signed windows on BLS12-381)",
+                     "subgroup": "kb200_msm_device_subgroup / gpukit_multi_pippenger_subgroup: points "
+                                 "promised in G1 (GLV split)"}[head],
+            "window_bits": kb.msm_window(CURVE, n, subgroup=(head == "subgroup")),
+            "l2": "inputs 512 MiB > L2 (no flush)", "parallelism": f"replicas x{ws}",
+            "parity": parity,
             "e2e": {"value": n * ws / (e2e_ms / 1e3) / 1e6, "unit": "Mpts/s",
                     "h2d_bytes_per_step": n * (32 + PB), "d2h_bytes_per_step": PB,
-                    "ms_per_step": e2e_ms, "api": "gpukit_multi_pippenger"},
+                    "ms_per_step": e2e_ms, "api": host_fn[head].__name__},
             "gpu_launches": launches,
             "roofline": roofline,
             "msm_roofline": msm_roof,
             "stage_ms": stage,
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "msm_other_path": other_line,
             "configs": extra,
             "kzg_batched": kzg_batched,
             "kzg_served": kzg_served,
+            "cpu_baselines": cpu_more,
         }
         print(json.dumps(line), flush=True)
 
 
-def bucket_traffic(entries):
+def bucket_traffic(path, entries):
     """DRAM bytes of one MSM's bucket accumulation (every pairing-level and
-    accumulation launch): the ncu capture committed under profiles/
-    (dram__bytes_read.sum + dram__bytes_write.sum summed over those launches
-    of one MSM), scaled by the number of sorted entries."""
+    accumulation launch): dram__bytes_read.sum + dram__bytes_write.sum summed
+    over those launches of one smaller MSM of the same path in an ncu
+    capture (profiles/msm_bucket_phase_dram.json), scaled by the number of
+    sorted entries (the phase's traffic grows with them)."""
     p = ROOT / "profiles" / "msm_bucket_phase_dram.json"
     if CURVE != 2 or not p.exists():
         return None
-    d = json.loads(p.read_text())["bls12_381"]
+    d = json.loads(p.read_text()).get(f"bls12_381_{path}")
+    if not d:
+        return None
     return (d["dram_read"] + d["dram_write"]) * entries / d["entries"]
 
 
@@ -646,17 +835,22 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--logn", type=int, default=LOGN)
-    ap.add_argument("--ref-logn", type=int, default=17)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-kzg", action="store_true")
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--case", default="msm", choices=["msm", "ntt"],
                     help="msm: the benchmark line; ntt: one Fr NTT size only (profiling)")
+    ap.add_argument("--path", default="plain", choices=["plain", "subgroup"],
+                    help="headline MSM entry point: plain (exact for every point) or subgroup (GLV)")
     ap.add_argument("--commits", type=int, default=512)
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[100.0, 400.0, 1600.0])
     ap.add_argument("--serve-requests", type=int, default=80)
     args = ap.parse_args()
     sys.path.insert(0, str(ROOT / "tests"))
+    if args.impl == "reference":
+        # host-only: no process group, no CUDA context, no CUDA library
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
     ws, rank, local = setup_dist()
     try:
         if args.case == "ntt":
@@ -676,10 +870,7 @@ def main():
             assert d.cpu().numpy().tobytes() == x
             print(json.dumps({"case": "ntt", "curve": "BLS12-381", "n": n, "ms_fwd_plus_inv": ms}))
             return
-        if args.impl == "reference":
-            run_reference(args, ws, rank)
-        else:
-            run_ours(args, ws, rank, local)
+        run_ours(args, ws, rank, local)
     finally:
         if ws > 1:
             import torch.distributed as dist

@@ -48,6 +48,10 @@ def lib() -> ctypes.CDLL:
         sigs = {
             "gpukit_multi_pippenger": (c.c_int, [c.c_uint32, u8p, u8p, sz, vp]),
             "gpukit_multi_pippenger_cuda": (c.c_int, [c.c_uint32, u8p, u8p, sz, vp]),
+            "gpukit_multi_pippenger_subgroup": (c.c_int, [c.c_uint32, u8p, u8p, sz, vp]),
+            "kb200_msm_device_subgroup": (c.c_int, [c.c_uint32, vp, vp, sz, vp, vp]),
+            "kb200_msm_window_subgroup": (c.c_int, [c.c_uint32, sz]),
+            "kb200_msm_entries_subgroup": (c.c_double, [c.c_uint32, sz]),
             "bls12_381_g1_msm": (c.c_int, [vp, vp, u8p, sz]),
             "kzg_blob_setup_load_g1_lagrange": (c.c_int, [u8p, sz]),
             "kzg_blob_setup_generate": (c.c_int, [u8p]),
@@ -119,6 +123,15 @@ def gpukit_multi_pippenger(curve: int, scalars: bytes, points: bytes, n: int) ->
     out = ctypes.create_string_buffer(POINT_BYTES.get(curve, 96))
     _check("gpukit_multi_pippenger",
            lib().gpukit_multi_pippenger(curve, scalars, points, n, out))
+    return out.raw
+
+
+def gpukit_multi_pippenger_subgroup(curve: int, scalars: bytes, points: bytes, n: int) -> bytes:
+    """The same sum for points the caller knows to lie in G1 (GLV split on
+    BLS12-381); unspecified for BLS12-381 curve points outside G1."""
+    out = ctypes.create_string_buffer(POINT_BYTES.get(curve, 96))
+    _check("gpukit_multi_pippenger_subgroup",
+           lib().gpukit_multi_pippenger_subgroup(curve, scalars, points, n, out))
     return out.raw
 
 
@@ -229,8 +242,9 @@ def gen_scalars(curve: int, seed: int, n: int, kind: int = 0) -> bytes:
     return out.raw
 
 
-def msm_window(curve: int, n: int) -> int:
-    return int(lib().kb200_msm_window(curve, n))
+def msm_window(curve: int, n: int, subgroup: bool = False) -> int:
+    f = lib().kb200_msm_window_subgroup if subgroup else lib().kb200_msm_window
+    return int(f(curve, n))
 
 
 def launch_count() -> int:

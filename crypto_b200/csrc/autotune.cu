@@ -1,8 +1,11 @@
-// Autotuner: per size class (log2 n) and curve, time the candidate MSM
-// window widths around the cost model's choice and the candidate NTT radix
-// splits on this GPU, keep the fastest, and cache the table in a text file
-// keyed by GPU name and driver version.  Plans consult the table first
-// (msm_tune_get / ntt_tune_get), falling back to the cost model.
+// Autotuner: per size class (log2 n) and curve, time on this GPU the
+// candidate MSM window widths around the cost model's choice (256-bit
+// windows and the windows of GLV halves), the candidate NTT radix splits,
+// and -- with a resident SRS -- the shifted-table window of single KZG
+// commits (13, 16 or 19 bits, which the batched and served commits use per
+// commit); keep the fastest and cache them in a text file keyed by GPU name
+// and driver version.  Plans consult the tables first (msm_tune_get,
+// ntt_tune_get, commit_tune_get), falling back to the cost models.
 #include "../../include/kinet_b200/crypto_b200.h"
 #include "kzg.cuh"
 #include "msm.cuh"
@@ -74,7 +77,7 @@ int kb200_autotune(uint32_t curve, int log_lo, int log_hi, const char* cache_pat
         out.reserve(256, st);
         KB_CUDA(cudaMemcpyAsync(sc.ptr, hs.data(), nmax * 32, cudaMemcpyHostToDevice, st));
         FixedBase* fb = fixed_base_create((int)curve, st);
-        fixed_base_mul(fb, sc.as<uint8_t>(), nmax, table.as<uint32_t>(), nullptr, st);
+        fixed_base_mul(fb, sc.as<uint8_t>(), nmax, table.as<uint32_t>(), pts.as<uint8_t>(), st);
         MsmEngine* eng = msm_engine_create((int)curve);
         NttEngine* ntt = ntt_engine_create((int)curve);
         nt.reserve(nmax * 32, st);
@@ -100,8 +103,33 @@ int kb200_autotune(uint32_t curve, int log_lo, int log_hi, const char* cache_pat
                     best_c = c;
                 }
             }
-            msm_tune_set((int)curve, lg, best_c);
+            msm_tune_set((int)curve, lg, best_c, false);
             log << key << " msm " << curve << " " << lg << " " << best_c << " " << best << "\n";
+            // windows of the GLV halves (the wire path with the G1 promise:
+            // BN254 always splits, BLS12-381 on the _subgroup entry points)
+            {
+                MsmOptions g;
+                g.points_in_g1 = true;
+                const int g0 = make_msm_plan_glv((int)curve, n, g).c;
+                int best_g = g0;
+                float best_gt = 1e30f;
+                for (int c = std::max(4, g0 - 2); c <= std::min(20, g0 + 2); ++c) {
+                    MsmOptions o;
+                    o.force_c = c;
+                    o.points_in_g1 = true;
+                    const int reps = lg >= 20 ? 2 : 5;
+                    const float ms = time_ms(st, [&] {
+                        msm_run_wire(eng, sc.as<uint8_t>(), pts.as<uint8_t>(), n, out.as<uint8_t>(),
+                                     nullptr, st, o);
+                    }, reps);
+                    if (ms < best_gt) {
+                        best_gt = ms;
+                        best_g = c;
+                    }
+                }
+                msm_tune_set((int)curve, lg, best_g, true);
+                log << key << " msm_glv " << curve << " " << lg << " " << best_g << " " << best_gt << "\n";
+            }
             // NTT first-pass radix (two- and three-pass sizes)
             if (lg > 12) {
                 KB_CUDA(cudaMemcpyAsync(nt.ptr, sc.ptr, n * 32, cudaMemcpyDeviceToDevice, st));
@@ -133,9 +161,12 @@ int kb200_autotune(uint32_t curve, int log_lo, int log_hi, const char* cache_pat
         fixed_base_destroy(fb);
         for (DevBuf* b : {&sc, &pts, &table, &out, &nt}) b->release();
         cudaStreamDestroy(st);
+        // shifted-table windows of single commits (BLS12-381, resident SRS)
+        std::string commit_log;
+        if (curve == 2) tune_commit_windows(log_lo, log_hi, key, commit_log);
         if (cache_path) {
             std::ofstream f(cache_path, std::ios::app);
-            f << log.str();
+            f << log.str() << commit_log;
         }
         return tuned;
     } catch (const std::exception& e) {
@@ -161,10 +192,16 @@ int kb200_autotune_load(const char* cache_path) {
             if (!(is >> k >> kind >> curve >> lg >> v)) continue;
             if (k != key) continue;
             if (kind == "msm") {
-                msm_tune_set(curve, lg, v);
+                msm_tune_set(curve, lg, v, false);
+                ++applied;
+            } else if (kind == "msm_glv") {
+                msm_tune_set(curve, lg, v, true);
                 ++applied;
             } else if (kind == "ntt") {
                 ntt_tune_set(curve, lg, v);
+                ++applied;
+            } else if (kind == "commit" && curve == 2) {
+                commit_tune_set(lg, v);
                 ++applied;
             }
         }
@@ -177,13 +214,22 @@ int kb200_autotune_load(const char* cache_path) {
 
 // Direct access to the tuning tables (also used by tests).
 int kb200_tune_get(int kind, uint32_t curve, int log_n) {
-    return kind == 0 ? msm_tune_get((int)curve, log_n) : ntt_tune_get((int)curve, log_n);
+    switch (kind) {
+        case 0: return msm_tune_get((int)curve, log_n, false);
+        case 1: return ntt_tune_get((int)curve, log_n);
+        case 2: return msm_tune_get((int)curve, log_n, true);
+        case 3: return curve == 2 ? commit_tune_get(log_n) : 0;
+        default: return 0;
+    }
 }
 void kb200_tune_set(int kind, uint32_t curve, int log_n, int value) {
-    if (kind == 0)
-        msm_tune_set((int)curve, log_n, value);
-    else
-        ntt_tune_set((int)curve, log_n, value);
+    switch (kind) {
+        case 0: msm_tune_set((int)curve, log_n, value, false); break;
+        case 1: ntt_tune_set((int)curve, log_n, value); break;
+        case 2: msm_tune_set((int)curve, log_n, value, true); break;
+        case 3: if (curve == 2) commit_tune_set(log_n, value); break;
+        default: break;
+    }
 }
 
 }  // extern "C"

@@ -160,7 +160,7 @@ static bool is_pow2(size_t n) { return n && !(n & (n - 1)); }
 // ---- MSM -------------------------------------------------------------------
 
 static int msm_host(uint32_t curve, const uint8_t* scalars, const uint8_t* points, size_t n,
-                    uint8_t* result) {
+                    uint8_t* result, bool points_in_g1) {
     if (!result) return KB200_GPUKIT_ERR_NULL_ARG;
     if (n > 0 && (!scalars || !points)) return KB200_GPUKIT_ERR_NULL_ARG;
     if (curve == 0 || curve == 3) {
@@ -180,6 +180,7 @@ static int msm_host(uint32_t curve, const uint8_t* scalars, const uint8_t* point
                        c->h_out.reserve(256, st);
                        MsmOptions opt;
                        opt.ref_carry_quirk = true;
+                       opt.points_in_g1 = points_in_g1;
                        if (n) {
                            msm_run_host_wire(c->msm_for((int)curve), scalars, points, n,
                                              c->d_a.as<uint8_t>(), c->d_b.as<uint8_t>(),
@@ -389,6 +390,65 @@ static void commit_on_device(DeviceCtx* c, uint32_t* d_evals, size_t n, uint8_t*
                   c->d_tmp.as<uint8_t>(), d_out48, st, opt);
 }
 
+// Autotuner step for single commits against the resident SRS: for each size
+// class 2^lg (lg in [log_lo, log_hi], at most the SRS length) time one
+// commit per shifted-table window 13 / 16 / 19 and keep the fastest in the
+// commit tuning table.  Appends "<key> commit 2 <lg> <c> <ms>" lines to log.
+// Returns the classes tuned (0 without a resident SRS).
+int tune_commit_windows(int log_lo, int log_hi, const std::string& key, std::string& log) {
+    DeviceCtx* c = get_ctx();
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!c->srs_n) return 0;
+    cudaStream_t st = c->stream;
+    int tuned = 0;
+    const size_t nmax = std::min(c->srs_n, (size_t)1 << log_hi);
+    std::vector<uint8_t> hs(nmax * 32);
+    kb200_gen_scalars(2, 0xC0117u, nmax, 0, hs.data());
+    DevBuf src;
+    src.reserve(nmax * 32, st);
+    c->d_a.reserve(nmax * 32 + 64, st);
+    c->d_out.reserve(256, st);
+    KB_CUDA(cudaMemcpyAsync(src.ptr, hs.data(), nmax * 32, cudaMemcpyHostToDevice, st));
+    cudaEvent_t a, b;
+    KB_CUDA(cudaEventCreate(&a));
+    KB_CUDA(cudaEventCreate(&b));
+    for (int lg = log_lo; lg <= log_hi && ((size_t)1 << lg) <= c->srs_n; ++lg) {
+        const size_t n = (size_t)1 << lg;
+        int best_c = 0;
+        float best = 1e30f;
+        for (int cand : {13, 16, 19}) {
+            commit_tune_set(lg, cand);
+            auto one = [&] {
+                KB_CUDA(cudaMemcpyAsync(c->d_a.ptr, src.ptr, n * 32, cudaMemcpyDeviceToDevice, st));
+                commit_on_device(c, c->d_a.as<uint32_t>(), n, c->d_out.as<uint8_t>(), st);
+            };
+            one();  // builds the window's shifted table and sizes the engines
+            KB_CUDA(cudaStreamSynchronize(st));
+            const int reps = lg >= 14 ? 3 : 8;
+            KB_CUDA(cudaEventRecord(a, st));
+            for (int r = 0; r < reps; ++r) one();
+            KB_CUDA(cudaEventRecord(b, st));
+            KB_CUDA(cudaEventSynchronize(b));
+            float ms = 0;
+            KB_CUDA(cudaEventElapsedTime(&ms, a, b));
+            ms /= reps;
+            if (ms < best) {
+                best = ms;
+                best_c = cand;
+            }
+        }
+        commit_tune_set(lg, best_c);
+        log += key + " commit 2 " + std::to_string(lg) + " " + std::to_string(best_c) + " " +
+               std::to_string(best) + "\n";
+        ++tuned;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    KB_CUDA(cudaStreamSynchronize(st));
+    src.release();
+    return tuned;
+}
+
 // After a new SRS: build the shifted tables of every window size a commit of
 // up to srs_n evaluations selects, and run one commit of zeros per power of
 // two, so the per-call engines reach their working size here.  Without it the
@@ -417,12 +477,17 @@ extern "C" {
 
 int gpukit_multi_pippenger(uint32_t curve, const uint8_t* scalars, const uint8_t* points, size_t n,
                            uint8_t* result) {
-    return msm_host(curve, scalars, points, n, result);
+    return msm_host(curve, scalars, points, n, result, false);
 }
 
 int gpukit_multi_pippenger_cuda(uint32_t curve, const uint8_t* scalars, const uint8_t* points,
                                 size_t n, uint8_t* result) {
-    return msm_host(curve, scalars, points, n, result);
+    return msm_host(curve, scalars, points, n, result, false);
+}
+
+int gpukit_multi_pippenger_subgroup(uint32_t curve, const uint8_t* scalars, const uint8_t* points,
+                                    size_t n, uint8_t* result) {
+    return msm_host(curve, scalars, points, n, result, true);
 }
 
 int ntt_fr_forward(int curve, uint8_t* coeffs32le, size_t n, int coset) {
@@ -547,8 +612,8 @@ int kzg_commit_batch(const uint8_t* evals32le, const size_t* sizes, size_t count
                    });
 }
 
-int kb200_msm_device(uint32_t curve, const void* d_scalars, const void* d_points, size_t n,
-                     void* d_result, void* stream) {
+static int msm_device(uint32_t curve, const void* d_scalars, const void* d_points, size_t n,
+                      void* d_result, void* stream, bool points_in_g1) {
     if (!d_result || (n && (!d_scalars || !d_points))) return KB200_GPUKIT_ERR_NULL_ARG;
     if (curve != 1 && curve != 2) return KB200_GPUKIT_ERR_BACKEND;
     return guarded(KB200_GPUKIT_ERR_DISPATCH, KB200_GPUKIT_ERR_BAD_SIZE, KB200_GPUKIT_ERR_DISPATCH,
@@ -557,11 +622,22 @@ int kb200_msm_device(uint32_t curve, const void* d_scalars, const void* d_points
                        std::lock_guard<std::mutex> lk(c->mu);
                        MsmOptions opt;
                        opt.ref_carry_quirk = true;
+                       opt.points_in_g1 = points_in_g1;
                        msm_run_wire(c->msm_for((int)curve), (const uint8_t*)d_scalars,
                                     (const uint8_t*)d_points, n, (uint8_t*)d_result, nullptr,
                                     (cudaStream_t)stream, opt);
                        return KB200_GPUKIT_OK;
                    });
+}
+
+int kb200_msm_device(uint32_t curve, const void* d_scalars, const void* d_points, size_t n,
+                     void* d_result, void* stream) {
+    return msm_device(curve, d_scalars, d_points, n, d_result, stream, false);
+}
+
+int kb200_msm_device_subgroup(uint32_t curve, const void* d_scalars, const void* d_points,
+                              size_t n, void* d_result, void* stream) {
+    return msm_device(curve, d_scalars, d_points, n, d_result, stream, true);
 }
 
 int kzg_blob_setup_load_g1_lagrange(const uint8_t* points48, size_t n) {
@@ -721,20 +797,31 @@ int kb200_msm_stage_ms(uint32_t curve, float* out, int max) {
     }
 }
 
-double kb200_msm_entries(uint32_t curve, size_t n) {
+static double msm_entries(uint32_t curve, size_t n, bool in_g1) {
     MsmOptions opt;
-    if (curve == 2) {  // the wire path splits BLS12-381 scalars (GLV)
-        const MsmPlan p = make_msm_plan_glv(n, opt);
-        return 2.0 * (double)n * (double)((128 + p.c - 1) / p.c) * (1.0 - std::ldexp(1.0, -p.c));
+    opt.points_in_g1 = in_g1;
+    if (curve != 1 && curve != 2) return 0.0;
+    if (msm_wire_uses_glv((int)curve, opt)) {
+        const MsmPlan p = make_msm_plan_glv((int)curve, n, opt);
+        // populated windows of the halves: their magnitudes are below 2^128 / 2^126
+        const int hb = curve == 2 ? 128 : 126;
+        return 2.0 * (double)n * (double)((hb + p.c - 1) / p.c) * (1.0 - std::ldexp(1.0, -p.c));
     }
     const MsmPlan p = make_msm_plan((int)curve, n, opt);
     return (double)n * (double)((255 + p.c - 1) / p.c) * (1.0 - std::ldexp(1.0, -p.c));
 }
 
-int kb200_msm_window(uint32_t curve, size_t n) {
+static int msm_window(uint32_t curve, size_t n, bool in_g1) {
     MsmOptions opt;
-    if (curve == 2) return make_msm_plan_glv(n, opt).c;
+    opt.points_in_g1 = in_g1;
+    if (curve != 1 && curve != 2) return 0;
+    if (msm_wire_uses_glv((int)curve, opt)) return make_msm_plan_glv((int)curve, n, opt).c;
     return make_msm_plan((int)curve, n, opt).c;
 }
+
+double kb200_msm_entries(uint32_t curve, size_t n) { return msm_entries(curve, n, false); }
+double kb200_msm_entries_subgroup(uint32_t curve, size_t n) { return msm_entries(curve, n, true); }
+int kb200_msm_window(uint32_t curve, size_t n) { return msm_window(curve, n, false); }
+int kb200_msm_window_subgroup(uint32_t curve, size_t n) { return msm_window(curve, n, true); }
 
 }  // extern "C"

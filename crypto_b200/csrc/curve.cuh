@@ -37,6 +37,15 @@ static __constant__ uint32_t kGlvBeta2Mont[12] = {0x8671f071, 0xcd03c9e4, 0x1fcd
                                                   0xd3851b95, 0x587042af, 0x01bacb9e, 0x8eb60ebe,
                                                   0x83d050d2, 0x03f97d6e, 0x54638741, 0x18f02065};
 
+// GLV endomorphism of BN254 G1: phi(x, y) = (beta x, y) = [lambda](x, y)
+// with lambda = 0xb3c4d79d41a917585bfc41088d8daaa78b17ea66b99c90dd (a cube
+// root of unity mod r) and beta = 0x59e26bcea0d48bacd4f263f1acdb5c4f5763473177fffffe
+// (a cube root of unity mod p; the pair is matched on the generator), here
+// in Montgomery form (beta * 2^256 mod p).  Every BN254 point has order r
+// (cofactor 1), so the identity holds for every input point.
+static __constant__ uint32_t kBnGlvBetaMont[8] = {0xd782e155, 0x71930c11, 0xffbe3323, 0xa6bb947c,
+                                                  0xd4741444, 0xaa303344, 0x26594943, 0x2c3b3f0d};
+
 struct G1BN {
     using F = FpBN;
     static constexpr uint32_t B = 3;

@@ -284,7 +284,28 @@ const uint32_t* shift_tables_get(ShiftTables* t, int c, cudaStream_t st) {
     return b.as<uint32_t>();
 }
 
+static std::mutex g_commit_tune_mu;
+static int g_commit_tune[48];
+
+void commit_tune_set(int log_n, int c) {
+    if (log_n < 0 || log_n >= 48 || (c != 0 && c != 13 && c != 16 && c != 19)) return;
+    std::lock_guard<std::mutex> lk(g_commit_tune_mu);
+    g_commit_tune[log_n] = c;
+}
+
+int commit_tune_get(int log_n) {
+    if (log_n < 0 || log_n >= 48) return 0;
+    std::lock_guard<std::mutex> lk(g_commit_tune_mu);
+    return g_commit_tune[log_n];
+}
+
 int shift_c_for(const size_t* sizes, size_t count) {
+    // A single commit: the autotuner's choice for its size class, if any.
+    if (count == 1 && sizes[0]) {
+        int lg = 0;
+        while (((size_t)1 << lg) < sizes[0]) ++lg;
+        if (const int t = commit_tune_get(lg)) return t;
+    }
     // Accumulation: one entry per window canonical scalars populate;
     // reduction: ~7 entry-equivalents per bucket of the single shared window
     // of each item.  Only three window sizes are offered, so a

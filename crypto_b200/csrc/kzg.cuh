@@ -6,6 +6,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <string>
 
 namespace kb200 {
 
@@ -36,6 +37,12 @@ const uint32_t* shift_tables_get(ShiftTables* t, int c, cudaStream_t st);
 // Window size minimising the modelled work of MSMs of these sizes against a
 // shifted table.
 int shift_c_for(const size_t* sizes, size_t count);
+// Autotuner: shifted-table window (13, 16 or 19; 0 = cost model) of a
+// single commit of 2^log_n evaluations.
+void commit_tune_set(int log_n, int c);
+int commit_tune_get(int log_n);
+// Times single commits against the resident SRS per window (capi.cu).
+int tune_commit_windows(int log_lo, int log_hi, const std::string& key, std::string& log);
 
 // out[i] = tau^i (canonical 32-byte little-endian Fr), i < n.
 void fr_powers(int curve, const uint8_t* d_tau, size_t n, uint8_t* d_out, cudaStream_t stream);

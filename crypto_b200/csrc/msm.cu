@@ -152,18 +152,18 @@ __global__ void k_fold_counts(const uint32_t* __restrict__ offsets, uint32_t K, 
 // ---------------------------------------------------------------------------
 
 static std::mutex g_tune_mu;
-static int g_tune[3][48];
+static int g_tune[2][3][48];  // [GLV][curve][log2 n]
 
-void msm_tune_set(int curve, int log_n, int c) {
+void msm_tune_set(int curve, int log_n, int c, bool glv) {
     if (curve < 1 || curve > 2 || log_n < 0 || log_n >= 48) return;
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[curve][log_n] = c;
+    g_tune[glv ? 1 : 0][curve][log_n] = c;
 }
 
-int msm_tune_get(int curve, int log_n) {
+int msm_tune_get(int curve, int log_n, bool glv) {
     if (curve < 1 || curve > 2 || log_n < 0 || log_n >= 48) return 0;
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    return g_tune[curve][log_n];
+    return g_tune[glv ? 1 : 0][curve][log_n];
 }
 
 int reference_best_c(size_t n) {
@@ -194,14 +194,24 @@ static uint32_t top_buckets(int c, int W, int scalar_bits = 256) {
     return 1u << bits;
 }
 
-// Live buckets of the top window of a GLV half.  Both halves are below
-// max(lambda - 1, (r - 1) / lambda) = 0xac45a4010001a402_0000000100000000;
-// the top window is unsigned (its digit is the raw bits plus the carry from
-// below, never negated), so nothing carries beyond it and the halves need
-// ceil(128 / c) windows.  For c = 4, 8, 16 its digit exceeds 2^(c-1).
-static uint32_t glv_top_buckets(int c, int W) {
-    const unsigned __int128 bound =
-        ((unsigned __int128)0xac45a4010001a402ull << 64) | (unsigned __int128)0x0000000100000000ull;
+// GLV halves: |k1|, |k2| <= glv_bound(curve), so ceil(bits / c) windows
+// cover them, the top window unsigned (its digit is the raw bits plus the
+// carry from below, never negated) so nothing carries beyond it.
+//   BLS12-381: k1 = k mod lambda, k2 = k div lambda, both at most
+//     max(lambda - 1, (r - 1) / lambda) = 0xac45a4010001a402_0000000100000000.
+//   BN254: Babai rounding on a reduced lattice basis; both magnitudes at
+//     most (|a1| + |a2|) (1/2 + 2^-129) < 0x37a6c124775c2cfecadc035e53799c78.
+static unsigned __int128 glv_bound(int curve) {
+    if (curve == 2)
+        return ((unsigned __int128)0xac45a4010001a402ull << 64) | (unsigned __int128)0x0000000100000000ull;
+    return ((unsigned __int128)0x37a6c124775c2cfeull << 64) | (unsigned __int128)0xcadc035e53799c78ull;
+}
+static int glv_bits(int curve) { return curve == 2 ? 128 : 126; }
+
+// Live buckets of the top window of a GLV half (for c = 4, 8, 16 on
+// BLS12-381 its digit exceeds 2^(c-1)).
+static uint32_t glv_top_buckets(int curve, int c, int W) {
+    const unsigned __int128 bound = glv_bound(curve);
     const int sh = c * (W - 1);
     return (uint32_t)(sh >= 128 ? 0 : (bound >> sh)) + 1u;
 }
@@ -219,7 +229,7 @@ MsmPlan make_msm_plan(int curve, size_t n, const MsmOptions& opt) {
         return v && *v ? std::atoi(v) : 0;
     }();
     int c = opt.force_c > 0 ? opt.force_c : env_c;
-    if (c <= 0) c = msm_tune_get(curve, ceil_log2(n ? n : 1));
+    if (c <= 0) c = msm_tune_get(curve, ceil_log2(n ? n : 1), false);
     if (c <= 0) {
         // Cost model in accumulation-entry units: one per entry over the
         // windows that canonical (< 2^255) scalars populate, plus ~7 per
@@ -245,18 +255,20 @@ MsmPlan make_msm_plan(int curve, size_t n, const MsmOptions& opt) {
     return p;
 }
 
-MsmPlan make_msm_plan_glv(size_t n, const MsmOptions& opt) {
+MsmPlan make_msm_plan_glv(int curve, size_t n, const MsmOptions& opt) {
     MsmPlan p;
     static const int env_c = [] {
         const char* v = std::getenv("KB200_MSM_GLV_C");
         return v && *v ? std::atoi(v) : 0;
     }();
+    const int hb = glv_bits(curve);
     int c = opt.force_c > 0 ? opt.force_c : env_c;
+    if (c <= 0) c = msm_tune_get(curve, ceil_log2(n ? n : 1), true);
     if (c <= 0) {
-        // 2n points, ceil(128/c) populated windows of the 128-bit halves.
+        // 2n points, ceil(hb/c) populated windows of the halves.
         double best = 1e300;
         for (int cc = 4; cc <= 20; ++cc) {
-            const double wl = (double)((128 + cc - 1) / cc);
+            const double wl = (double)((hb + cc - 1) / cc);
             const double red = wl * 2.0 * (double)n >= PAIRED_ENTRIES ? RED_COST_PAIRED : RED_COST;
             const double cost = wl * 2.0 * (double)n + red * wl * (double)(1u << (cc - 1));
             if (cost < best) {
@@ -268,10 +280,15 @@ MsmPlan make_msm_plan_glv(size_t n, const MsmOptions& opt) {
     if (c < 2) c = 2;
     if (c > 22) c = 22;
     p.c = c;
-    p.W = (128 + c - 1) / c;
+    p.W = (hb + c - 1) / c;
     p.M = 1u << (c - 1);
-    p.M_top = glv_top_buckets(c, p.W);
+    p.M_top = glv_top_buckets(curve, c, p.W);
     return p;
+}
+
+bool msm_wire_uses_glv(int curve, const MsmOptions& opt) {
+    if (opt.shift_c > 0) return false;
+    return curve == 1 || (curve == 2 && opt.points_in_g1);
 }
 
 class MsmBatchPlan {
@@ -334,9 +351,9 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         const size_t n = items[i].n;
         if (n >= (1ull << 31) || items[i].point_off + n >= (1ull << 31))
             throw std::invalid_argument("msm: more than 2^31 points");
-        const bool glv = opt.glv && curve == 2 && opt.shift_c <= 0;
+        const bool glv = opt.glv && opt.shift_c <= 0;
         if (glv) {
-            plans[i] = make_msm_plan_glv(n, opt);
+            plans[i] = make_msm_plan_glv(curve, n, opt);
             if (items[i].point_off + n > opt.glv_rows || 2 * opt.glv_rows >= (1ull << 31))
                 throw std::invalid_argument("msm: item outside the GLV table");
         } else if (opt.shift_c > 0) {
@@ -919,16 +936,11 @@ void msm_run_table(MsmEngine* e, const uint8_t* d_scalars, const uint32_t* d_tab
 void msm_run_wire(MsmEngine* e, const uint8_t* d_scalars, const uint8_t* d_points, size_t n,
                   uint8_t* d_out_wire, uint8_t* d_out_comp, cudaStream_t st,
                   const MsmOptions& opt) {
-    // BLS12-381: GLV split (the table gains the phi(P) rows).  phi(P) =
-    // [lambda]P holds on G1, the prime-order subgroup every caller's points
-    // live in; KB200_MSM_NO_GLV=1 keeps 256-bit windows, whose sum is also
-    // exact for curve points outside G1.
-    static const bool glv_env_off = [] {
-        const char* v = std::getenv("KB200_MSM_NO_GLV");
-        return v && *v && *v != '0';
-    }();
+    // GLV split (the table gains the phi(P) rows) where phi(P) = [lambda]P
+    // holds for every input point: always on BN254, and on BLS12-381 when
+    // the caller vouches that the points lie in G1.
     MsmOptions o2 = opt;
-    const bool glv = e->curve == 2 && opt.shift_c <= 0 && !opt.no_glv && !glv_env_off;
+    const bool glv = msm_wire_uses_glv(e->curve, opt);
     if (glv) {
         o2.glv = true;
         o2.glv_rows = n;
@@ -946,12 +958,8 @@ void msm_run_wire(MsmEngine* e, const uint8_t* d_scalars, const uint8_t* d_point
 void msm_run_host_wire(MsmEngine* e, const uint8_t* h_scalars, const uint8_t* h_points, size_t n,
                        uint8_t* d_scalars, uint8_t* d_points, uint8_t* d_out_wire, cudaStream_t st,
                        const MsmOptions& opt) {
-    static const bool glv_env_off = [] {
-        const char* v = std::getenv("KB200_MSM_NO_GLV");
-        return v && *v && *v != '0';
-    }();
     MsmOptions o2 = opt;
-    const bool glv = e->curve == 2 && opt.shift_c <= 0 && !opt.no_glv && !glv_env_off;
+    const bool glv = msm_wire_uses_glv(e->curve, opt);
     if (glv) {
         o2.glv = true;
         o2.glv_rows = n;

@@ -70,12 +70,18 @@ struct MsmOptions {
     // 0 = plain table.
     int shift_c = 0;
     size_t shift_stride = 0;
-    // GLV split (BLS12-381 only, plain tables): rows glv_rows + i of the
-    // table hold phi(row i) = [lambda] row i; scalars split into two 128-bit
-    // halves (half the windows over twice the points).
+    // GLV split (plain tables): rows glv_rows + i of the table hold
+    // phi(row i) = (beta x, y); scalars split into two halves of at most
+    // 128 bits (half the windows over twice the points).  phi acts as
+    // [lambda] on the prime-order subgroup: on every BN254 point (cofactor
+    // 1), but on BLS12-381 only on G1, not on the whole curve.
     bool glv = false;
     size_t glv_rows = 0;
-    bool no_glv = false;  // msm_run_wire: keep the plain 256-bit windows
+    // msm_run_wire / msm_run_host_wire: the caller vouches that every point
+    // lies in the prime-order subgroup, which lets BLS12-381 use the GLV
+    // split.  Without it BLS12-381 keeps 256-bit windows, whose sum equals
+    // the reference's for every curve point.  (BN254 always splits.)
+    bool points_in_g1 = false;
     int pair_levels = -1; // batch-affine pairing levels (-1: planner's choice or KB200_MSM_PAIR_LEVELS)
     // Host-input pipeline: the first pairing level runs per chunk of point
     // rows as the chunks arrive (sort keys chunk-major).  Single items only;
@@ -96,8 +102,12 @@ int msm_windows_for(int c);
 int reference_best_c(size_t n);
 // Window plan for one MSM of size n (autotuner cache, else cost model).
 MsmPlan make_msm_plan(int curve, size_t n, const MsmOptions& opt);
-// Window plan for a GLV-split MSM of n scalars (2n points, 128-bit halves).
-MsmPlan make_msm_plan_glv(size_t n, const MsmOptions& opt);
+// Window plan for a GLV-split MSM of n scalars (2n points; halves below
+// 2^128 on BLS12-381, 2^126 on BN254).
+MsmPlan make_msm_plan_glv(int curve, size_t n, const MsmOptions& opt);
+// Whether a single MSM through msm_run_wire / msm_run_host_wire splits its
+// scalars (BN254 always; BLS12-381 when the caller vouches for G1).
+bool msm_wire_uses_glv(int curve, const MsmOptions& opt);
 
 // One MSM of a batch: n scalars starting at scalar index `scalar_off` of the
 // batch's scalar array, against table rows point_off .. point_off + n - 1.
@@ -171,8 +181,9 @@ size_t msm_scratch_bytes(int curve, const size_t* ns, size_t count);
 size_t msm_item_scratch_bytes(int curve, size_t n);
 size_t msm_batch_fixed_bytes(int curve);
 
-// Autotuner: record the best window for a size class (log2 n) and curve.
-void msm_tune_set(int curve, int log_n, int c);
-int msm_tune_get(int curve, int log_n);  // 0 if untuned
+// Autotuner: record the best window for a size class (log2 n) and curve,
+// for 256-bit windows or for the windows of GLV halves.
+void msm_tune_set(int curve, int log_n, int c, bool glv);
+int msm_tune_get(int curve, int log_n, bool glv);  // 0 if untuned
 
 }  // namespace kb200

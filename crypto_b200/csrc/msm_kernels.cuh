@@ -105,6 +105,114 @@ static __device__ void glv_split(const uint32_t k[8], uint32_t k1[4], uint32_t k
     }
 }
 
+// GLV split for BN254 G1 (Gallant-Lambert-Vanstone, CRYPTO 2001, with
+// Babai rounding): the lattice {(x, y) : x + y lambda = 0 mod r} has the
+// reduced basis v1 = (a1, -b1), v2 = (a2, b2) (extended Euclid on (r,
+// lambda), det = r), a1 = b2 = 0x89d3256894d213e3,
+// b1 = 0x6f4d8248eeb859fc8211bbeb7d4f1128, a2 = 0x6f4d8248eeb859fd0be4e1541221250b.
+// With cA = round(k b2 / r), cB = round(k b1 / r) -- each computed as
+// (k g + 2^383) >> 384, g = round(2^384 b / r) --
+//   k1 = k - cA a1 - cB a2,   k2 = cA b1 - cB b2,
+// so k1 + k2 lambda = k (mod r) exactly and |k1|, |k2| < 2^126 for every
+// k < r.  The halves are signed: their signs go to the entries' sign bits.
+static __constant__ uint32_t kBnGlvG2[7] = {0x2fafba64, 0x8fa7d32d, 0x773a6ef2, 0x6eb9c714,
+                                            0xc7e0b3d7, 0xd91d232e, 0x00000002};
+static __constant__ uint32_t kBnGlvG1[9] = {0x9b9bdffa, 0x86937516, 0x5eaa26d9, 0xa5e38cfb, 0x391eb18d,
+                                            0x7a7bd9d4, 0xa773d2cf, 0x4ccef014, 0x00000002};
+static __constant__ uint32_t kBnGlvA1[2] = {0x94d213e3, 0x89d32568};
+static __constant__ uint32_t kBnGlvB1[4] = {0x7d4f1128, 0x8211bbeb, 0xeeb859fc, 0x6f4d8248};
+static __constant__ uint32_t kBnGlvA2[4] = {0x1221250b, 0x0be4e154, 0xeeb859fd, 0x6f4d8248};
+static __constant__ uint32_t kBnGlvB2[2] = {0x94d213e3, 0x89d32568};
+// 2^256 mod r (BN254): the reference's dropped top carry subtracts 2^256.
+static __constant__ uint32_t kBnR256ModR[8] = {0x4ffffffb, 0xac96341c, 0x9f60cd29, 0x36fc7695,
+                                               0x7879462e, 0x666ea36f, 0x9a07df2f, 0x0e0a77c1};
+
+// round(k g / 2^384) for k of 8 words and g of ng <= 9 words: nr words out.
+static __device__ void mul_round384(const uint32_t k[8], const uint32_t* g, int ng, uint32_t* out,
+                                    int nr) {
+    uint32_t prod[17];
+    for (int i = 0; i < 17; ++i) prod[i] = 0;
+    for (int i = 0; i < 8; ++i) {
+        uint64_t carry = 0;
+        for (int j = 0; j < ng; ++j) {
+            const uint64_t t = (uint64_t)k[i] * g[j] + prod[i + j] + carry;
+            prod[i + j] = (uint32_t)t;
+            carry = t >> 32;
+        }
+        prod[i + ng] = (uint32_t)carry;
+    }
+    // + 2^383 (bit 31 of word 11), then the words from 12 up
+    uint64_t cy = (uint64_t)prod[11] + 0x80000000u;
+    prod[11] = (uint32_t)cy;
+    cy >>= 32;
+    for (int i = 12; i < 17; ++i) {
+        cy += prod[i];
+        prod[i] = (uint32_t)cy;
+        cy >>= 32;
+    }
+    for (int i = 0; i < nr; ++i) out[i] = prod[12 + i];
+}
+
+// acc (8 words, two's complement) += sgn * (a (na words) * b (nb words)).
+static __device__ void mac_signed(uint32_t acc[8], const uint32_t* a, int na, const uint32_t* b,
+                                  int nb, bool subtract) {
+    uint32_t t[8];
+    for (int i = 0; i < 8; ++i) t[i] = 0;
+    for (int i = 0; i < na; ++i) {
+        uint64_t carry = 0;
+        for (int j = 0; j < nb && i + j < 8; ++j) {
+            const uint64_t v = (uint64_t)a[i] * b[j] + t[i + j] + carry;
+            t[i + j] = (uint32_t)v;
+            carry = v >> 32;
+        }
+        if (i + nb < 8) t[i + nb] = (uint32_t)carry;
+    }
+    if (subtract) {
+        sub_words(acc, t, 8);
+    } else {
+        uint64_t cy = 0;
+        for (int i = 0; i < 8; ++i) {
+            cy += (uint64_t)acc[i] + t[i];
+            acc[i] = (uint32_t)cy;
+            cy >>= 32;
+        }
+    }
+}
+
+// Two's complement (8 words) -> magnitude (4 words) and sign.
+static __device__ void signed_to_mag(const uint32_t v[8], uint32_t mag[4], uint32_t& neg) {
+    neg = v[7] >> 31;
+    uint32_t cy = neg;
+    for (int i = 0; i < 4; ++i) {
+        const uint64_t x = (uint64_t)(neg ? ~v[i] : v[i]) + cy;
+        mag[i] = (uint32_t)x;
+        cy = (uint32_t)(x >> 32);
+    }
+}
+
+// k (8 words, < r) -> |k1|, |k2| (4 words each) and their signs.
+static __device__ void glv_split_bn(const uint32_t k[8], uint32_t k1[4], uint32_t k2[4],
+                                    uint32_t& neg1, uint32_t& neg2) {
+    uint32_t cA[2], cB[4];
+    mul_round384(k, kBnGlvG2, 7, cA, 2);
+    mul_round384(k, kBnGlvG1, 9, cB, 4);
+    uint32_t a1[2] = {kBnGlvA1[0], kBnGlvA1[1]};
+    uint32_t a2[4] = {kBnGlvA2[0], kBnGlvA2[1], kBnGlvA2[2], kBnGlvA2[3]};
+    uint32_t b1[4] = {kBnGlvB1[0], kBnGlvB1[1], kBnGlvB1[2], kBnGlvB1[3]};
+    uint32_t b2[2] = {kBnGlvB2[0], kBnGlvB2[1]};
+    uint32_t s1[8], s2[8];
+    for (int i = 0; i < 8; ++i) {
+        s1[i] = k[i];
+        s2[i] = 0;
+    }
+    mac_signed(s1, cA, 2, a1, 2, true);
+    mac_signed(s1, cB, 4, a2, 4, true);
+    mac_signed(s2, cA, 2, b1, 4, false);
+    mac_signed(s2, cB, 4, b2, 2, true);
+    signed_to_mag(s1, k1, neg1);
+    signed_to_mag(s2, k2, neg2);
+}
+
 // Signed-digit recoding, one thread per scalar of the batch.  Entry (w, j)
 // of item i lives at entry_base_i + w * n_i + j (GLV items: k1's digit at
 // entry_base_i + w * 2 n_i + j, k2's at entry_base_i + w * 2 n_i + n_i + j).
@@ -232,6 +340,39 @@ __global__ void k_recode(const ItemDesc* __restrict__ items, uint32_t n_items,
             return;
         }
     }
+    if constexpr (C::CURVE_ID == 1) {
+        if (it.glv) {
+            // k = s mod r (s < 2^256 < 6r), minus 2^256 where the reference
+            // drops its top carry; signed halves, signs into the entries
+            uint32_t k[8], r8[8];
+            for (int i = 0; i < 8; ++i) {
+                k[i] = s[i];
+                r8[i] = FrBN::P(i);
+            }
+            for (int guard = 0; guard < 6 && geq_words(k, r8, 8); ++guard) sub_words(k, r8, 8);
+            if (dropped_carry) {
+                uint32_t t[8];
+                for (int i = 0; i < 8; ++i) t[i] = kBnR256ModR[i];
+                if (geq_words(k, t, 8)) {
+                    sub_words(k, t, 8);
+                } else {  // k + r - t
+                    uint64_t cy = 0;
+                    for (int i = 0; i < 8; ++i) {
+                        cy += (uint64_t)k[i] + r8[i];
+                        k[i] = (uint32_t)cy;
+                        cy >>= 32;
+                    }
+                    sub_words(k, t, 8);
+                }
+            }
+            uint32_t k1[4], k2[4], n1, n2;
+            glv_split_bn(k, k1, k2, n1, n2);
+            const unsigned long long base = it.entry_base + j;
+            emit(k1, 4, row, base, 2ull * it.n, n1);
+            emit(k2, 4, row + it.glv_off, base + it.n, 2ull * it.n, n2);
+            return;
+        }
+    }
     if (dropped_carry) {
         uint32_t cy = 1;
 #pragma unroll
@@ -248,7 +389,8 @@ __global__ void k_recode(const ItemDesc* __restrict__ items, uint32_t n_items,
 // Wire points (big-endian x || y, all-zero = infinity) -> table rows, read
 // in 16-byte pieces when the wire base is 16-byte aligned (rows are 64 or
 // 96 bytes), byte by byte otherwise.  glv_stride: 0, or the row distance of
-// the BLS12-381 GLV rows: row i + glv_stride gets phi(P_i) = (beta2 x, y).
+// the GLV rows: row i + glv_stride gets phi(P_i) = (beta x, y) (beta2 on
+// BLS12-381).
 template <class C, bool V16>
 __global__ void k_wire_to_table(const uint8_t* __restrict__ wire, uint32_t* __restrict__ table,
                                 size_t n, size_t glv_stride) {
@@ -302,15 +444,13 @@ __global__ void k_wire_to_table(const uint8_t* __restrict__ wire, uint32_t* __re
     fe_to_mont(y, y);
     fe_store16(dst, x);
     fe_store16(dst + N, y);
-    if constexpr (C::CURVE_ID == 2) {
-        if (glv_stride) {
-            Fe<F> b;
+    if (glv_stride) {
+        Fe<F> b;
 #pragma unroll
-            for (int k = 0; k < N; ++k) b.v[k] = kGlvBeta2Mont[k];
-            fe_mul(x, x, b);
-            fe_store16(dst + glv_stride * 2 * N, x);
-            fe_store16(dst + glv_stride * 2 * N + N, y);
-        }
+        for (int k = 0; k < N; ++k) b.v[k] = C::CURVE_ID == 2 ? kGlvBeta2Mont[k] : kBnGlvBetaMont[k % 8];
+        fe_mul(x, x, b);
+        fe_store16(dst + glv_stride * 2 * N, x);
+        fe_store16(dst + glv_stride * 2 * N + N, y);
     }
 }
 

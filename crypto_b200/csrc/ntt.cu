@@ -594,11 +594,12 @@ void ntt_run_list(NttEngine* e, uint32_t* d, size_t n, int inverse, int coset, s
 // ---------------------------------------------------------------------------
 // Allocation-free Fr NTT.
 //
-// Some callers cannot allocate device memory: code that runs while a CUDA
-// graph is being captured, a latency-critical path where cudaMalloc's
-// implicit device-wide synchronisation is unacceptable, or a process whose
-// device memory is entirely owned by another allocator (a framework's
-// caching pool).  For them ntt_fr_transform_noalloc keeps all its scratch --
+// Some callers cannot allocate device memory: a process whose device memory
+// is reserved up front by another allocator (a framework's caching pool, a
+// fixed arena), where cudaMalloc fails or fragments that reservation, and a
+// latency-bound service that cannot afford the device-wide waits of
+// cudaMalloc and cudaFree while other work runs.  For them
+// ntt_fr_transform_noalloc keeps all its scratch --
 // the transform buffer, the pass ping-pong buffer, the twiddle table, the
 // coset tables and the constants -- in one file-scope device array of fixed
 // size, so a call allocates nothing.  The limit is n <= 2^16 elements

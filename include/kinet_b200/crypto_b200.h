@@ -60,10 +60,12 @@ extern "C" {
  * secp256k1 (0) and banderwagon (3) return GPUKIT_ERR_NOTIMPL so the
  * reference dispatcher's CPU fallback still covers them; unknown ids return
  * GPUKIT_ERR_BACKEND as the CPU body does.  Points must be on the curve
- * (neither implementation checks; off-curve input is undefined).  For
- * BLS12-381 the sum is computed with the GLV endomorphism, which equals the
- * reference's sum for points of G1 (the prime-order subgroup); for curve
- * points outside G1 set KB200_MSM_NO_GLV=1 to keep plain 256-bit windows. */
+ * (neither implementation checks; off-curve input is undefined).  Like the
+ * reference's reader (gpukit/curve_traits/bls12_381_g1_first_party_traits.h:
+ * 58-69), no subgroup check is made and none is needed: a BLS12-381 point
+ * outside G1 gets the same bytes as from the reference.  (BN254 sums use
+ * the GLV endomorphism, which acts as [lambda] on every BN254 point:
+ * cofactor 1.) */
 int gpukit_multi_pippenger(uint32_t curve, const uint8_t* scalars, const uint8_t* points,
                            size_t n, uint8_t* result);
 
@@ -71,6 +73,17 @@ int gpukit_multi_pippenger(uint32_t curve, const uint8_t* scalars, const uint8_t
  * to NOTIMPL at gpukit/gpu/cuda/multi_pippenger.cu:38-44).  Same contract. */
 int gpukit_multi_pippenger_cuda(uint32_t curve, const uint8_t* scalars,
                                 const uint8_t* points, size_t n, uint8_t* result);
+
+/* New (no reference counterpart): gpukit_multi_pippenger for callers that
+ * know every point lies in the prime-order subgroup G1 -- points they
+ * validated, an SRS, multiples of the generator.  The BLS12-381 sum then
+ * uses the GLV endomorphism phi(x, y) = (beta x, y) = [lambda](x, y), which
+ * holds on G1 only: half the windows over twice the points, half the
+ * buckets.  For G1 points the bytes equal gpukit_multi_pippenger's; for a
+ * curve point outside G1 the result is unspecified (use
+ * gpukit_multi_pippenger).  BN254: identical to gpukit_multi_pippenger. */
+int gpukit_multi_pippenger_subgroup(uint32_t curve, const uint8_t* scalars,
+                                    const uint8_t* points, size_t n, uint8_t* result);
 
 /* ---- EIP-4844 blobs (replaces kzg_blob_to_commit / kzg_commit_to_proof,
  * crypto.h:238-239, bodies kzg/c-abi/c_kzg_blob.cpp:26-43) ------------------ */
@@ -201,18 +214,23 @@ int kzg_server_stats(void* server, double* p50_ms, double* p99_ms, double* commi
 int kzg_server_destroy(void* server);
 
 /* ---- Allocation-free Fr NTT -------------------------------------------- */
-/* No counterpart in the reference.  For callers that cannot allocate device
- * memory (inside a CUDA graph capture, on a latency-critical path where
- * cudaMalloc's implicit device synchronisation is unacceptable, or in a
- * process whose device memory belongs to another allocator): the same
- * transform as ntt_fr_forward / ntt_fr_inverse (inverse != 0) for
- * n <= 2^16, with all scratch in a fixed 6.8 MB file-scope device array that
- * every GPU loading this library holds until exit.  Allocates nothing: no
- * cudaMalloc/cudaFree or allocating library call.  n > 2^16 returns
- * CRYPTO_ERR_LENGTH.  The first call on a device resolves the array's
- * address for that device and should come before any stream capture.  All
- * calls share the one array, so calls that overlap on the GPU (from several
- * host threads) race; callers must serialise them. */
+/* No counterpart in the reference.  ntt_fr_forward / ntt_fr_inverse grow
+ * their device scratch with cudaMalloc the first time they meet a size.
+ * Some callers cannot allow that: a process whose device memory is reserved
+ * up front by another allocator (a framework's caching pool, a fixed
+ * arena), where cudaMalloc fails or fragments that reservation, or a
+ * latency-bound service that cannot afford the device-wide waits of
+ * cudaMalloc and cudaFree.  This entry point computes the same transform
+ * (inverse != 0: ntt_fr_inverse's) for n <= 2^16 with all its scratch in
+ * one fixed 6.8 MB file-scope device array, which every GPU that loads this
+ * library holds until the process exits, and calls no cudaMalloc, cudaFree
+ * or allocating library routine.  n > 2^16 returns CRYPTO_ERR_LENGTH.  The
+ * first call on a device looks up the array's device address for that
+ * device (cudaGetSymbolAddress) and should come before any stream capture.
+ * The call is synchronous: it copies the host buffer in and out and runs
+ * its kernels on the legacy default stream.  All calls share the one
+ * array, so calls that overlap on the GPU (from several host threads) race;
+ * callers must serialise them. */
 int ntt_fr_transform_noalloc(int curve, uint8_t* coeffs32le, size_t n, int inverse, int coset);
 
 /* ---- Device-pointer entry points (inputs already resident in HBM) ------ */
@@ -221,6 +239,9 @@ int ntt_fr_transform_noalloc(int curve, uint8_t* coeffs32le, size_t n, int inver
  * synchronised.  Calls sharing a device must not overlap across streams. */
 int kb200_msm_device(uint32_t curve, const void* d_scalars, const void* d_points, size_t n,
                      void* d_result, void* stream);
+/* kb200_msm_device with the G1 promise of gpukit_multi_pippenger_subgroup. */
+int kb200_msm_device_subgroup(uint32_t curve, const void* d_scalars, const void* d_points,
+                              size_t n, void* d_result, void* stream);
 /* bls12_381_g1_msm on device memory: d_out_wire96 receives x || y (48 B BE
  * each, zeros for infinity), d_status one 32-bit word: 0 valid, 1 invalid. */
 int kb200_bls12_381_g1_msm_device(const void* d_xycs, size_t size, void* d_out_wire96,
@@ -247,13 +268,19 @@ int kb200_kzg_commit_device(void* d_evals, size_t n, void* d_commit48, void* str
 int kb200_gen_scalars(int curve, uint64_t seed, size_t n, int kind, uint8_t* out32le);
 
 /* ---- Autotuner (new) --------------------------------------------------- */
-/* Time MSM window widths and NTT radix splits for log2 sizes in
- * [log_lo, log_hi] on this GPU, keep the fastest, append them to cache_path
- * (keyed by GPU name and driver version).  Returns classes tuned or < 0. */
+/* Time, for log2 sizes in [log_lo, log_hi] on this GPU: MSM window widths
+ * around the cost model's choice (256-bit windows, and the windows of GLV
+ * halves), NTT first-pass radix splits, and -- for BLS12-381 with a
+ * resident SRS -- the shifted-table window (13, 16 or 19) of single KZG
+ * commits, which batched and served commits use per commit.  Keeps the
+ * fastest, appends them to cache_path (keyed by GPU name and driver
+ * version).  Returns size classes tuned or < 0. */
 int kb200_autotune(uint32_t curve, int log_lo, int log_hi, const char* cache_path);
 /* Apply the cached entries that match this GPU; returns entries applied. */
 int kb200_autotune_load(const char* cache_path);
-/* kind 0 = MSM window bits, 1 = NTT first-pass log radix (0 = untuned). */
+/* kind 0 = MSM window bits (256-bit windows), 1 = NTT first-pass log radix,
+ * 2 = MSM window bits of GLV halves, 3 = commit window (BLS12-381 only);
+ * 0 = untuned. */
 int kb200_tune_get(int kind, uint32_t curve, int log_n);
 void kb200_tune_set(int kind, uint32_t curve, int log_n, int value);
 
@@ -261,12 +288,16 @@ void kb200_tune_set(int kind, uint32_t curve, int log_n, int value);
 const char* kb200_last_error(void);
 /* 1 if a CUDA device is usable, else 0. */
 int kb200_device_available(void);
-/* Window size the MSM planner picks for n (for tests of the planner; for
- * BLS12-381 the window of the GLV-split 128-bit halves). */
+/* Window size the MSM planner picks for n on gpukit_multi_pippenger's path
+ * (for tests of the planner; on BN254 the window of the GLV halves), and on
+ * the G1-promise path of gpukit_multi_pippenger_subgroup (GLV halves on both
+ * curves). */
 int kb200_msm_window(uint32_t curve, size_t n);
-/* Expected bucket additions of one n-point MSM through the wire path (entries
+int kb200_msm_window_subgroup(uint32_t curve, size_t n);
+/* Expected bucket additions of one n-point MSM on those two paths (entries
  * of non-zero digits: points x populated windows x (1 - 2^-c)). */
 double kb200_msm_entries(uint32_t curve, size_t n);
+double kb200_msm_entries_subgroup(uint32_t curve, size_t n);
 /* Device self-check of the field inversion used throughout (binary GCD)
  * against the Fermat chain a^(p-2), plus x * x^-1 = 1, over `count` elements
  * (edge values, then seeded pseudo-random ones) of field 0 = BLS12-381 Fp,

@@ -877,3 +877,222 @@ int orc_kzg_blob_proof(const uint8_t* blob_be, const uint8_t z_be[32], const uin
     free(c);
     return orc_g1_compress(pt, proof48);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Seeded workload inputs, made on the CPU (test and benchmark inputs).      */
+/* ------------------------------------------------------------------------ */
+
+/* The xorshift64* streams of the library's kb200_gen_scalars (the generator
+ * family of kzg/test/kzg_gpu_determinism_test.cpp:29-36), restated so that
+ * the CPU-only legs (the reference arm of the benchmark, the golden-vector
+ * script) build the same workload without loading the CUDA library.
+ * kind 0: uniform in [0, r) by rejection sampling of 255-bit (BLS12-381) or
+ * 254-bit (BN254) draws; kind 1: 25% zero, 25% one, 20% below 2^64, 30%
+ * uniform in [0, r). */
+typedef struct { u64 x; } xs64;
+static u64 xs_next(xs64* g) {
+    g->x ^= g->x >> 12;
+    g->x ^= g->x << 25;
+    g->x ^= g->x >> 27;
+    return g->x * 0x2545F4914F6CDD1DULL;
+}
+static void xs_uniform_fr(xs64* g, const field* R, u64 mask, u64 w[4]) {
+    for (;;) {
+        for (int i = 0; i < 4; ++i) w[i] = xs_next(g);
+        w[3] &= mask;
+        fe t;
+        memset(&t, 0, sizeof t);
+        for (int i = 0; i < 4; ++i) t.l[i] = w[i];
+        if (fe_cmp(R, &t, &R->p) < 0) return;
+    }
+}
+
+int orc_gen_scalars(uint32_t curve_id, uint64_t seed, size_t n, int kind, uint8_t* out) {
+    if ((curve_id != ORC_CURVE_BN254 && curve_id != ORC_CURVE_BLS12_381) || (kind != 0 && kind != 1))
+        return -1;
+    if (!out && n) return -1;
+    const field* R = curve_id == ORC_CURVE_BLS12_381 ? &F_BLS_FR : &F_BN_FR;
+    const u64 mask = curve_id == ORC_CURVE_BLS12_381 ? 0x7FFFFFFFFFFFFFFFULL : 0x3FFFFFFFFFFFFFFFULL;
+    xs64 g = {seed ^ 0x9E3779B97F4A7C15ULL};
+    if (g.x == 0) g.x = 0x2545F4914F6CDD1DULL;
+    for (size_t i = 0; i < n; ++i) {
+        u64 w[4] = {0, 0, 0, 0};
+        if (kind == 0) {
+            xs_uniform_fr(&g, R, mask, w);
+        } else {
+            const u64 u = xs_next(&g) % 100;
+            if (u < 25) {
+            } else if (u < 50) {
+                w[0] = 1;
+            } else if (u < 70) {
+                w[0] = xs_next(&g);
+            } else {
+                xs_uniform_fr(&g, R, mask, w);
+            }
+        }
+        for (int l = 0; l < 4; ++l)
+            for (int b = 0; b < 8; ++b) out[32 * i + 8 * l + b] = (uint8_t)(w[l] >> (8 * b));
+    }
+    return 0;
+}
+
+/* Fixed-base k_i * G for many scalars: 8-bit windows over a table of
+ * d * 2^(8w) * G (d < 256, w < 32, affine Montgomery), one mixed Jacobian
+ * addition per non-zero byte, then one batched affine normalisation
+ * (Montgomery's trick) per block of outputs.  The result is the unique
+ * affine point k_i * G, so it equals every other correct route (the
+ * double-and-add of orc_g1_mul_gen, the reference ladder, the device
+ * fixed-base kernel) byte for byte. */
+#include <pthread.h>
+
+typedef struct { fe x, y; } aff;
+
+/* madd-2007-bl (Z2 = 1); equal or opposite operands fall back to the
+ * complete formulas above. */
+static jac jac_add_affine(const curve* C, jac a, const aff* q) {
+    const field* F = C->F;
+    if (a.inf) {
+        jac r = {q->x, q->y, f_one(F), 0};
+        return r;
+    }
+    fe Z1Z1 = f_sqr(F, a.Z);
+    fe U2 = f_mul(F, q->x, Z1Z1);
+    fe S2 = f_mul(F, f_mul(F, q->y, a.Z), Z1Z1);
+    fe H = f_sub(F, U2, a.X);
+    if (fe_is_zero(F, &H)) {
+        jac b = {q->x, q->y, f_one(F), 0};
+        return jac_add(C, a, b);
+    }
+    fe HH = f_sqr(F, H);
+    fe I = f_add(F, HH, HH);
+    I = f_add(F, I, I);
+    fe J = f_mul(F, H, I);
+    fe rr = f_sub(F, S2, a.Y);
+    rr = f_add(F, rr, rr);
+    fe V = f_mul(F, a.X, I);
+    fe X3 = f_sub(F, f_sub(F, f_sqr(F, rr), J), f_add(F, V, V));
+    fe Y1J = f_mul(F, a.Y, J);
+    fe Y3 = f_sub(F, f_mul(F, rr, f_sub(F, V, X3)), f_add(F, Y1J, Y1J));
+    fe Z3 = f_sub(F, f_sub(F, f_sqr(F, f_add(F, a.Z, H)), Z1Z1), HH);
+    jac out = {X3, Y3, Z3, 0};
+    return out;
+}
+
+static aff* g_fb_table[3];  /* by curve id; 32 x 256 entries (entry 0 unused) */
+static pthread_mutex_t g_fb_mu = PTHREAD_MUTEX_INITIALIZER;
+
+static void to_affine_batch(const curve* C, jac* P, size_t m, aff* out, int* inf, fe* scratch) {
+    const field* F = C->F;
+    fe acc = f_one(F);
+    for (size_t i = 0; i < m; ++i) {
+        inf[i] = P[i].inf || fe_is_zero(F, &P[i].Z);
+        scratch[i] = acc;
+        if (!inf[i]) acc = f_mul(F, acc, P[i].Z);
+    }
+    fe inv = f_inv(F, acc);
+    for (size_t i = m; i-- > 0;) {
+        if (inf[i]) continue;
+        fe zi = f_mul(F, inv, scratch[i]);
+        inv = f_mul(F, inv, P[i].Z);
+        fe zi2 = f_sqr(F, zi);
+        out[i].x = f_mul(F, P[i].X, zi2);
+        out[i].y = f_mul(F, P[i].Y, f_mul(F, zi2, zi));
+    }
+}
+
+static const aff* fixed_base_table(const curve* C, uint32_t curve_id) {
+    pthread_mutex_lock(&g_fb_mu);
+    if (!g_fb_table[curve_id]) {
+        const size_t m = 32 * 256;
+        jac* P = (jac*)calloc(m, sizeof(jac));
+        aff* T = (aff*)calloc(m, sizeof(aff));
+        int* inf = (int*)calloc(m, sizeof(int));
+        fe* scr = (fe*)calloc(m, sizeof(fe));
+        jac base = generator(C);
+        for (int w = 0; w < 32; ++w) {
+            P[w * 256] = jac_zero();
+            for (int d = 1; d < 256; ++d) P[w * 256 + d] = jac_add(C, P[w * 256 + d - 1], base);
+            for (int k = 0; k < 8; ++k) base = jac_double(C, base);
+        }
+        to_affine_batch(C, P, m, T, inf, scr);
+        free(P);
+        free(inf);
+        free(scr);
+        g_fb_table[curve_id] = T;
+    }
+    pthread_mutex_unlock(&g_fb_mu);
+    return g_fb_table[curve_id];
+}
+
+typedef struct {
+    const curve* C;
+    const aff* T;
+    const uint8_t* k;
+    uint8_t* out;
+    size_t lo, hi;
+} fb_job;
+
+static void* fb_worker(void* arg) {
+    fb_job* j = (fb_job*)arg;
+    const curve* C = j->C;
+    const field* F = C->F;
+    enum { BLK = 2048 };
+    jac* P = (jac*)malloc(BLK * sizeof(jac));
+    aff* A = (aff*)malloc(BLK * sizeof(aff));
+    int* inf = (int*)malloc(BLK * sizeof(int));
+    fe* scr = (fe*)malloc(BLK * sizeof(fe));
+    for (size_t b = j->lo; b < j->hi; b += BLK) {
+        const size_t m = (j->hi - b) < BLK ? (j->hi - b) : BLK;
+        for (size_t i = 0; i < m; ++i) {
+            const uint8_t* k = j->k + 32 * (b + i);
+            jac acc = jac_zero();
+            for (int w = 0; w < 32; ++w)
+                if (k[w]) acc = jac_add_affine(C, acc, &j->T[w * 256 + k[w]]);
+            P[i] = acc;
+        }
+        to_affine_batch(C, P, m, A, inf, scr);
+        for (size_t i = 0; i < m; ++i) {
+            uint8_t* o = j->out + (size_t)C->pt_bytes * (b + i);
+            if (inf[i]) {
+                memset(o, 0, (size_t)C->pt_bytes);
+                continue;
+            }
+            fe x = f_from_mont(F, A[i].x), y = f_from_mont(F, A[i].y);
+            fe_to_be(F, &x, o);
+            fe_to_be(F, &y, o + F->bytes);
+        }
+    }
+    free(P);
+    free(A);
+    free(inf);
+    free(scr);
+    return NULL;
+}
+
+int orc_g1_fixed_base_batch(uint32_t curve_id, const uint8_t* scalars_le, size_t n,
+                            uint8_t* out, int threads) {
+    const curve* C = curve_by_id(curve_id);
+    if (!C || ((!scalars_le || !out) && n)) return -1;
+    if (n == 0) return 0;
+    const aff* T = fixed_base_table(C, curve_id);
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    if ((size_t)threads > n) threads = (int)n;
+    pthread_t th[256];
+    fb_job jobs[256];
+    for (int t = 0; t < threads; ++t) {
+        jobs[t].C = C;
+        jobs[t].T = T;
+        jobs[t].k = scalars_le;
+        jobs[t].out = out;
+        jobs[t].lo = n * (size_t)t / (size_t)threads;
+        jobs[t].hi = n * (size_t)(t + 1) / (size_t)threads;
+        if (pthread_create(&th[t], NULL, fb_worker, &jobs[t]) != 0) {
+            fb_worker(&jobs[t]);
+            th[t] = 0;
+        }
+    }
+    for (int t = 0; t < threads; ++t)
+        if (th[t]) pthread_join(th[t], NULL);
+    return 0;
+}

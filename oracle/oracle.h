@@ -116,6 +116,15 @@ int orc_kzg_blob_proof(const uint8_t* blob_be, const uint8_t z_be[32], const uin
 int orc_word_ntt_forward(uint64_t* a, size_t n, uint64_t q, uint64_t root);
 int orc_word_ntt_inverse(uint64_t* a, size_t n, uint64_t q, uint64_t root_inv);
 
+/* Seeded scalars with the contract of the library's kb200_gen_scalars
+ * (xorshift64*; kind 0 uniform in [0, r), 1 skewed), restated so CPU-only
+ * code builds the same workload.  32 B LE each. */
+int orc_gen_scalars(uint32_t curve, uint64_t seed, size_t n, int kind, uint8_t* out);
+/* out[i] = k_i * G (BE affine, all-zero for infinity) for n scalars k_i
+ * (32 B LE), fixed-base 8-bit windows, `threads` POSIX threads. */
+int orc_g1_fixed_base_batch(uint32_t curve, const uint8_t* scalars_le, size_t n,
+                            uint8_t* out, int threads);
+
 #ifdef __cplusplus
 }
 #endif

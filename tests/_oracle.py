@@ -51,12 +51,33 @@ def orc() -> ctypes.CDLL:
                                    ctypes.c_void_p],
             "orc_word_ntt_forward": [ctypes.c_void_p, sz, ctypes.c_uint64, ctypes.c_uint64],
             "orc_word_ntt_inverse": [ctypes.c_void_p, sz, ctypes.c_uint64, ctypes.c_uint64],
+            "orc_gen_scalars": [ctypes.c_uint32, ctypes.c_uint64, sz, ctypes.c_int, ctypes.c_void_p],
+            "orc_g1_fixed_base_batch": [ctypes.c_uint32, ctypes.c_void_p, sz, ctypes.c_void_p,
+                                        ctypes.c_int],
         }.items():
             f = getattr(L, name)
             f.restype = ctypes.c_int
             f.argtypes = args
         _orc = L
     return _orc
+
+
+def gen_scalars(curve: int, seed: int, n: int, kind: int = 0) -> bytes:
+    """The library's seeded scalar streams (kb200_gen_scalars), made on the CPU."""
+    out = ctypes.create_string_buffer(32 * n)
+    assert orc().orc_gen_scalars(curve, seed, n, kind, out) == 0
+    return out.raw
+
+
+def fixed_base_points(curve: int, scalars: bytes, threads: int = 0) -> bytes:
+    """k_i * G for every 32-byte LE scalar k_i (CPU, fixed-base windows)."""
+    import os
+    n = len(scalars) // 32
+    out = ctypes.create_string_buffer(PB[curve] * n)
+    src = ctypes.create_string_buffer(bytes(scalars), len(scalars))
+    rc = orc().orc_g1_fixed_base_batch(curve, src, n, out, threads or (os.cpu_count() or 1))
+    assert rc == 0, rc
+    return out.raw
 
 
 def ref_available() -> bool:

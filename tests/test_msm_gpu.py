@@ -41,17 +41,70 @@ def rand_points(curve: int, n: int, seed: int) -> bytes:
     return pts
 
 
-def test_golden_vectors(cuda_lib):
+# The drop-in (exact for every curve point) and the G1-promise entry point
+# (GLV split on BLS12-381); every input below is in G1 unless a test says
+# otherwise, so both must give the reference's bytes.
+PATHS = ["plain", "subgroup"]
+
+
+def msm(path: str, curve: int, scalars: bytes, points: bytes, n: int) -> bytes:
+    if path == "subgroup":
+        return kb().gpukit_multi_pippenger_subgroup(curve, scalars, points, n)
+    return kb().gpukit_multi_pippenger(curve, scalars, points, n)
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_golden_vectors(cuda_lib, path):
     with gzip.open(GOLDEN, "rt") as f:
         cases = json.load(f)["msm"]
     for c in cases:
-        got = kb().gpukit_multi_pippenger(c["curve"], bytes.fromhex(c["scalars"]),
-                                          bytes.fromhex(c["points"]), c["n"])
+        got = msm(path, c["curve"], bytes.fromhex(c["scalars"]), bytes.fromhex(c["points"]), c["n"])
         assert got.hex() == c["expected"], (c["curve"], c["n"], c["mode"])
 
 
+@pytest.mark.parametrize("curve,n,frac", [(2, 97, 2), (2, 3000, 3), (2, 1 << 17, 16), (1, 3000, 3)])
+def test_points_outside_g1_match_reference(cuda_lib, curve, n, frac):
+    """The reference reads any affine curve point with no subgroup check
+    (gpukit/curve_traits/bls12_381_g1_first_party_traits.h:58-69), so its
+    sum is defined for BLS12-381 points outside G1 too.  The drop-in must
+    give its bytes for them: G1 points shifted by points of cofactor order,
+    random curve points and pure torsion points, one in `frac` of the
+    inputs, at a size with a reference window of 4 or 8 (full 256-bit
+    scalars), a mid size and one large enough for the pairing levels.  The
+    G1-promise entry point's GLV split is wrong there, which shows the
+    drop-in does not take it.  (BN254 has cofactor 1: every point is in G1.)"""
+    import _eip2537 as E
+    rng = random.Random(n)
+    pb = O.PB[curve]
+    pts = bytearray(rand_points(curve, n, seed=300 + n))
+    if curve == 2:
+        tors = [E.torsion_point(rng) for _ in range(4)]
+        odd = [E.curve_point_not_in_g1(rng) for _ in range(4)]
+        for i in range(0, n, frac):
+            kind = rng.randrange(3)
+            if kind == 0:
+                q = O.g1_add(2, bytes(pts[pb * i:pb * (i + 1)]), tors[rng.randrange(4)])
+            elif kind == 1:
+                q = odd[rng.randrange(4)]
+            else:
+                q = tors[rng.randrange(4)]
+            pts[pb * i:pb * (i + 1)] = q
+    pts = bytes(pts)
+    full = n < 128
+    S = b"".join((rng.getrandbits(256) if full else rng.randrange(O.FR[curve])).to_bytes(32, "little")
+                 for _ in range(n))
+    want = O.ref_msm(curve, S, pts, n, threads=16) if O.ref_available() else O.msm(curve, S, pts, n)
+    if n <= 4096:
+        assert O.msm(curve, S, pts, n) == want
+    assert kb().gpukit_multi_pippenger(curve, S, pts, n) == want
+    assert kb().gpukit_multi_pippenger_cuda(curve, S, pts, n) == want
+    if curve == 2:
+        assert kb().gpukit_multi_pippenger_subgroup(curve, S, pts, n) != want
+
+
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("curve", [1, 2])
-def test_reference_harness_sizes(cuda_lib, curve):
+def test_reference_harness_sizes(cuda_lib, curve, path):
     """Sizes of gpukit/test/multi_pippenger_test.cpp:37 with its scalar mask."""
     rng = random.Random(100 + curve)
     pts_all = rand_points(curve, 4096, seed=31 + curve)
@@ -61,11 +114,12 @@ def test_reference_harness_sizes(cuda_lib, curve):
         scs = b"".join((rng.getrandbits(256) & ((1 << 252) - 1)).to_bytes(32, "little")
                        for _ in range(n))
         want = O.ref_msm(curve, scs, pts, n, threads=8) if O.ref_available() else O.msm(curve, scs, pts, n)
-        assert kb().gpukit_multi_pippenger(curve, scs, pts, n) == want, n
+        assert msm(path, curve, scs, pts, n) == want, n
 
 
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("curve", [1, 2])
-def test_full_range_scalars_reproduce_reference_carry(cuda_lib, curve):
+def test_full_range_scalars_reproduce_reference_carry(cuda_lib, curve, path):
     """Scalars >= 2^255 at sizes whose reference window is 4 or 8 bits."""
     rng = random.Random(9)
     pts_all = rand_points(curve, 1500, seed=77)
@@ -73,11 +127,12 @@ def test_full_range_scalars_reproduce_reference_carry(cuda_lib, curve):
     for n in (2, 8, 9, 700, 1500):
         pts = pts_all[:pb * n]
         scs = b"".join(rng.getrandbits(256).to_bytes(32, "little") for _ in range(n))
-        assert kb().gpukit_multi_pippenger(curve, scs, pts, n) == O.msm(curve, scs, pts, n), n
+        assert msm(path, curve, scs, pts, n) == O.msm(curve, scs, pts, n), n
 
 
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("curve", [1, 2])
-def test_edge_cases(cuda_lib, curve):
+def test_edge_cases(cuda_lib, curve, path):
     pb = O.PB[curve]
     r = O.FR[curve]
     g = O.g1_mul_gen(curve, 1)
@@ -97,7 +152,7 @@ def test_edge_cases(cuda_lib, curve):
     for pts, scs in cases:
         P = b"".join(pts)
         S = b"".join(s.to_bytes(32, "little") for s in scs)
-        assert kb().gpukit_multi_pippenger(curve, S, P, len(pts)) == O.msm(curve, S, P, len(pts))
+        assert msm(path, curve, S, P, len(pts)) == O.msm(curve, S, P, len(pts))
 
 
 def test_n_zero_and_errors(cuda_lib):
@@ -110,25 +165,33 @@ def test_n_zero_and_errors(cuda_lib):
     assert k.msm_rc(0, b"\0" * 32, b"\0" * 64, 1, out) == -5   # secp256k1: NOTIMPL
     assert k.msm_rc(3, b"\0" * 32, b"\0" * 64, 1, out) == -5   # banderwagon: NOTIMPL
     assert k.msm_rc(9, b"\0" * 32, b"\0" * 64, 1, out) == -3   # unknown: BACKEND
+    L = k.lib()
+    assert L.gpukit_multi_pippenger_subgroup(2, None, None, 0, out) == 0
+    assert out.raw == bytes(96)
+    assert L.gpukit_multi_pippenger_subgroup(2, None, None, 1, out) == -1
+    assert L.gpukit_multi_pippenger_subgroup(0, b"\0" * 32, b"\0" * 64, 1, out) == -5
+    assert L.gpukit_multi_pippenger_subgroup(9, b"\0" * 32, b"\0" * 64, 1, out) == -3
 
 
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("curve", [1, 2])
-def test_skewed_scalars(cuda_lib, curve):
+def test_skewed_scalars(cuda_lib, curve, path):
     """50% of scalars in {0,1}, 20% below 2^64, rest uniform (bucket imbalance)."""
     n = 1 << 14
     pts = rand_points(curve, n, seed=5)
     scs = kb().gen_scalars(curve, 1234, n, kind=1)
     want = O.ref_msm(curve, scs, pts, n, threads=8) if O.ref_available() else O.msm(curve, scs, pts, n)
-    assert kb().gpukit_multi_pippenger(curve, scs, pts, n) == want
+    assert msm(path, curve, scs, pts, n) == want
 
 
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("curve", [1, 2])
-def test_2_16_against_reference(cuda_lib, curve):
+def test_2_16_against_reference(cuda_lib, curve, path):
     n = 1 << 16
     pts = rand_points(curve, n, seed=8)
     scs = kb().gen_scalars(curve, 4321, n)
     want = O.ref_msm(curve, scs, pts, n, threads=8) if O.ref_available() else O.msm(curve, scs, pts, n)
-    assert kb().gpukit_multi_pippenger(curve, scs, pts, n) == want
+    assert msm(path, curve, scs, pts, n) == want
 
 
 @pytest.mark.parametrize("curve", [1, 2])
@@ -154,8 +217,9 @@ def test_linearity_large(cuda_lib, curve):
     assert O.g1_add(curve, lo, hi) == a
 
 
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("curve,logn,bits", [(1, 20, 10), (2, 18, 8)])
-def test_many_big_buckets(cuda_lib, curve, logn, bits):
+def test_many_big_buckets(cuda_lib, curve, logn, bits, path):
     """Small scalars over many points: every bucket of window 0 holds
     thousands of entries, so thousands of buckets take the fold path."""
     n = 1 << logn
@@ -163,7 +227,7 @@ def test_many_big_buckets(cuda_lib, curve, logn, bits):
     rng = random.Random(logn)
     scs = b"".join(rng.getrandbits(bits).to_bytes(32, "little") for _ in range(n))
     want = O.ref_msm(curve, scs, pts, n, threads=16) if O.ref_available() else O.msm(curve, scs, pts, n)
-    assert kb().gpukit_multi_pippenger(curve, scs, pts, n) == want
+    assert msm(path, curve, scs, pts, n) == want
 
 
 def test_glv_halves_share_a_bucket(cuda_lib):
@@ -180,7 +244,38 @@ def test_glv_halves_share_a_bucket(cuda_lib):
         scs.append(((a + a * lam) % O.FR[2]).to_bytes(32, "little"))
     S = b"".join(scs)
     want = O.ref_msm(2, S, pts, n, threads=16) if O.ref_available() else O.msm(2, S, pts, n)
+    assert kb().gpukit_multi_pippenger_subgroup(2, S, pts, n) == want
     assert kb().gpukit_multi_pippenger(2, S, pts, n) == want
+
+
+def test_bn254_glv_halves_signs_and_bounds(cuda_lib):
+    """BN254 splits every scalar as k = k1 + k2 lambda with signed halves
+    (Babai rounding).  Scalars near the rounding boundaries of the split --
+    k = round(j r / b) for the basis entries b, their neighbours, multiples
+    of lambda and the range ends -- give the reference's bytes."""
+    r = O.FR[1]
+    lam = 0xB3C4D79D41A917585BFC41088D8DAAA78B17EA66B99C90DD
+    b1 = 0x6F4D8248EEB859FC8211BBEB7D4F1128
+    b2 = 0x89D3256894D213E3
+    ks = {0, 1, 2, r - 1, r - 2, lam, lam - 1, lam + 1, (r - 1) // 2, (r + 1) // 2}
+    rng = random.Random(254)
+    for b in (b1, b2):
+        for _ in range(300):
+            j = rng.randrange(1, b)
+            c = (2 * j + 1) * r // (2 * b)  # k b / r just below / above j + 1/2
+            ks.update({c % r, (c + 1) % r, (c - 1) % r})
+    for _ in range(100):
+        ks.add(rng.randrange(1, 1 << 64) * lam % r)
+    ks = sorted(ks)
+    n = len(ks)
+    pts = rand_points(1, n, seed=254)
+    S = b"".join(k.to_bytes(32, "little") for k in ks)
+    want = O.ref_msm(1, S, pts, n, threads=8) if O.ref_available() else O.msm(1, S, pts, n)
+    assert kb().gpukit_multi_pippenger(1, S, pts, n) == want
+    # a sample of the scalars alone (n = 1: a single point per MSM)
+    for i in range(0, n, 97):
+        assert kb().gpukit_multi_pippenger(1, S[32 * i:32 * i + 32], pts[64 * i:64 * i + 64], 1) == \
+            O.msm(1, S[32 * i:32 * i + 32], pts[64 * i:64 * i + 64], 1)
 
 
 @pytest.mark.parametrize("levels", [1, 4])
@@ -209,7 +304,9 @@ for curve, n in ((2, 1 << 13), (1, 1 << 13)):
         pts.append(p)
         scs.append(rng.choice((1, 2, 3, 7, 1 << 70)).to_bytes(32, "little"))
     P, S = b"".join(pts), b"".join(scs)
-    assert kb.gpukit_multi_pippenger(curve, S, P, n) == O.msm(curve, S, P, n), curve
+    want = O.msm(curve, S, P, n)
+    assert kb.gpukit_multi_pippenger(curve, S, P, n) == want, curve
+    assert kb.gpukit_multi_pippenger_subgroup(curve, S, P, n) == want, curve
 print("ok")
 '''
     env = dict(os.environ, KB200_MSM_PAIR_LEVELS=str(levels))
@@ -219,8 +316,9 @@ print("ok")
     assert out.returncode == 0 and "ok" in out.stdout, out.stdout + out.stderr
 
 
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("curve,logn", [(2, 20), (1, 17), (1, 20)])
-def test_host_pipeline_with_infinity_points(cuda_lib, curve, logn):
+def test_host_pipeline_with_infinity_points(cuda_lib, curve, logn, path):
     """gpukit_multi_pippenger overlaps the point copy with the recode and
     sort (chunked copies, conversion per chunk), so infinity points reach
     the buckets and are skipped there: one point in eight is the identity,
@@ -236,7 +334,7 @@ def test_host_pipeline_with_infinity_points(cuda_lib, curve, logn):
     pts = bytes(pts)
     S = b"".join(rng.randrange(O.FR[curve]).to_bytes(32, "little") for _ in range(n))
     want = O.ref_msm(curve, S, pts, n, threads=16) if O.ref_available() else O.msm(curve, S, pts, n)
-    assert kb().gpukit_multi_pippenger(curve, S, pts, n) == want
+    assert msm(path, curve, S, pts, n) == want
 
 
 @pytest.mark.parametrize("curve", [1, 2])
@@ -260,11 +358,12 @@ def test_device_entry_aligned_and_unaligned_points(cuda_lib, curve):
     for shift in (0, 1):
         buf = torch.zeros(n * pb + 16, dtype=torch.uint8, device="cuda")
         buf[shift:shift + n * pb] = torch.frombuffer(bytearray(pts), dtype=torch.uint8).cuda()
-        rc = kb().lib().kb200_msm_device(curve, d_sc.data_ptr(), buf.data_ptr() + shift, n,
-                                         d_out.data_ptr(), None)
-        assert rc == 0, kb().last_error()
-        torch.cuda.synchronize()
-        assert bytes(d_out.cpu().numpy().tobytes()) == want, shift
+        for fn in (kb().lib().kb200_msm_device, kb().lib().kb200_msm_device_subgroup):
+            d_out.zero_()
+            rc = fn(curve, d_sc.data_ptr(), buf.data_ptr() + shift, n, d_out.data_ptr(), None)
+            assert rc == 0, kb().last_error()
+            torch.cuda.synchronize()
+            assert bytes(d_out.cpu().numpy().tobytes()) == want, shift
 
 
 @pytest.mark.parametrize("quad,curve,logn", [(1, 2, 20), (1, 1, 17), (0, 2, 12), (0, 1, 14)])

@@ -61,6 +61,6 @@ def test_reference_arm_runs_on_rank_zero_only(capsys):
     import argparse
 
     import bench
-    args = argparse.Namespace(ref_logn=10, steps=1, warmup=0, gpus=2)
+    args = argparse.Namespace(logn=10, steps=1, warmup=0, gpus=2)
     assert bench.run_reference(args, 2, 1) is None
     assert capsys.readouterr().out == ""

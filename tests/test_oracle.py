@@ -121,3 +121,23 @@ def test_points_on_curve():
     for curve in (1, 2):
         assert O.on_curve(curve, O.g1_mul_gen(curve, 12345))
         assert O.on_curve(curve, bytes(O.PB[curve]))
+
+
+@pytest.mark.parametrize("curve", [1, 2])
+def test_cpu_input_generators_match_library(curve):
+    """The CPU-only legs (reference arm, golden script) rebuild the workload
+    with the oracle's restated generators: the same scalar streams as the
+    library's kb200_gen_scalars, and fixed-base points equal to the
+    double-and-add k * G of the oracle."""
+    import crypto_b200 as kb
+    for kind in (0, 1):
+        for seed in (1, 55, 1001):
+            assert O.gen_scalars(curve, seed, 3000, kind) == kb.gen_scalars(curve, seed, 3000, kind)
+    sc = O.gen_scalars(curve, 5, 200)
+    edge = [0, 1, 2, 255, 256, 1 << 248, O.FR[curve] - 1, (1 << 254) - 1]
+    sc += b"".join(k.to_bytes(32, "little") for k in edge)
+    pts = O.fixed_base_points(curve, sc, threads=3)
+    pb = O.PB[curve]
+    for i in range(len(sc) // 32):
+        k = int.from_bytes(sc[32 * i:32 * i + 32], "little")
+        assert pts[pb * i:pb * (i + 1)] == O.g1_mul_gen(curve, k), i
