@@ -412,9 +412,20 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
     // at most RED_THREADS stage-1 blocks.  Measured stage-1 times, one block
     // per SM against two: BLS12-381 2^22 (273 K buckets) 1.43 / 1.75 ms,
     // BN254 2^24 1.43 / 1.53 ms; 2^18 (41 K buckets) 1.15 / 0.99 ms.
+    // Many buckets (>= 12 per thread at one block per SM, e.g. the 524 K of
+    // a BLS12-381 2^22 MSM with 16-bit windows over 256-bit scalars) run two
+    // blocks per SM as well: the serial additions then hide each other's
+    // latency (stage 1 2.65 -> 2.50 ms there; at 983 K buckets 4.26 -> 3.87
+    // ms; at 262 K, 7 per thread, one block stays faster, 2.02 vs 2.18 ms).
+    // KB200_MSM_RED_BPS forces the blocks per SM.
+    static const int env_red_bps = [] {
+        const char* v = std::getenv("KB200_MSM_RED_BPS");
+        return v && *v ? std::atoi(v) : 0;
+    }();
     const size_t per_sm = (size_t)device_sms() * RED_THREADS;
     size_t s_one = (total_live + per_sm - 1) / per_sm;
-    if (s_one < 4) s_one = (total_live + 2 * per_sm - 1) / (2 * per_sm);
+    if (s_one < 4 || s_one >= 12) s_one = (total_live + 2 * per_sm - 1) / (2 * per_sm);
+    if (env_red_bps > 0) s_one = (total_live + env_red_bps * per_sm - 1) / (env_red_bps * per_sm);
     const uint32_t S0 = (uint32_t)std::min<size_t>(64, std::max<size_t>(1, s_one));
     // Few buckets (KZG commits up to 2^16, blobs): the reduction is bound by
     // the latency of its serial additions, not by throughput, so it runs one

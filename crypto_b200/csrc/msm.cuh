@@ -38,12 +38,14 @@ namespace kb200 {
 // model does not see; window choices were checked against measured times.)
 constexpr double RED_COST = 2.8;
 // The same weight once the batch-affine pairing levels run (from about 2^22
-// sorted entries: a level needs 2M pair sums): entries cost less than a mixed addition, so a bucket
-// weighs more.  Fitted on B200: reduction 1.0 ms + 3.0 ns per bucket against
-// 0.40 ns per sorted entry (BLS12-381 GLV at 2^22, windows 16-19: 16 wins,
-// 33.5 ms against 35.0 ms for 19; BN254 at 2^24, windows 17-21: 17 wins,
-// 64.0 / 30.8 ms uniform / skewed against 67.3 / 36.4 ms for 20).
-constexpr double RED_COST_PAIRED = 7.5;
+// sorted entries: a level needs 2M pair sums): entries cost less than a
+// mixed addition, so a bucket weighs more.  Fitted on B200: BLS12-381 at
+// 2^22 over 256-bit windows (the exact drop-in) takes 28.57 / 30.03 / 29.34
+// ms at windows 16 / 17 / 15 (reduction 3.9 ms at 524 K buckets, 5.5 ms at
+// 983 K), which needs a weight between 9.1 and 17; the GLV halves at 2^22
+// keep window 16 (27.2 ms) for any weight above 5.3, BN254 GLV at 2^24
+// window 18.
+constexpr double RED_COST_PAIRED = 12.0;
 constexpr double PAIRED_ENTRIES = (double)(1u << 22);
 
 struct MsmPlan {

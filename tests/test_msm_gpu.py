@@ -93,11 +93,21 @@ def test_points_outside_g1_match_reference(cuda_lib, curve, n, frac):
     full = n < 128
     S = b"".join((rng.getrandbits(256) if full else rng.randrange(O.FR[curve])).to_bytes(32, "little")
                  for _ in range(n))
-    want = O.ref_msm(curve, S, pts, n, threads=16) if O.ref_available() else O.msm(curve, S, pts, n)
-    if n <= 4096:
+    # one reference call below 2^12 points: with full 256-bit scalars its
+    # dropped top carry depends on the window it picks for n, so slicing the
+    # input (ref_msm_parallel) would change the bytes; above, the scalars are
+    # canonical and the sliced run is exact
+    if not O.ref_available():
+        want = O.msm(curve, S, pts, n)
+    elif n <= 4096:
+        want = O.ref_msm(curve, S, pts, n)
         assert O.msm(curve, S, pts, n) == want
+    else:
+        want = O.ref_msm(curve, S, pts, n, threads=16)
     assert kb().gpukit_multi_pippenger(curve, S, pts, n) == want
-    assert kb().gpukit_multi_pippenger_cuda(curve, S, pts, n) == want
+    out = ctypes.create_string_buffer(O.PB[curve])
+    assert kb().lib().gpukit_multi_pippenger_cuda(curve, S, pts, n, out) == 0
+    assert out.raw == want
     if curve == 2:
         assert kb().gpukit_multi_pippenger_subgroup(curve, S, pts, n) != want
 
