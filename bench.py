@@ -674,12 +674,13 @@ def run_ours(args, ws, rank, local):
     # sum of the same workload from the reference CPU MSM) and each other
     want = golden_expected(args.logn) if rank == 0 else None
     sums = {}
-    for path in (other, head):
+    for path in ((head,) if args.single_path else (other, head)):
         for _ in range(args.warmup):
             run(path)
         torch.cuda.synchronize()
         sums[path] = d_out.cpu().numpy().tobytes()
-    assert sums["plain"] == sums["subgroup"], "the two MSM paths disagree"
+    if not args.single_path:
+        assert sums["plain"] == sums["subgroup"], "the two MSM paths disagree"
     parity = {"reference_sum_equal": (sums[head].hex() == want) if want else None,
               "against": "reference CPU MSM of this workload (tests/golden/large.json)"}
     if want:
@@ -764,16 +765,18 @@ def run_ours(args, ws, rank, local):
         return roof, whole
 
     roofline, msm_roof = rooflines(head, stage, ms)
-    # the other path, same protocol (device time, then e2e)
-    o_ms, _, o_stage, _ = timed(other, args.steps, False)
-    o_e2e = e2e(other)
-    o_roof, o_whole = rooflines(other, o_stage, o_ms)
-    other_line = {"path": other, "value": n * ws / (o_ms / 1e3) / 1e6, "unit": "Mpts/s", "ms_per_step": o_ms,
-                  "window_bits": kb.msm_window(CURVE, n, subgroup=(other == "subgroup")),
-                  "e2e": {"value": n * ws / (o_e2e / 1e3) / 1e6, "unit": "Mpts/s", "ms_per_step": o_e2e,
-                          "api": host_fn[other].__name__},
-                  "roofline_frac": o_roof["frac"] if o_roof else None, "msm_roofline_frac": o_whole["frac"],
-                  "stage_ms": o_stage}
+    other_line = None
+    if not args.single_path:
+        # the other path, same protocol (device time, then e2e)
+        o_ms, _, o_stage, _ = timed(other, args.steps, False)
+        o_e2e = e2e(other)
+        o_roof, o_whole = rooflines(other, o_stage, o_ms)
+        other_line = {"path": other, "value": n * ws / (o_ms / 1e3) / 1e6, "unit": "Mpts/s",
+                      "ms_per_step": o_ms, "window_bits": kb.msm_window(CURVE, n, subgroup=(other == "subgroup")),
+                      "e2e": {"value": n * ws / (o_e2e / 1e3) / 1e6, "unit": "Mpts/s", "ms_per_step": o_e2e,
+                              "api": host_fn[other].__name__},
+                      "roofline_frac": o_roof["frac"] if o_roof else None,
+                      "msm_roofline_frac": o_whole["frac"], "stage_ms": o_stage}
 
     extra = None
     if rank == 0 and not args.no_extra:
@@ -856,6 +859,8 @@ def main():
                     help="headline MSM entry point: plain (exact for every point) or subgroup (GLV)")
     ap.add_argument("--ntt-curve", type=int, default=CURVE, choices=[1, 2], help="--case ntt: curve")
     ap.add_argument("--coset", action="store_true", help="--case ntt: coset transform")
+    ap.add_argument("--single-path", action="store_true",
+                    help="time only the --path entry point (profiling runs)")
     ap.add_argument("--commits", type=int, default=512)
     ap.add_argument("--serve-rates", type=float, nargs="*",
                     default=[100.0, 200.0, 400.0, 800.0, 1200.0, 1600.0, 2400.0])

@@ -692,22 +692,6 @@ __device__ __forceinline__ void pair_den(const PairArgs& a, uint32_t k, uint32_t
     if (fe_eq(y0, y1) && !fe_is_zero(y0)) fe_dbl(den, y0);
 }
 
-#ifndef KB_PAIR_PREFETCH
-#define KB_PAIR_PREFETCH 0
-#endif
-// L2 prefetch of slot k's two input rows (bucket b holds slot k).
-template <class F>
-__device__ __forceinline__ void pair_prefetch(const PairArgs& a, uint32_t k, uint32_t b) {
-    const uint32_t i0 = a.in_off[b] + 2 * (k - a.out_off[b]);
-    bool n;
-    const uint32_t* r0 = pair_row<F>(a, i0, n);
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(r0));
-    if (i0 + 1 < a.in_off[b + 1]) {
-        const uint32_t* r1 = pair_row<F>(a, i0 + 1, n);
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(r1));
-    }
-}
-
 template <class C>
 __global__ void __launch_bounds__(256) k_pair_fwd(PairArgs a, uint32_t T, uint32_t* __restrict__ pre,
                                                   uint32_t* __restrict__ tot) {
@@ -723,13 +707,6 @@ __global__ void __launch_bounds__(256) k_pair_fwd(PairArgs a, uint32_t T, uint32
         uint32_t b = bucket_of(a.out_off, a.B, k0);
         for (uint32_t k = k0; k < kend; ++k) {
             while (a.out_off[b + 1] <= k) ++b;
-#if KB_PAIR_PREFETCH
-            if (k + 1 < kend) {
-                uint32_t bn = b;
-                while (a.out_off[bn + 1] <= k + 1) ++bn;
-                pair_prefetch<F>(a, k + 1, bn);
-            }
-#endif
             Fe<F> den;
             pair_den<F>(a, k, b, den);
             fe_mul(run, run, den);
@@ -756,13 +733,6 @@ __global__ void __launch_bounds__(256, 2) k_pair_bwd(PairArgs a, uint32_t T, con
     for (int j = (int)(kend - k0) - 1; j >= 0; --j) {
         const uint32_t k = k0 + (uint32_t)j;
         while (a.out_off[bend] > k) --bend;
-#if KB_PAIR_PREFETCH
-        if (j > 0) {
-            uint32_t bp = bend;
-            while (a.out_off[bp] > k - 1) --bp;
-            pair_prefetch<F>(a, k - 1, bp);
-        }
-#endif
         Affine<F> P0, P1;
         bool inf0;
         Fe<F> den, inv;
