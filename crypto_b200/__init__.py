@@ -81,6 +81,7 @@ def lib() -> ctypes.CDLL:
             "kb200_msm_window": (c.c_int, [c.c_uint32, sz]),
             "kb200_msm_entries": (c.c_double, [c.c_uint32, sz]),
             "kb200_field_inverse_check": (c.c_int, [c.c_int, c.c_uint64, sz, c.POINTER(c.c_ulonglong)]),
+            "kb200_field_mul_check": (c.c_int, [c.c_int, u8p, u8p, sz, vp, vp, c.POINTER(c.c_ulonglong)]),
             "kb200_launch_count": (c.c_ulonglong, []),
             "kzg_server_create": (vp, [sz, c.c_int, sz]),
             "kzg_server_submit": (c.c_int, [vp, u8p, sz, c.POINTER(c.c_uint64)]),

@@ -239,6 +239,9 @@ KB_DEV void reduce_once(Fe<F>& r, const uint32_t* t) {
     for (int i = 0; i < N; ++i) r.v[i] = borrow ? t[i] : d[i];
 }
 
+template <class F>
+KB_DEV void mont_reduce_wide(Fe<F>& r, uint32_t* T);
+
 // r = a * b * R^-1 mod p, inputs and output in [0, p).
 //
 // The double-width product T = a * b uses one level of Karatsuba on the
@@ -296,6 +299,18 @@ KB_DEV void fe_mul_ks_inl(Fe<F>& r, const Fe<F>& a, const Fe<F>& b) {
     for (int k = 1; k <= N; ++k) T[H + k] = addc_cc(T[H + k], M[k]);
 #pragma unroll
     for (int k = H + N + 1; k < 2 * N; ++k) T[k] = addc_cc(T[k], 0);
+    mont_reduce_wide<F>(r, T);
+}
+
+// r = T * 2^(-32N) mod p for a double-width T < p 2^(32N) (2N words, T is
+// consumed): word-serial Montgomery reduction; row i adds m_i p at word i,
+// m_i = T[i] (-p^-1 mod 2^32), as two carry chains whose final carries pc
+// are kept aside and added to the upper half at the end, so no carry has to
+// ripple through T row by row.  (T + m p) / 2^(32N) < 2p, then one
+// conditional subtraction.
+template <class F>
+KB_DEV void mont_reduce_wide(Fe<F>& r, uint32_t* T) {
+    constexpr int N = F::N;
     // reduction rows; pc[k] collects the chains' carries into word N + k
     uint32_t pc[N + 1];
 #pragma unroll
@@ -329,6 +344,7 @@ KB_DEV void fe_mul_ks_inl(Fe<F>& r, const Fe<F>& a, const Fe<F>& b) {
     for (int k = 1; k < N; ++k) U[k] = addc_cc(T[N + k], pc[k]);
     reduce_once<F>(r, U);
 }
+
 
 // r = a * b * R^-1 mod p in the interleaved (CIOS) form: for each word b_i,
 // the row a b_i and the reduction row m p (m = t_0 (-p^-1) mod 2^32) are

@@ -304,6 +304,15 @@ double kb200_msm_entries_subgroup(uint32_t curve, size_t n);
  * 1 = BLS12-381 Fr, 2 = BN254 Fp, 3 = BN254 Fr.  *mismatches receives the
  * number of failing elements.  Diagnostic: no reference counterpart. */
 int kb200_field_inverse_check(int field, uint64_t seed, size_t count, unsigned long long* mismatches);
+/* Device products of n canonical little-endian elements of the same fields
+ * (48 B for BLS12-381 Fp, 32 B otherwise): out_mul[i] = a[i] * b[i] and
+ * out_sqr[i] = a[i]^2, computed in Montgomery form by the Karatsuba product
+ * and squaring every kernel uses; *form_mismatches counts elements where the
+ * interleaved (CIOS) product disagrees.  Diagnostic: no reference
+ * counterpart. */
+int kb200_field_mul_check(int field, const uint8_t* a_le, const uint8_t* b_le, size_t n,
+                          uint8_t* out_mul_le, uint8_t* out_sqr_le,
+                          unsigned long long* form_mismatches);
 /* Number of this library's kernel launches since load. */
 unsigned long long kb200_launch_count(void);
 /* Per-stage CUDA-event timing of MSMs (off by default). */

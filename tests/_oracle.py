@@ -234,3 +234,11 @@ FR = {2: 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001,
       1: 21888242871839275222246405745257275088548364400416034343698204186575808495617}
 FP = {2: 0x1A0111EA397FE69A4B1BA7B6434BACD764774B84F38512BF6730D2A0F6B0F6241EABFFFEB153FFFFB9FEFFFFFFFFAAAB,
       1: 21888242871839275222246405745257275088696311157297823662689037894645226208583}
+
+
+def field_mul(which: int, a: bytes, b: bytes) -> bytes:
+    """Canonical a * b in field `which` (0 BLS12-381 Fp, 1 BLS12-381 Fr,
+    2 BN254 Fp, 3 BN254 Fr), little-endian bytes of the field's width."""
+    out = ctypes.create_string_buffer(len(a))
+    assert orc().orc_field_mul(which, a, b, out) == 0
+    return out.raw
