@@ -1269,7 +1269,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_windows(RedArgs a) {
         }
         __syncwarp();
         sm_load(V, sA, 0);
-        for (uint32_t k = 0; k < wd.shift; ++k) xyzz_dbl_warp(V);
+        // an empty window (the carry window of 256-bit windows is empty for
+        // scalars below 2^255) skips its chain: it would be the longest
+        if (!xyzz_is_inf(V))
+            for (uint32_t k = 0; k < wd.shift; ++k) xyzz_dbl_warp(V);
         if (t == 0) xyzz_store(a.win_out + (size_t)blockIdx.x * PW, V);
     }
 }
