@@ -442,11 +442,34 @@ def bench_batched_commits(args) -> dict:
     """512 BLS12-381 commits, sizes log-uniform over 2^8..2^16 (powers of
     two), uniform Fr evaluations, one resident 2^16 SRS: the batched pass
     (grouped iNTTs + one batched MSM, CUDA graph) against 512 sequential
-    plain kzg_commit_fr calls on the same GPU, byte-equal."""
+    plain kzg_commit_fr calls on the same GPU, byte-equal.  The autotuner
+    first times the candidate commit windows, MSM windows and NTT radix
+    splits of every size class on this GPU (kb200_autotune), writes its
+    cache, and the run loads it (kb200_autotune_load): both forms then use
+    the tuned choices, reported under "autotune"."""
     import random
     import crypto_b200 as kb
+    L = kb.lib()
     rng = random.Random(4096)
     sizes = [1 << rng.randint(8, 16) for _ in range(args.commits)]
+    kb.kzg_srs_generate(_tau(7), 1 << 16)
+    fd, cache = tempfile.mkstemp(suffix=".tune")
+    os.close(fd)
+    t0 = time.perf_counter()
+    tuned = L.kb200_autotune(CURVE, 8, 16, cache.encode())
+    tune_s = time.perf_counter() - t0
+    for kind in range(4):  # start from empty tables, then apply the cache
+        for lg in range(8, 17):
+            L.kb200_tune_set(kind, CURVE, lg, 0)
+    applied = L.kb200_autotune_load(cache.encode())
+    os.unlink(cache)
+    choices = {str(lg): {"commit_window": L.kb200_tune_get(3, CURVE, lg),
+                         "msm_window": L.kb200_tune_get(0, CURVE, lg),
+                         "msm_glv_window": L.kb200_tune_get(2, CURVE, lg),
+                         "ntt_first_pass_log_radix": L.kb200_tune_get(1, CURVE, lg)}
+               for lg in range(8, 17)}
+    # new commit windows may need their shifted tables and larger engines:
+    # the setup builds and warms them before anything is timed
     kb.kzg_srs_generate(_tau(7), 1 << 16)
     evs = [kb.gen_scalars(CURVE, 100000 + i, n) for i, n in enumerate(sizes)]
     blob = b"".join(evs)
@@ -463,6 +486,8 @@ def bench_batched_commits(args) -> dict:
         batch = kb.kzg_commit_batch(blob, sizes)
     t_batch = (time.perf_counter() - t0) / reps
     return {"commits": len(sizes), "sizes": "2^8..2^16 log-uniform", "srs": "2^16 resident",
+            "autotune": {"size_classes": tuned, "entries_applied": applied, "seconds": tune_s,
+                         "choices_by_log_n": choices},
             "per_call_commits_per_s": len(sizes) / t_single,
             "batched_commits_per_s": len(sizes) / t_batch,
             "batched_over_per_call": t_single / t_batch,
