@@ -188,6 +188,179 @@ KB_DEV void xyzz_dbl_warp(Xyzz<F>& p) {
     fe_sub(p.Y, Ya, WY);  // Y3 = M(S - X3) - W Y
 }
 
+// dbl-2008-s-1 on a point held in shared memory (X, Y, ZZ, ZZZ as 4N
+// consecutive words), the products spread over lanes 0..3 of the warp like
+// xyzz_dbl_warp, with every operand and result passing through shared memory
+// (tmp: 7N words of scratch) so that no lane holds the point in registers:
+// for kernels whose register budget is tight.  All 32 lanes must call it.
+template <class F>
+KB_DEV void xyzz_dbl_warp_sm(uint32_t* p, uint32_t* tmp) {
+    constexpr int N = F::N;
+    const int lane = threadIdx.x & 31;
+    uint32_t* pX = p;
+    uint32_t* pY = p + N;
+    uint32_t* pZZ = p + 2 * N;
+    uint32_t* pZZZ = p + 3 * N;
+    uint32_t* tU = tmp;
+    uint32_t* tV = tmp + N;
+    uint32_t* tM = tmp + 2 * N;
+    uint32_t* tW = tmp + 3 * N;
+    uint32_t* tS = tmp + 4 * N;
+    uint32_t* tM2 = tmp + 5 * N;
+    uint32_t* tWY = tmp + 6 * N;
+    Fe<F> a, b, r;
+    // stage 1: V = U^2 with U = 2Y (lane 0), X^2 -> M = 3 X^2 (lane 1)
+    fe_load(a, lane == 1 ? pX : pY);
+    fe_dbl(b, a);
+#pragma unroll
+    for (int i = 0; i < N; ++i) a.v[i] = lane == 1 ? a.v[i] : b.v[i];
+    fe_mul_inl(r, a, a);
+    if (lane == 0) {
+        fe_store(tU, a);
+        fe_store(tV, r);
+    } else if (lane == 1) {
+        fe_dbl(b, r);
+        fe_add(b, b, r);
+        fe_store(tM, b);
+    }
+    __syncwarp();
+    // stage 2: W = U V (0), S = X V (1), ZZ3 = V ZZ (2), M^2 (3)
+    fe_load(a, lane == 1 ? pX : (lane == 2 ? pZZ : (lane == 3 ? tM : tU)));
+    fe_load(b, lane == 3 ? tM : tV);
+    fe_mul_inl(r, a, b);
+    if (lane < 4) fe_store(lane == 1 ? tS : (lane == 2 ? pZZ : (lane == 3 ? tM2 : tW)), r);
+    __syncwarp();
+    // stage 3: M (S - X3) (0), W Y (1), W ZZZ (2), with X3 = M^2 - 2S
+    Fe<F> X3, Sd;
+    fe_load(a, tM2);
+    fe_load(Sd, tS);
+    fe_sub(X3, a, Sd);
+    fe_sub(X3, X3, Sd);
+    fe_sub(Sd, Sd, X3);
+    if (lane == 0) fe_store(pX, X3);  // nothing reads X in this stage
+    fe_load(a, lane == 0 ? tM : tW);
+    fe_load(b, lane == 2 ? pZZZ : pY);  // only lane 2 reads what it rewrites
+#pragma unroll
+    for (int i = 0; i < N; ++i) b.v[i] = lane == 0 ? Sd.v[i] : b.v[i];
+    fe_mul_inl(r, a, b);
+    if (lane == 1) fe_store(tWY, r);
+    if (lane == 2) fe_store(pZZZ, r);
+    __syncwarp();
+    // Y3 = M (S - X3) - W Y
+    if (lane == 0) {
+        fe_load(a, tWY);
+        fe_sub(r, r, a);
+        fe_store(pY, r);
+    }
+    __syncwarp();
+}
+
+// k >= 0 doublings of a point in shared memory (4N words: X, Y, ZZ, ZZZ)
+// with the coordinates dbl-2008-s-1 gives, two product levels per doubling
+// instead of three: the chain carries X^2, 3X^3 and 2Y^2 beside the point.
+// With t = 3X^3 - 2Y^2 and u = 3t - 2Y^2 (= 9X^3 - 8Y^2), the Jacobian
+// doubling for a = 0 (X' = 9X^4 - 8XY^2, Y' = 36X^3Y^2 - 27X^6 - 8Y^4,
+// Z' = 2YZ, with ZZ = Z^2 and ZZZ = Z^3) reads
+//   X' = X u,  Y' = 2 (2Y^2 t) - 3X^3 u,  ZZ' = 2 (ZZ 2Y^2),  ZZZ' = 4 ((Y 2Y^2) ZZZ),
+//   X'^2 = X^2 u^2,  3X'^3 = (3X^3 u) u^2,  2Y'^2 = (2Y') Y',
+// level 1 on lanes 0..5 (X u, u^2, 3X^3 u, 2Y^2 t, Y 2Y^2, ZZ 2Y^2), level 2
+// on lanes 0..3.  tmp: 8N words of shared scratch.  All 32 lanes call it.
+template <class F>
+KB_DEV void xyzz_dbl_chain_warp_sm(uint32_t* p, uint32_t k, uint32_t* tmp) {
+    constexpr int N = F::N;
+    const int lane = threadIdx.x & 31;
+    if (k == 0) return;
+    uint32_t* pX = p;
+    uint32_t* pY = p + N;
+    uint32_t* pZZ = p + 2 * N;
+    uint32_t* pZZZ = p + 3 * N;
+    uint32_t* tX2 = tmp;          // X^2
+    uint32_t* tX3 = tmp + N;      // 3 X^3
+    uint32_t* tY2 = tmp + 2 * N;  // 2 Y^2
+    uint32_t* tXn = tmp + 3 * N;  // X u = X'
+    uint32_t* tU2 = tmp + 4 * N;  // u^2
+    uint32_t* tVU = tmp + 5 * N;  // 3 X^3 u
+    uint32_t* tT = tmp + 6 * N;   // 2 Y^2 t
+    uint32_t* tY3 = tmp + 7 * N;  // Y 2Y^2
+    Fe<F> a, b, r, c;
+    // set-up: X^2 (lane 0), Y^2 (lane 1); then X X^2 (lane 0)
+    fe_load(a, lane == 1 ? pY : pX);
+    fe_mul_inl(r, a, a);
+    if (lane == 0) fe_store(tX2, r);
+    if (lane == 1) {
+        fe_dbl(r, r);
+        fe_store(tY2, r);
+    }
+    __syncwarp();
+    fe_load(a, pX);
+    fe_load(b, tX2);
+    fe_mul_inl(r, a, b);
+    if (lane == 0) {
+        fe_dbl(c, r);
+        fe_add(r, c, r);
+        fe_store(tX3, r);
+    }
+    __syncwarp();
+    for (uint32_t it = 0; it < k; ++it) {
+        Fe<F> t, u, y2;
+        fe_load(c, tX3);
+        fe_load(y2, tY2);
+        fe_sub(t, c, y2);
+        fe_dbl(u, t);
+        fe_add(u, u, t);
+        fe_sub(u, u, y2);
+        // level 1 (lanes that compute nothing read tX3, which no lane writes here)
+        fe_load(a, lane == 0 ? pX
+                             : (lane == 3 ? tY2 : (lane == 4 ? pY : (lane == 5 ? pZZ : tX3))));
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            a.v[i] = lane == 1 ? u.v[i] : a.v[i];
+            b.v[i] = lane <= 2 ? u.v[i] : (lane == 3 ? t.v[i] : y2.v[i]);
+        }
+        fe_mul_inl(r, a, b);
+        if (lane == 0) fe_store(tXn, r);
+        if (lane == 1) fe_store(tU2, r);
+        if (lane == 2) fe_store(tVU, r);
+        if (lane == 3) fe_store(tT, r);
+        if (lane == 4) fe_store(tY3, r);
+        if (lane == 5) {
+            fe_dbl(r, r);
+            fe_store(pZZ, r);  // ZZ' = 2 (ZZ 2Y^2); only lane 5 reads ZZ
+        }
+        __syncwarp();
+        // Y' = 2 (2Y^2 t) - 3X^3 u and 2Y'
+        Fe<F> yn, yd;
+        fe_load(a, tT);
+        fe_load(b, tVU);
+        fe_dbl(yn, a);
+        fe_sub(yn, yn, b);
+        fe_dbl(yd, yn);
+        // level 2
+        fe_load(a, lane == 0 ? tX2 : (lane == 3 ? tY3 : tVU));
+        fe_load(b, lane == 3 ? pZZZ : tU2);
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            a.v[i] = lane == 2 ? yd.v[i] : a.v[i];
+            b.v[i] = lane == 2 ? yn.v[i] : b.v[i];
+        }
+        fe_mul_inl(r, a, b);
+        if (lane == 0) fe_store(tX2, r);
+        if (lane == 1) fe_store(tX3, r);
+        if (lane == 2) fe_store(tY2, r);
+        if (lane == 3) {
+            fe_dbl(r, r);
+            fe_dbl(r, r);
+            fe_store(pZZZ, r);
+        }
+        if (lane == 4) {
+            fe_load(c, tXn);
+            fe_store(pX, c);
+        }
+        if (lane == 5) fe_store(pY, yn);
+        __syncwarp();
+    }
+}
+
 // Broadcast from lane k (0..3) of this thread's quad (lanes 4i .. 4i+3) to
 // the quad's four lanes; only the quad's lanes take part.
 template <class F>
@@ -401,6 +574,23 @@ KB_DEV void xyzz_load(Xyzz<F>& p, const uint32_t* w) {  // w 16-byte aligned
     fe_load16(p.Y, w + F::N);
     fe_load16(p.ZZ, w + 2 * F::N);
     fe_load16(p.ZZZ, w + 3 * F::N);
+}
+// The same through L2 only (ld.global.cg): for records that other blocks of
+// the running kernel wrote, which this SM's L1 may not see.
+template <class F>
+KB_DEV void xyzz_load_cg(Xyzz<F>& p, const uint32_t* w) {  // w 16-byte aligned
+    const uint4* s = reinterpret_cast<const uint4*>(w);
+    Fe<F>* f[4] = {&p.X, &p.Y, &p.ZZ, &p.ZZZ};
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int k = 0; k < F::N / 4; ++k) {
+            const uint4 v = __ldcg(s + c * (F::N / 4) + k);
+            f[c]->v[4 * k] = v.x;
+            f[c]->v[4 * k + 1] = v.y;
+            f[c]->v[4 * k + 2] = v.z;
+            f[c]->v[4 * k + 3] = v.w;
+        }
 }
 template <class F>
 KB_DEV void xyzz_store(uint32_t* w, const Xyzz<F>& p) {  // w 16-byte aligned

@@ -76,17 +76,18 @@ __global__ void k_pair_counts(const uint32_t* __restrict__ in_off, uint32_t B, u
 // Pass 2, after the scan of the counts, writes val to offsets[key] + rank:
 // no atomics.  The order inside a bucket is whatever order the atomics
 // granted; bucket sums do not depend on it.
-__global__ void k_rank(const uint32_t* __restrict__ keys, unsigned long long total,
-                       uint32_t* __restrict__ counts, uint32_t* __restrict__ ranks) {
-    const unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total) return;
+// Rank of entry slot t among the entries with its key: the next free place
+// of the key's run, by one atomic on its count.  Repeated keys (skewed
+// scalars, where one bucket can take millions of entries) show up between
+// neighbouring lanes; only then group the warp by key.  Without that, one
+// atomic per lane: every atomicAdd returns a distinct rank, so both paths
+// are exact.  All lanes of the warp that hold a slot call it together.
+__device__ __forceinline__ void rank_entry(const uint32_t* __restrict__ keys, unsigned long long t,
+                                           uint32_t* __restrict__ counts,
+                                           uint32_t* __restrict__ ranks) {
     const uint32_t key = keys[t];
     const unsigned mask = __activemask();
     const int lane = threadIdx.x & 31;
-    // Repeated keys (skewed scalars, where one bucket can take millions of
-    // entries) show up between neighbouring lanes; only then group the warp
-    // by key.  Without that, one atomic per lane: every atomicAdd returns a
-    // distinct rank, so both paths are exact.
     const uint32_t up = __shfl_down_sync(mask, key, 1);
     const bool dup = (lane < 31) && ((mask >> (lane + 1)) & 1u) && up == key && key != KEY_SENTINEL;
     if (!__any_sync(mask, dup)) {
@@ -99,6 +100,25 @@ __global__ void k_rank(const uint32_t* __restrict__ keys, unsigned long long tot
     if (lane == leader && key != KEY_SENTINEL) base = atomicAdd(&counts[key], (uint32_t)__popc(peers));
     base = __shfl_sync(peers, base, leader);
     ranks[t] = base + __popc(peers & ((1u << lane) - 1u));
+}
+
+__global__ void k_rank(const uint32_t* __restrict__ keys, unsigned long long total,
+                       uint32_t* __restrict__ counts, uint32_t* __restrict__ ranks) {
+    const unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    rank_entry(keys, t, counts, ranks);
+}
+
+// The same over the entries of scalar rows [lo, lo + len) of one MSM of n
+// scalars, whose entry slots are g * n + j (entry group g < G: a window, or
+// a window of one GLV half; row j): ranking as each chunk of scalars lands.
+__global__ void k_rank_rows(const uint32_t* __restrict__ keys, uint32_t n, uint32_t G, uint32_t lo,
+                            uint32_t len, uint32_t* __restrict__ counts,
+                            uint32_t* __restrict__ ranks) {
+    const unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (unsigned long long)G * len) return;
+    const uint32_t g = (uint32_t)(t / len), j = lo + (uint32_t)(t % len);
+    rank_entry(keys, (unsigned long long)g * n + j, counts, ranks);
 }
 
 __global__ void k_scatter(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
@@ -424,9 +444,38 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
     }();
     const size_t per_sm = (size_t)device_sms() * RED_THREADS;
     size_t s_one = (total_live + per_sm - 1) / per_sm;
-    if (s_one < 4 || s_one >= 12) s_one = (total_live + 2 * per_sm - 1) / (2 * per_sm);
-    if (env_red_bps > 0) s_one = (total_live + env_red_bps * per_sm - 1) / (env_red_bps * per_sm);
-    const uint32_t S0 = (uint32_t)std::min<size_t>(64, std::max<size_t>(1, s_one));
+    size_t bps = 1;
+    if (s_one < 4 || s_one >= 12) bps = 2;
+    if (env_red_bps > 0) bps = (size_t)env_red_bps;
+    s_one = (total_live + bps * per_sm - 1) / (bps * per_sm);
+    // Each window rounds its block count up, so the S that covers the total
+    // can still leave a few blocks for a second wave, which costs a whole
+    // block's latency (24 levels of scan and trees) for them alone: raise S
+    // (at most to twice) until every block fits the first wave (BLS12-381
+    // 2^22: S 7 -> 8 takes 305 blocks to 257 against 296 slots).
+    auto window_live = [&](size_t i, uint32_t w) -> uint32_t {
+        const ItemDesc& d = P.items[i];
+        return d.row_stride ? d.M : ((w == d.W - 1) ? plans[i].M_top : d.M);
+    };
+    auto blocks_for = [&](uint32_t S) {
+        size_t nb = 0;
+        for (size_t i = 0; i < count; ++i)
+            for (uint32_t w = 0; w < P.items[i].Wr; ++w) {
+                const size_t Mw = window_live(i, w);
+                const size_t Sw = std::max<size_t>(S, (Mw + (size_t)RED_THREADS * RED_THREADS - 1) /
+                                                          ((size_t)RED_THREADS * RED_THREADS));
+                nb += std::max<size_t>(1, (Mw + RED_THREADS * Sw - 1) / (RED_THREADS * Sw));
+            }
+        return nb;
+    };
+    uint32_t S0 = (uint32_t)std::min<size_t>(64, std::max<size_t>(1, s_one));
+    const size_t slots = bps * (size_t)device_sms();
+    if (blocks_for(S0) > slots)
+        for (uint32_t S = S0 + 1; S <= std::min<uint32_t>(64, 2 * S0); ++S)
+            if (blocks_for(S) <= slots) {
+                S0 = S;
+                break;
+            }
     // Few buckets (KZG commits up to 2^16, blobs): the reduction is bound by
     // the latency of its serial additions, not by throughput, so it runs one
     // quad of lanes per slot with the quad addition (k_reduce_blocks_quad),
@@ -443,7 +492,7 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
         for (uint32_t w = 0; w < d.Wr; ++w) {
             WinDesc wd;
             wd.bucket_base = d.bucket_base + w * d.M;
-            wd.Mw = d.row_stride ? d.M : ((w == d.W - 1) ? plans[i].M_top : d.M);
+            wd.Mw = window_live(i, w);
             const uint32_t per_block_min =
                 (uint32_t)(((size_t)wd.Mw + (size_t)RED_THREADS * RED_THREADS - 1) /
                            ((size_t)RED_THREADS * RED_THREADS));
@@ -455,7 +504,8 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
                 wd.S = std::max<uint32_t>(S0, std::max<uint32_t>(1, per_block_min));
                 wd.blk = (uint32_t)RED_THREADS * wd.S;
             }
-            wd.nb = (wd.Mw + wd.blk - 1) / wd.blk;
+            // at least one block: the window's stage 2 runs in its last block
+            wd.nb = std::max<uint32_t>(1, (wd.Mw + wd.blk - 1) / wd.blk);
             wd.shift = d.row_stride ? 0u : d.c * w;
             wd.blk_base = (uint32_t)P.blks.size();
             for (uint32_t b = 0; b < wd.nb; ++b)
@@ -594,7 +644,7 @@ class MsmEngine {
    public:
     int curve = 0;
     DevBuf table, keys, vals, counts, offsets, cursor, sorted, rec_first, rec_last, fold_buf,
-        buckets, blk_out, win_out, scan_tmp, queue, fold_counts, fold_prefix, ranks, pair_off[2],
+        buckets, blk_out, win_out, win_done, scan_tmp, queue, fold_counts, fold_prefix, ranks, pair_off[2],
         pair_rows[2], pair_scratch, pair_cntT, pair_dst, pair_in1;
     std::map<std::tuple<size_t, bool, int, int, int, size_t, bool, size_t, int>, MsmBatchPlan*> single_plans;
     cudaEvent_t ev[N_STAGE_EVENTS] = {};
@@ -607,7 +657,8 @@ class MsmEngine {
     static constexpr int HOST_CHUNKS_MAX = 8;
     static constexpr int HOST_CHUNKS = 4;
     cudaStream_t st_copy = nullptr, st_conv = nullptr;
-    cudaEvent_t ev_start = nullptr, ev_chunk[HOST_CHUNKS_MAX] = {}, ev_conv[HOST_CHUNKS_MAX] = {};
+    cudaEvent_t ev_start = nullptr, ev_chunk[HOST_CHUNKS_MAX] = {}, ev_conv[HOST_CHUNKS_MAX] = {},
+                ev_scal[HOST_CHUNKS_MAX] = {};
     void host_streams() {
         if (st_copy) return;
         KB_CUDA(cudaStreamCreateWithFlags(&st_copy, cudaStreamNonBlocking));
@@ -615,6 +666,7 @@ class MsmEngine {
         KB_CUDA(cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming));
         for (auto& c : ev_chunk) KB_CUDA(cudaEventCreateWithFlags(&c, cudaEventDisableTiming));
         for (auto& c : ev_conv) KB_CUDA(cudaEventCreateWithFlags(&c, cudaEventDisableTiming));
+        for (auto& c : ev_scal) KB_CUDA(cudaEventCreateWithFlags(&c, cudaEventDisableTiming));
     }
     void mark(int i, cudaStream_t st) {
         if (!profiling_enabled()) return;
@@ -635,9 +687,10 @@ class MsmEngine {
             cudaEventDestroy(ev_start);
             for (auto& c : ev_chunk) cudaEventDestroy(c);
             for (auto& c : ev_conv) cudaEventDestroy(c);
+            for (auto& c : ev_scal) cudaEventDestroy(c);
         }
         for (DevBuf* b : {&table, &keys, &vals, &counts, &offsets, &cursor, &sorted, &rec_first,
-                          &rec_last, &fold_buf, &buckets, &blk_out, &win_out, &scan_tmp, &queue,
+                          &rec_last, &fold_buf, &buckets, &blk_out, &win_out, &win_done, &scan_tmp, &queue,
                           &fold_counts, &fold_prefix, &ranks, &pair_off[0], &pair_off[1], &pair_rows[0],
                           &pair_rows[1], &pair_scratch, &pair_cntT, &pair_dst, &pair_in1})
             b->release();
@@ -709,6 +762,7 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
     e->buckets.reserve(std::max<size_t>(1, (size_t)P.B) * PW * 4, st);
     e->blk_out.reserve(std::max<size_t>(1, P.blks.size()) * 2 * PW * 4, st);
     e->win_out.reserve(std::max<size_t>(1, P.wins.size()) * PW * 4, st);
+    e->win_done.reserve(std::max<size_t>(1, P.wins.size()) * 4, st);
     e->scan_tmp.reserve(
         scan_tmp_words(std::max<size_t>(BS, (size_t)std::max(1, P.levels) * P.big_cap) + 1) * 4, st);
     const size_t fold_all = (size_t)std::max(1, P.levels) * P.big_cap;
@@ -732,7 +786,8 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
 
 void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_scalars,
                        const uint32_t* d_table, uint8_t* d_out_wire, uint8_t* d_out_comp,
-                       cudaStream_t st, const cudaEvent_t* table_ready, int n_ready) {
+                       cudaStream_t st, const cudaEvent_t* table_ready, int n_ready,
+                       const cudaEvent_t* scalars_ready) {
     const MsmBatchPlan& P = *p;
     const MsmLaunchers& K = msm_launchers(e->curve);
     const ItemDesc* items = P.d_items.as<ItemDesc>();
@@ -746,20 +801,38 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
         if (ms > 2.0) std::fprintf(stderr, "[msm] launch step %d: %.3f ms\n", where, ms);
         tt = t1;
     };
-    if (P.L > 0) {
-        K.recode(items, nitems, P.total_scalars, reinterpret_cast<const uint32_t*>(d_scalars),
-                 table_ready ? nullptr : d_table, e->keys.as<uint32_t>(), e->vals.as<uint32_t>(),
-                 st);
-    }
-    e->mark(2, st);
-    lap(2);
     const uint32_t BS = std::max<uint32_t>(P.B, P.B_sort);  // sort keys
     KB_CUDA(cudaMemsetAsync(e->counts.ptr, 0, ((size_t)BS + 1) * 4, st));
-    if (P.L > 0) {
+    const uint32_t* scal = reinterpret_cast<const uint32_t*>(d_scalars);
+    const uint32_t* rec_table = table_ready ? nullptr : d_table;
+    // Scalars arriving in row chunks (one MSM; entry slot g * n + j): each
+    // chunk's recode and ranking start as soon as it lands.
+    const size_t n0 = P.count == 1 ? (size_t)P.items[0].n : 0;
+    const bool by_rows = scalars_ready && n_ready > 0 && n0 > 0 && P.L > 0 && P.L % n0 == 0 &&
+                         P.items[0].entry_base == 0 && P.items[0].scalar_off == 0;
+    if (by_rows) {
+        const size_t G = P.L / n0, S = (n0 + n_ready - 1) / n_ready;
+        for (int c = 0; c < n_ready; ++c) {
+            const size_t lo = std::min(n0, (size_t)c * S), hi = std::min(n0, lo + S);
+            KB_CUDA(cudaStreamWaitEvent(st, scalars_ready[c], 0));
+            if (hi == lo) continue;
+            K.recode(items, nitems, lo, hi - lo, scal, rec_table, e->keys.as<uint32_t>(),
+                     e->vals.as<uint32_t>(), st);
+            k_rank_rows<<<ceil_div_u(G * (hi - lo), 256), 256, 0, st>>>(
+                e->keys.as<uint32_t>(), (uint32_t)n0, (uint32_t)G, (uint32_t)lo, (uint32_t)(hi - lo),
+                e->counts.as<uint32_t>(), e->ranks.as<uint32_t>());
+            KB_LAUNCH_CHECK();
+        }
+    } else if (P.L > 0) {
+        if (scalars_ready && n_ready > 0) KB_CUDA(cudaStreamWaitEvent(st, scalars_ready[n_ready - 1], 0));
+        K.recode(items, nitems, 0, P.total_scalars, scal, rec_table, e->keys.as<uint32_t>(),
+                 e->vals.as<uint32_t>(), st);
         k_rank<<<ceil_div_u(P.L, 256), 256, 0, st>>>(e->keys.as<uint32_t>(), P.L,
                                                     e->counts.as<uint32_t>(), e->ranks.as<uint32_t>());
         KB_LAUNCH_CHECK();
     }
+    e->mark(2, st);
+    lap(2);
     exclusive_scan_u32(e->counts.as<uint32_t>(), e->offsets.as<uint32_t>(), BS, 0,
                        e->scan_tmp.as<uint32_t>(), st);
     if (P.L > 0) {
@@ -904,13 +977,15 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
     ra.blks = P.d_blks.as<BlkDesc>();
     ra.blk_out = e->blk_out.as<uint32_t>();
     ra.win_out = e->win_out.as<uint32_t>();
+    ra.win_done = e->win_done.as<uint32_t>();
+    // one launch: each window's stage 2 runs in the block that finishes it
+    KB_CUDA(cudaMemsetAsync(ra.win_done, 0, P.wins.size() * 4, st));
     if (P.red_quad)
         K.reduce_blocks_quad(ra, (unsigned)P.blks.size(), st);
     else
         K.reduce_blocks(ra, (unsigned)P.blks.size(), st);
     e->mark(7, st);
     lap(7);
-    K.reduce_windows(ra, (unsigned)P.wins.size(), st);
     e->mark(8, st);
     lap(8);
     K.combine(items, nitems, e->win_out.as<uint32_t>(), d_out_wire, d_out_comp, st);
@@ -995,10 +1070,20 @@ void msm_run_host_wire(MsmEngine* e, const uint8_t* h_scalars, const uint8_t* h_
     KB_CUDA(cudaEventRecord(e->ev_start, st));
     KB_CUDA(cudaStreamWaitEvent(e->st_copy, e->ev_start, 0));
     KB_CUDA(cudaStreamWaitEvent(e->st_conv, e->ev_start, 0));
-    KB_CUDA(cudaMemcpyAsync(d_scalars, h_scalars, n * 32, cudaMemcpyHostToDevice, st));
     // chunk c = rows [c S, (c + 1) S), S = ceil(n / chunks): the rows the
-    // plan's chunk-major sort keys (when it pairs per chunk) assign to c
+    // plan's chunk-major sort keys (when it pairs per chunk) assign to c.
+    // One copy stream, all scalars first: the sort needs every scalar before
+    // the first pairing level, the points only chunk by chunk after it; each
+    // scalar chunk's recode and ranking run while the next chunk copies.
     const size_t S = (n + chunks - 1) / chunks;
+    for (size_t c = 0; c < chunks; ++c) {
+        const size_t lo = std::min(n, c * S), hi = std::min(n, lo + S);
+        if (hi > lo) {
+            KB_CUDA(cudaMemcpyAsync(d_scalars + lo * 32, h_scalars + lo * 32, (hi - lo) * 32,
+                                    cudaMemcpyHostToDevice, e->st_copy));
+        }
+        KB_CUDA(cudaEventRecord(e->ev_scal[c], e->st_copy));
+    }
     for (size_t c = 0; c < chunks; ++c) {
         const size_t lo = std::min(n, c * S), hi = std::min(n, lo + S);
         if (hi > lo) {
@@ -1012,7 +1097,8 @@ void msm_run_host_wire(MsmEngine* e, const uint8_t* h_scalars, const uint8_t* h_
     }
     e->mark(0, st);
     e->mark(1, st);
-    msm_engine_launch(e, p, d_scalars, table, d_out_wire, nullptr, st, e->ev_conv, (int)chunks);
+    msm_engine_launch(e, p, d_scalars, table, d_out_wire, nullptr, st, e->ev_conv, (int)chunks,
+                      e->ev_scal);
 }
 
 void points_wire_to_table(int curve, const uint8_t* d_wire, uint32_t* d_table, size_t n,

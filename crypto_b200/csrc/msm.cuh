@@ -147,19 +147,23 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t stream
 // the plan sorts by chunk).  The recode and sort then run without reading
 // the table; the stream waits for chunk c before its first pairing level,
 // or for the last event before the first stage that reads points.
+// scalars_ready: null, or n_ready events, event c when scalar rows
+// [c S, (c + 1) S) (S = ceil(n / n_ready)) are resident; for a one-MSM plan
+// each chunk's recode and ranking wait only for their own rows.
 void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_scalars,
                        const uint32_t* d_table, uint8_t* d_out_wire, uint8_t* d_out_comp,
                        cudaStream_t stream, const cudaEvent_t* table_ready = nullptr,
-                       int n_ready = 0);
+                       int n_ready = 0, const cudaEvent_t* scalars_ready = nullptr);
 
 // Convenience single-MSM entry points (plan cached per (n, options)).
 void msm_run_wire(MsmEngine* e, const uint8_t* d_scalars, const uint8_t* d_points, size_t n,
                   uint8_t* d_out_wire, uint8_t* d_out_comp, cudaStream_t stream,
                   const MsmOptions& opt);
-// From host buffers: the scalars are copied first on `stream` and the
-// recode and sort start at once, while the points arrive in chunks on a
-// copy stream and are converted to table rows chunk by chunk on a third;
-// d_scalars (n * 32 bytes) and d_points (n * WIRE bytes) are the staging.
+// From host buffers: one copy stream brings the scalars, then the points,
+// in row chunks; each scalar chunk is recoded and ranked on `stream` as it
+// lands, each point chunk converted to table rows on a third stream and
+// paired (first level) as soon as the sort is done; d_scalars (n * 32
+// bytes) and d_points (n * WIRE bytes) are the staging.
 void msm_run_host_wire(MsmEngine* e, const uint8_t* h_scalars, const uint8_t* h_points, size_t n,
                        uint8_t* d_scalars, uint8_t* d_points, uint8_t* d_out_wire,
                        cudaStream_t stream, const MsmOptions& opt);

@@ -135,21 +135,21 @@ struct RedArgs {
     int K2;
     const WinDesc* wins;
     const BlkDesc* blks;
-    uint32_t* blk_out;  // 2 XYZZ points per stage-1 block
-    uint32_t* win_out;  // 1 XYZZ point per window
+    uint32_t* blk_out;   // 2 XYZZ points per stage-1 block
+    uint32_t* win_out;   // 1 XYZZ point per window
+    uint32_t* win_done;  // stage-1 blocks finished per window (zeroed before the launch)
 };
 
 struct MsmLaunchers {
     void (*wire_to_table)(const uint8_t*, uint32_t*, size_t, size_t, cudaStream_t);
     void (*table_to_wire)(const uint32_t*, uint8_t*, size_t, cudaStream_t);
-    void (*recode)(const ItemDesc*, uint32_t, unsigned long long, const uint32_t*,
-                   const uint32_t*, uint32_t*, uint32_t*, cudaStream_t);
+    void (*recode)(const ItemDesc*, uint32_t, unsigned long long, unsigned long long,
+                   const uint32_t*, const uint32_t*, uint32_t*, uint32_t*, cudaStream_t);
     void (*accumulate)(const AccArgs&, unsigned, cudaStream_t);
     void (*pair_level)(const PairArgs&, uint32_t, uint32_t*, cudaStream_t);
     void (*fold)(const FoldArgs&, int, const uint32_t*, uint32_t*, unsigned, cudaStream_t);
     void (*reduce_blocks)(const RedArgs&, unsigned, cudaStream_t);
     void (*reduce_blocks_quad)(const RedArgs&, unsigned, cudaStream_t);
-    void (*reduce_windows)(const RedArgs&, unsigned, cudaStream_t);
     void (*combine)(const ItemDesc*, uint32_t, const uint32_t*, uint8_t*, uint8_t*, cudaStream_t);
     int (*accumulate_occupancy)();
     int point_words;  // XYZZ point

@@ -221,12 +221,14 @@ static __device__ void glv_split_bn(const uint32_t k[8], uint32_t k1[4], uint32_
 // carry threshold 0x8888...88 (c = 4) or 0x8080...80 (c = 8).
 template <class C>
 __global__ void k_recode(const ItemDesc* __restrict__ items, uint32_t n_items,
-                         unsigned long long total, const uint32_t* __restrict__ scalars,
+                         unsigned long long first, unsigned long long count,
+                         const uint32_t* __restrict__ scalars,
                          const uint32_t* __restrict__ table, uint32_t* __restrict__ keys,
                          uint32_t* __restrict__ vals) {
     using F = typename C::F;
-    const unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= total) return;
+    const unsigned long long idx = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= count) return;
+    const unsigned long long g = first + idx;  // scalar index over all items
     // item: largest i with items[i].scalar_off <= g
     uint32_t lo = 0, hi = n_items;
     while (hi - lo > 1) {
@@ -1071,6 +1073,228 @@ __device__ __forceinline__ void smem_tree_sum_quad(uint32_t* sm, int width) {
     }
 }
 
+// Reduction stage 2 of window w over its nb <= RED_THREADS stage-1 results
+// (Fb, Sb):  V = sum_b Fb + BLK * sum_{b>=1} Y_b + Y_0, Y_b = sum_{b'>=b} Sb',
+// then the window weight 2^shift.  Run by all threads of the stage-1 block
+// that finished the window last (reduce_tail), in its shared memory (two
+// RED_THREADS-slot point arrays); the other blocks' results are read through
+// L2 (ld.global.cg), after the fence that ordered their stores before their
+// completion count.
+template <class C>
+__device__ __forceinline__ void reduce_window(const RedArgs& a, uint32_t w, uint32_t* smr) {
+    using F = typename C::F;
+    constexpr int PW = 4 * F::N;
+    uint32_t* sA = smr;
+    uint32_t* sB = smr + RED_THREADS * PW;
+    const WinDesc wd = a.wins[w];
+    const uint32_t t = threadIdx.x;
+    {
+        Xyzz<F> Fb, Sb;
+        xyzz_set_inf(Fb);
+        xyzz_set_inf(Sb);
+        if (t < wd.nb) {
+            xyzz_load_cg(Fb, a.blk_out + ((size_t)(wd.blk_base + t) * 2) * PW);
+            xyzz_load_cg(Sb, a.blk_out + ((size_t)(wd.blk_base + t) * 2 + 1) * PW);
+        }
+        sm_store(sA, (int)t, Sb);
+        sm_store(sB, (int)t, Fb);
+    }
+    __syncthreads();
+    // slots nb .. RED_THREADS-1 hold infinity: scan and sum only the power of
+    // two that covers the window's stage-1 blocks
+    int width = 1;
+    while (width < (int)wd.nb) width <<= 1;
+    const bool quad = width <= RED_QSLOTS;
+    if (quad)
+        smem_suffix_scan_quad<F>(sA, width);
+    else
+        smem_suffix_scan<F>(sA, width);
+    Xyzz<F> Y0;
+    if (t == 0) {
+        sm_load(Y0, sA, 0);
+        Xyzz<F> inf;
+        xyzz_set_inf(inf);
+        sm_store(sA, 0, inf);
+    }
+    __syncthreads();
+    if (quad) {
+        smem_tree_sum_quad<F>(sA, width);
+        smem_tree_sum_quad<F>(sB, width);
+    } else {
+        smem_tree_sum<F>(sA, width);
+        smem_tree_sum<F>(sB, width);
+    }
+    // Warp 0 finishes: V = [blk] (sum over b >= 1 of Y_b) + sum Fb + Y_0,
+    // then the window weight 2^(c*w) by the doubling chain with its products
+    // spread over the warp's lanes (two product latencies per doubling).
+    if (t < 32) {
+        Xyzz<F> V, u;
+        sm_load(V, sA, 0);
+        xyzz_mul_small_warp(V, wd.blk);
+        if (t == 0) {
+            sm_load(u, sB, 0);
+            xyzz_add(V, u);
+            xyzz_add(V, Y0);
+            sm_store(sA, 0, V);
+        }
+        __syncwarp();
+        // the doubling chain on a contiguous copy in sB (free now); an empty
+        // window (the carry window of 256-bit windows is empty for scalars
+        // below 2^255) skips it: it would be the longest
+        uint32_t* pv = sB;
+        if (t == 0) {
+            sm_load(V, sA, 0);
+            xyzz_store(pv, V);
+        }
+        __syncwarp();
+        if (!SmXyzz<F, 1>{pv}.is_inf()) xyzz_dbl_chain_warp_sm<F>(pv, wd.shift, sB + PW);
+        if (t == 0) SmXyzz<F, 1>{pv}.to_global(a.win_out + (size_t)w * PW);
+    }
+}
+
+// V = [k] V for a small k by double-and-add on a point in shared memory (4N
+// consecutive words), the doublings spread over the warp (xyzz_dbl_warp_sm),
+// the additions on lane 0; tmp: 7N words, R: 4N words of shared scratch.
+// All 32 lanes must call it.
+template <class F>
+__device__ __forceinline__ void xyzz_mul_small_warp_sm(uint32_t* p, uint32_t k, uint32_t* tmp,
+                                                       uint32_t* R) {
+    using S1 = SmXyzz<F, 1>;
+    const int lane = threadIdx.x & 31;
+    if (k == 0) {
+        if (lane == 0) S1{p}.set_inf();
+        __syncwarp();
+        return;
+    }
+    if (lane == 0) xyzz_copy(S1{R}, S1{p});
+    __syncwarp();
+    for (int b = 30 - __clz(k); b >= 0; --b) {
+        xyzz_dbl_warp_sm<F>(p, tmp);
+        if ((k >> b) & 1u) {
+            if (lane == 0) xyzz_add(S1{p}, S1{R});
+            __syncwarp();
+        }
+    }
+}
+
+// reduce_window for the two-blocks-per-SM stage-1 kernel (at most 128
+// registers a thread): every point stays in shared memory (SmXyzz) as in
+// k_reduce_blocks, the scan and trees one slot per thread, the [blk] product
+// and the doubling chain on warp 0 (xyzz_dbl_warp_sm, xyzz_dbl_chain_warp_sm).
+// smr holds two RED_THREADS-slot point arrays and three stash points
+// (red_blocks_smem).
+template <class C>
+__device__ __forceinline__ void reduce_window_sm(const RedArgs& a, uint32_t w, uint32_t* smr) {
+    using F = typename C::F;
+    constexpr int PW = 4 * F::N;
+    using SP = SmXyzz<F, RED_THREADS>;
+    using S1 = SmXyzz<F, 1>;
+    uint32_t* sA = smr;
+    uint32_t* sB = smr + RED_THREADS * PW;
+    uint32_t* sX = smr + 2 * RED_THREADS * PW;
+    const WinDesc wd = a.wins[w];
+    const int me = threadIdx.x;
+    int width = 1;
+    while (width < (int)wd.nb) width <<= 1;
+    if (me < width) {
+        if (me < (int)wd.nb) {
+            // Sb -> slot of sA, Fb -> slot of sB (word j at [j * RED_THREADS])
+            const uint4* g =
+                reinterpret_cast<const uint4*>(a.blk_out + ((size_t)(wd.blk_base + me) * 2) * PW);
+#pragma unroll 4
+            for (int k = 0; k < PW / 4; ++k) {
+                const uint4 f = __ldcg(g + k);
+                const uint4 v = __ldcg(g + PW / 4 + k);
+                sB[(4 * k) * RED_THREADS + me] = f.x;
+                sB[(4 * k + 1) * RED_THREADS + me] = f.y;
+                sB[(4 * k + 2) * RED_THREADS + me] = f.z;
+                sB[(4 * k + 3) * RED_THREADS + me] = f.w;
+                sA[(4 * k) * RED_THREADS + me] = v.x;
+                sA[(4 * k + 1) * RED_THREADS + me] = v.y;
+                sA[(4 * k + 2) * RED_THREADS + me] = v.z;
+                sA[(4 * k + 3) * RED_THREADS + me] = v.w;
+            }
+        } else {
+            SP{sA + me}.set_inf();
+            SP{sB + me}.set_inf();
+        }
+    }
+    __syncthreads();
+    // sum of Fb -> stash 0
+    for (int d = width >> 1; d >= 1; d >>= 1) {
+        if (me < d) xyzz_add(SP{sB + me}, SP{sB + me + d});
+        __syncthreads();
+    }
+    if (me == 0) xyzz_copy(S1{sX}, SP{sB});
+    // suffix scan of Sb over the width slots, ping-pong between sA and sB
+    uint32_t* src = sA;
+    uint32_t* dst = sB;
+    for (int d = 1; d < width; d <<= 1) {
+        if (me < width) {
+            const SP o{dst + me};
+            xyzz_copy(o, SP{src + me});
+            if (me + d < width) xyzz_add(o, SP{src + me + d});
+        }
+        __syncthreads();
+        uint32_t* tmp = src;
+        src = dst;
+        dst = tmp;
+    }
+    if (me == 0) {
+        xyzz_copy(S1{sX + PW}, SP{src});  // Y_0
+        SP{src}.set_inf();                // the tree below sums Y_b for b >= 1
+    }
+    __syncthreads();
+    for (int d = width >> 1; d >= 1; d >>= 1) {
+        if (me < d) xyzz_add(SP{src + me}, SP{src + me + d});
+        __syncthreads();
+    }
+    // Warp 0: V = [blk] (sum over b >= 1 of Y_b) + sum Fb + Y_0, then the
+    // window weight 2^shift; dst is free scratch now.
+    if (me < 32) {
+        uint32_t* pv = dst;
+        uint32_t* tmp = dst + PW;
+        uint32_t* R = dst + PW + 7 * F::N;
+        if (me == 0) xyzz_copy(S1{pv}, SP{src});
+        __syncwarp();
+        xyzz_mul_small_warp_sm<F>(pv, wd.blk, tmp, R);
+        if (me == 0) {
+            xyzz_add(S1{pv}, S1{sX});
+            xyzz_add(S1{pv}, S1{sX + PW});
+        }
+        __syncwarp();
+        // an empty window (the carry window of 256-bit windows is empty for
+        // scalars below 2^255) skips its chain: it would be the longest
+        if (!S1{pv}.is_inf()) xyzz_dbl_chain_warp_sm<F>(pv, wd.shift, tmp);
+        if (me == 0) S1{pv}.to_global(a.win_out + (size_t)w * PW);
+    }
+}
+
+// End of a stage-1 block: thread 0 has stored the block's (Fb, Sb).  It
+// fences those stores and counts the block done for its window; the block
+// that completes the window's count runs the window's stage 2 at once, so
+// the windows' doubling chains (the longest first: blocks run top window
+// first) overlap the remaining stage-1 blocks instead of following them.
+// No block waits for another.  win_done holds one zeroed counter per window.
+template <class C, bool SMEM_ONLY>
+__device__ __forceinline__ void reduce_tail(const RedArgs& a, uint32_t win, uint32_t nb,
+                                            uint32_t* smr) {
+    __shared__ uint32_t s_last;
+    __syncthreads();  // every thread is done with smr
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t done = atomicAdd(a.win_done + win, 1u);
+        s_last = done + 1u == nb;
+        if (s_last) __threadfence();
+    }
+    __syncthreads();
+    if (!s_last) return;
+    if constexpr (SMEM_ONLY)
+        reduce_window_sm<C>(a, win, smr);
+    else
+        reduce_window<C>(a, win, smr);
+}
+
 // Reduction stage 1 for small bucket counts (latency-bound: few blocks),
 // one quad per slot, RED_QSLOTS slots of S buckets per block, the quad
 // addition throughout; the same outputs as k_reduce_blocks (Fb, Sb per
@@ -1082,7 +1306,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_blocks_quad(RedArgs a) {
     extern __shared__ __align__(16) uint32_t smr[];
     uint32_t* sA = smr;
     uint32_t* sB = smr + RED_THREADS * PW;
-    const BlkDesc bd = a.blks[blockIdx.x];
+    const uint32_t bi = gridDim.x - 1u - blockIdx.x;  // top window first
+    const BlkDesc bd = a.blks[bi];
     const WinDesc wd = a.wins[bd.win];
     const uint32_t S = wd.S;
     const int sl = threadIdx.x >> 2;
@@ -1121,10 +1346,11 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_blocks_quad(RedArgs a) {
         if (threadIdx.x == 0) {
             sm_load(u, sB, 0);
             xyzz_add(V, u);
-            xyzz_store(a.blk_out + ((size_t)blockIdx.x * 2) * PW, V);
-            xyzz_store(a.blk_out + ((size_t)blockIdx.x * 2 + 1) * PW, Y0);
+            xyzz_store(a.blk_out + ((size_t)bi * 2) * PW, V);
+            xyzz_store(a.blk_out + ((size_t)bi * 2 + 1) * PW, Y0);
         }
     }
+    reduce_tail<C, false>(a, bd.win, wd.nb, smr);
 }
 
 // Reduction stage 1.  Block -> (window, b) via its BlkDesc.  Thread t owns
@@ -1148,7 +1374,8 @@ __global__ void __launch_bounds__(RED_THREADS, 2) k_reduce_blocks(RedArgs a) {
     uint32_t* sA = smr;
     uint32_t* sB = smr + RED_THREADS * PW;
     uint32_t* sX = smr + 2 * RED_THREADS * PW;
-    const BlkDesc bd = a.blks[blockIdx.x];
+    const uint32_t bi = gridDim.x - 1u - blockIdx.x;  // top window first
+    const BlkDesc bd = a.blks[bi];
     const WinDesc wd = a.wins[bd.win];
     const uint32_t S = wd.S;
     const uint32_t first = bd.b * wd.blk + threadIdx.x * S;
@@ -1200,107 +1427,60 @@ __global__ void __launch_bounds__(RED_THREADS, 2) k_reduce_blocks(RedArgs a) {
             if ((S >> b) & 1u) xyzz_add(Fb, R);
         }
         xyzz_add(Fb, S1{sX});
-        Fb.to_global(a.blk_out + ((size_t)blockIdx.x * 2) * PW);
-        S1{sX + PW}.to_global(a.blk_out + ((size_t)blockIdx.x * 2 + 1) * PW);
+        Fb.to_global(a.blk_out + ((size_t)bi * 2) * PW);
+        S1{sX + PW}.to_global(a.blk_out + ((size_t)bi * 2 + 1) * PW);
     }
-}
-
-// Reduction stage 2, one block per window over its nb <= RED_THREADS
-// stage-1 results (Fb, Sb):  V = sum_b Fb + BLK * sum_{b>=1} Y_b + Y_0,
-// Y_b = sum_{b'>=b} Sb'.
-template <class C>
-__global__ void __launch_bounds__(RED_THREADS) k_reduce_windows(RedArgs a) {
-    using F = typename C::F;
-    constexpr int PW = 4 * F::N;
-    extern __shared__ __align__(16) uint32_t smr[];
-    uint32_t* sA = smr;
-    uint32_t* sB = smr + RED_THREADS * PW;
-    const WinDesc wd = a.wins[blockIdx.x];
-    const uint32_t t = threadIdx.x;
-    {
-        Xyzz<F> Fb, Sb;
-        xyzz_set_inf(Fb);
-        xyzz_set_inf(Sb);
-        if (t < wd.nb) {
-            xyzz_load(Fb, a.blk_out + ((size_t)(wd.blk_base + t) * 2) * PW);
-            xyzz_load(Sb, a.blk_out + ((size_t)(wd.blk_base + t) * 2 + 1) * PW);
-        }
-        sm_store(sA, (int)t, Sb);
-        sm_store(sB, (int)t, Fb);
-    }
-    __syncthreads();
-    // slots nb .. RED_THREADS-1 hold infinity: scan and sum only the power of
-    // two that covers the window's stage-1 blocks
-    int width = 1;
-    while (width < (int)wd.nb) width <<= 1;
-    const bool quad = width <= RED_QSLOTS;
-    if (quad)
-        smem_suffix_scan_quad<F>(sA, width);
-    else
-        smem_suffix_scan<F>(sA, width);
-    Xyzz<F> Y0;
-    if (t == 0) {
-        sm_load(Y0, sA, 0);
-        Xyzz<F> inf;
-        xyzz_set_inf(inf);
-        sm_store(sA, 0, inf);
-    }
-    __syncthreads();
-    if (quad) {
-        smem_tree_sum_quad<F>(sA, width);
-        smem_tree_sum_quad<F>(sB, width);
-    } else {
-        smem_tree_sum<F>(sA, width);
-        smem_tree_sum<F>(sB, width);
-    }
-    // Warp 0 finishes: V = [blk] (sum over b >= 1 of Y_b) + sum Fb + Y_0,
-    // then the window weight 2^(c*w).  The doubling chains run with their
-    // products spread over the warp's lanes (three product latencies per
-    // doubling), one chain per window block, all windows in parallel.
-    if (t < 32) {
-        Xyzz<F> V, u;
-        sm_load(V, sA, 0);
-        xyzz_mul_small_warp(V, wd.blk);
-        if (t == 0) {
-            sm_load(u, sB, 0);
-            xyzz_add(V, u);
-            xyzz_add(V, Y0);
-            sm_store(sA, 0, V);
-        }
-        __syncwarp();
-        sm_load(V, sA, 0);
-        // an empty window (the carry window of 256-bit windows is empty for
-        // scalars below 2^255) skips its chain: it would be the longest
-        if (!xyzz_is_inf(V))
-            for (uint32_t k = 0; k < wd.shift; ++k) xyzz_dbl_warp(V);
-        if (t == 0) xyzz_store(a.win_out + (size_t)blockIdx.x * PW, V);
-    }
+    reduce_tail<C, true>(a, bd.win, wd.nb, smr);
 }
 
 // Sum of each item's (already weighted) windows, then affine + wire
-// (+ compressed for BLS12-381).  One thread per item.
+// (+ compressed for BLS12-381).  One warp per item: quad q (lanes 4q..4q+3)
+// sums windows q, q + 8, q + 16, ... with the quad addition, then three
+// shuffle levels fold the eight quads' sums into quad 0 (at 17 windows: five
+// quad additions deep instead of sixteen serial additions), and lane 0
+// converts and encodes.
+constexpr int COMBINE_WARPS = 4;
+
+template <class F>
+__device__ __forceinline__ void xyzz_shfl_down(Xyzz<F>& r, const Xyzz<F>& p, int d) {
+#pragma unroll
+    for (int k = 0; k < F::N; ++k) {
+        r.X.v[k] = __shfl_down_sync(0xffffffffu, p.X.v[k], d);
+        r.Y.v[k] = __shfl_down_sync(0xffffffffu, p.Y.v[k], d);
+        r.ZZ.v[k] = __shfl_down_sync(0xffffffffu, p.ZZ.v[k], d);
+        r.ZZZ.v[k] = __shfl_down_sync(0xffffffffu, p.ZZZ.v[k], d);
+    }
+}
+
 template <class C>
-__global__ void k_combine(const ItemDesc* __restrict__ items, uint32_t n_items,
-                          const uint32_t* __restrict__ wins, uint8_t* __restrict__ out_wire,
-                          uint8_t* __restrict__ out_comp) {
+__global__ void __launch_bounds__(COMBINE_WARPS * 32)
+    k_combine(const ItemDesc* __restrict__ items, uint32_t n_items,
+              const uint32_t* __restrict__ wins, uint8_t* __restrict__ out_wire,
+              uint8_t* __restrict__ out_comp) {
     using F = typename C::F;
     constexpr int PW = 4 * F::N;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_items) return;
+    const uint32_t i = blockIdx.x * COMBINE_WARPS + (threadIdx.x >> 5);
+    if (i >= n_items) return;  // whole warps
+    const int lane = threadIdx.x & 31;
+    const int q = lane >> 2;
     const ItemDesc it = items[i];
-    uint8_t* ow = out_wire + (size_t)it.out_index * C::WIRE;
-    uint8_t* oc = out_comp ? out_comp + (size_t)it.out_index * 48 : nullptr;
     Xyzz<F> acc, t;
-    if (it.n == 0) {
-        xyzz_set_inf(acc);
-    } else {
+    xyzz_set_inf(acc);
+    if (it.n != 0) {
         // windows arrive already weighted by 2^(c*w): a plain sum
-        xyzz_load(acc, wins + (size_t)(it.win_base + it.Wr - 1) * PW);
-        for (int w = (int)it.Wr - 2; w >= 0; --w) {
-            xyzz_load(t, wins + (size_t)(it.win_base + (uint32_t)w) * PW);
-            xyzz_add(acc, t);
+        for (uint32_t w = (uint32_t)q; w < it.Wr; w += 8) {
+            xyzz_load(t, wins + (size_t)(it.win_base + w) * PW);
+            xyzz_add_quad(acc, t);
         }
     }
+    for (int d = 16; d >= 4; d >>= 1) {
+        xyzz_shfl_down(t, acc, d);
+        if (lane >= d) xyzz_set_inf(t);  // no partner: nothing to add
+        xyzz_add_quad(acc, t);
+    }
+    if (lane != 0) return;
+    uint8_t* ow = out_wire + (size_t)it.out_index * C::WIRE;
+    uint8_t* oc = out_comp ? out_comp + (size_t)it.out_index * 48 : nullptr;
     Affine<F> af;
     const bool fin = xyzz_to_affine(af, acc);
     Fe<F> x, y;
@@ -1355,12 +1535,12 @@ struct MsmLaunchImpl {
         k_table_to_wire<C><<<ceil_div_u(n, 128), 128, 0, st>>>(t, w, n);
         KB_LAUNCH_CHECK();
     }
-    static void recode(const ItemDesc* items, uint32_t n_items, unsigned long long total,
-                       const uint32_t* scalars, const uint32_t* table, uint32_t* keys,
-                       uint32_t* vals, cudaStream_t st) {
-        if (!total) return;
-        k_recode<C><<<ceil_div_u(total, 256), 256, 0, st>>>(items, n_items, total, scalars, table,
-                                                           keys, vals);
+    static void recode(const ItemDesc* items, uint32_t n_items, unsigned long long first,
+                       unsigned long long count, const uint32_t* scalars, const uint32_t* table,
+                       uint32_t* keys, uint32_t* vals, cudaStream_t st) {
+        if (!count) return;
+        k_recode<C><<<ceil_div_u(count, 256), 256, 0, st>>>(items, n_items, first, count, scalars,
+                                                           table, keys, vals);
         KB_LAUNCH_CHECK();
     }
     // One pairing level over T0 = ceil(slots / PAIR_J) threads; scratch holds
@@ -1404,16 +1584,11 @@ struct MsmLaunchImpl {
         k_reduce_blocks_quad<C><<<nblk, RED_THREADS, red_smem(), st>>>(a);
         KB_LAUNCH_CHECK();
     }
-    static void reduce_windows(const RedArgs& a, unsigned nwin, cudaStream_t st) {
-        if (!nwin) return;
-        set_smem_attr((const void*)k_reduce_windows<C>, red_smem());
-        k_reduce_windows<C><<<nwin, RED_THREADS, red_smem(), st>>>(a);
-        KB_LAUNCH_CHECK();
-    }
     static void combine(const ItemDesc* items, uint32_t n_items, const uint32_t* wins,
                         uint8_t* ow, uint8_t* oc, cudaStream_t st) {
         if (!n_items) return;
-        k_combine<C><<<ceil_div_u(n_items, 32), 32, 0, st>>>(items, n_items, wins, ow, oc);
+        k_combine<C><<<ceil_div_u(n_items, COMBINE_WARPS), COMBINE_WARPS * 32, 0, st>>>(
+            items, n_items, wins, ow, oc);
         KB_LAUNCH_CHECK();
     }
     static int accumulate_occupancy() {
@@ -1431,7 +1606,6 @@ struct MsmLaunchImpl {
         L.fold = &fold;
         L.reduce_blocks = &reduce_blocks;
         L.reduce_blocks_quad = &reduce_blocks_quad;
-        L.reduce_windows = &reduce_windows;
         L.combine = &combine;
         L.accumulate_occupancy = &accumulate_occupancy;
         L.point_words = 4 * F::N;
