@@ -257,8 +257,7 @@ def profile_enable(on: bool) -> None:
     lib().kb200_profile_enable(int(on))
 
 
-MSM_STAGES = ("wire_to_table", "recode", "sort", "pair", "accumulate", "fold", "reduce_blocks",
-              "reduce_windows", "combine")
+MSM_STAGES = ("wire_to_table", "recode", "sort", "pair", "accumulate", "fold", "reduce", "combine")
 
 
 def msm_stage_ms(curve: int) -> dict[str, float]:

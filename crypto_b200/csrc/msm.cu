@@ -638,7 +638,7 @@ size_t msm_batch_plan_count(const MsmBatchPlan* p) { return p->count; }
 // Engine
 // ---------------------------------------------------------------------------
 
-constexpr int N_STAGE_EVENTS = 10;
+constexpr int N_STAGE_EVENTS = 9;
 
 class MsmEngine {
    public:
@@ -986,11 +986,9 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
         K.reduce_blocks(ra, (unsigned)P.blks.size(), st);
     e->mark(7, st);
     lap(7);
+    K.combine(items, nitems, e->win_out.as<uint32_t>(), d_out_wire, d_out_comp, st);
     e->mark(8, st);
     lap(8);
-    K.combine(items, nitems, e->win_out.as<uint32_t>(), d_out_wire, d_out_comp, st);
-    e->mark(9, st);
-    lap(9);
 }
 
 static MsmBatchPlan* single_plan(MsmEngine* e, size_t n, const MsmOptions& opt, cudaStream_t st) {

@@ -318,9 +318,9 @@ unsigned long long kb200_launch_count(void);
 /* Per-stage CUDA-event timing of MSMs (off by default). */
 void kb200_profile_enable(int on);
 /* Stage times (ms) of the last MSM on this device for the curve, in order:
- * wire->table, recode, sort, accumulate, fold, reduce_blocks, reduce_windows,
- * combine.  Returns the
- * number written (0 if none recorded), or -1. */
+ * wire->table, recode (with the ranking of the sort), sort (scan and
+ * scatter), pairing levels, accumulation, fold, reduction (both stages),
+ * combine.  Returns the number written (0 if none recorded), or -1. */
 int kb200_msm_stage_ms(uint32_t curve, float* out, int max);
 
 #ifdef __cplusplus
