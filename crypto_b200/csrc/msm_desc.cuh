@@ -100,9 +100,11 @@ struct PairArgs {
 // INV_T-thread blocks, each thread chaining up to INV_G elements and each
 // block inverting its own product.  G is the smallest chain length that keeps
 // the grid at about INV_FILL threads (two 256-thread blocks on each of 148
-// SMs), so large levels stay throughput-bound and small ones short.
+// SMs), so large levels stay throughput-bound and small ones short; up to 32
+// keeps a 2^22 MSM's first level in one wave (16 left it 549 blocks, about
+// two waves, each paying a block's inversion latency).
 constexpr int PAIR_J = 16;
-constexpr int INV_G = 16;
+constexpr int INV_G = 32;
 constexpr int INV_T = 256;
 constexpr size_t INV_FILL = (size_t)2 * 148 * INV_T;
 
