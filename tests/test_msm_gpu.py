@@ -329,11 +329,11 @@ print("ok")
 @pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("curve,logn", [(2, 20), (1, 17), (1, 20)])
 def test_host_pipeline_with_infinity_points(cuda_lib, curve, logn, path):
-    """gpukit_multi_pippenger overlaps the point copy with the recode and
-    sort (chunked copies, conversion per chunk), so infinity points reach
-    the buckets and are skipped there: one point in eight is the identity,
-    at a size with eight chunks (and, at 2^20 on BLS12-381, GLV rows and
-    pairing levels)."""
+    """gpukit_multi_pippenger copies the scalars and then the points in row
+    chunks (four at these sizes), recodes and ranks each scalar chunk as it
+    lands and converts each point chunk on its own stream, so infinity
+    points reach the buckets and are skipped there: one point in eight is
+    the identity (and, at 2^20 on BLS12-381, with pairing levels)."""
     n = 1 << logn
     pb = O.PB[curve]
     pts = bytearray(rand_points(curve, n, seed=90 + curve))
@@ -400,6 +400,43 @@ assert kb.gpukit_multi_pippenger(curve, S, pts, n) == want
 print("ok")
 ''' % (curve, logn)
     env = dict(os.environ, KB200_MSM_RED_QUAD=str(quad))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True,
+                         text=True, timeout=900)
+    assert out.returncode == 0 and "ok" in out.stdout, out.stdout + out.stderr
+
+
+@pytest.mark.parametrize("chunks", [3, 8])
+@pytest.mark.parametrize("curve", [1, 2])
+def test_host_pipeline_uneven_chunks(cuda_lib, curve, chunks):
+    """Row chunks that do not divide n (3: the last chunk shorter) and the
+    largest count (8): each scalar chunk's recode and ranking cover exactly
+    its rows (KB200_MSM_HOST_CHUNKS), with infinity points among the inputs;
+    the bytes equal the reference's."""
+    import os
+    import subprocess
+    import sys
+    code = r'''
+import random, sys
+sys.path.insert(0, "tests")
+import crypto_b200 as kb, _oracle as O
+from test_msm_gpu import rand_points
+curve = %d
+n = (1 << 17) + 5
+pb = O.PB[curve]
+pts = bytearray(rand_points(curve, n, seed=160 + curve))
+for j in (0, 1, n // 3, n - 1):
+    pts[pb * j:pb * (j + 1)] = bytes(pb)
+pts = bytes(pts)
+rng = random.Random(160 + curve)
+S = b"".join(rng.randrange(O.FR[curve]).to_bytes(32, "little") for _ in range(n))
+want = O.ref_msm(curve, S, pts, n, threads=16) if O.ref_available() else O.msm(curve, S, pts, n)
+for path in ("plain", "subgroup"):
+    f = kb.gpukit_multi_pippenger if path == "plain" else kb.gpukit_multi_pippenger_subgroup
+    assert f(curve, S, pts, n) == want, path
+print("ok")
+''' % curve
+    env = dict(os.environ, KB200_MSM_HOST_CHUNKS=str(chunks))
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True,
                          text=True, timeout=900)
