@@ -195,6 +195,19 @@ def test_skewed_scalars(cuda_lib, curve, path):
 
 
 @pytest.mark.parametrize("path", PATHS)
+def test_skewed_scalars_tiled_ranking(cuda_lib, path):
+    """Skewed scalars at a size whose sort ranks by tiles (BLS12-381, 2^17
+    points: over 2^20 entries, windows of at most 2^15 buckets): the hot
+    buckets of the {0, 1} scalars meet in a tile's shared counters through
+    the warp's grouping of equal keys; the bytes equal the reference's."""
+    n = 1 << 17
+    pts = rand_points(2, n, seed=6)
+    scs = kb().gen_scalars(2, 4321, n, kind=1)
+    want = O.ref_msm(2, scs, pts, n, threads=16) if O.ref_available() else O.msm(2, scs, pts, n)
+    assert msm(path, 2, scs, pts, n) == want
+
+
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("curve", [1, 2])
 def test_2_16_against_reference(cuda_lib, curve, path):
     n = 1 << 16
