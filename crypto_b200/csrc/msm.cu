@@ -124,15 +124,18 @@ __global__ void k_rank_rows(const uint32_t* __restrict__ keys, uint32_t n, uint3
 // ---- Tiled ranking (one MSM whose windows have at most RANK_TILE_M buckets) --
 // A tile is a row range of one entry group (window, or window of a GLV half)
 // within one row chunk: all its keys lie in one window's bucket range, so its
-// block counts them in shared memory (local ranks) and then reserves each
-// bucket's places with one global atomic per distinct bucket: at the 2^22
-// headline a tile of ~440 K entries over 32 K buckets takes ~14x fewer global
-// atomics than one per entry.  Entries whose key falls outside the tile's
-// counter range (the GLV top window's buckets past M) take a global atomic
-// each and carry RANK_GLOBAL in their rank.
+// block counts them in shared memory (local ranks), reserves each bucket's
+// places with one global atomic per distinct bucket (at the 2^22 headline a
+// tile of ~440 K entries over 32 K buckets: ~14x fewer global atomics than
+// one per entry), then adds the reserved base to every local rank, so the
+// plain scatter (offsets[key] + rank) follows.  Entries whose key falls
+// outside the tile's counter range (the GLV top window's buckets past M)
+// take a global atomic each.  Each thread handles RANK_TILE_U entries per
+// round, their loads issued together.
 constexpr uint32_t RANK_TILE_M = 32768;          // shared-memory counters per tile (128 KiB)
 constexpr uint32_t RANK_GLOBAL = 0x80000000u;    // rank taken from the global count
 constexpr int RANK_TILE_THREADS = 1024;
+constexpr int RANK_TILE_U = 4;
 
 struct RankTiles {
     uint32_t n;             // scalars (rows); entry slot g * n + j
@@ -147,84 +150,82 @@ struct RankTiles {
     uint32_t chunk_stride;  // keys per key chunk
 };
 
-__device__ __forceinline__ uint32_t tile_key_base(const RankTiles& t, uint32_t c, uint32_t g) {
-    return (t.chunk_rows ? c * t.chunk_stride : 0u) + t.bucket_base + (t.glv ? g >> 1 : g) * t.M;
-}
-
 // Grid (G Q) per row chunk, chunks c0, c0 + 1, ... (blockIdx.y).
 __global__ void __launch_bounds__(RANK_TILE_THREADS) k_rank_tiles(const uint32_t* __restrict__ keys,
                                                                   RankTiles t, uint32_t c0,
                                                                   uint32_t* __restrict__ counts,
-                                                                  uint32_t* __restrict__ ranks,
-                                                                  uint32_t* __restrict__ base) {
+                                                                  uint32_t* __restrict__ ranks) {
     extern __shared__ uint32_t sc[];
     const uint32_t c = c0 + blockIdx.y;
     const uint32_t g = blockIdx.x / t.Q, q = blockIdx.x % t.Q;
-    const uint32_t tile = (c * t.G + g) * t.Q + q;
-    const uint32_t kb = tile_key_base(t, c, g);
+    const uint32_t kb = (t.chunk_rows ? c * t.chunk_stride : 0u) + t.bucket_base + (t.glv ? g >> 1 : g) * t.M;
     const uint32_t chunk_end = min(t.n, (c + 1) * t.TS);
     const uint32_t r0 = min(chunk_end, c * t.TS + q * t.R), r1 = min(chunk_end, r0 + t.R);
+    const unsigned long long gbase = (unsigned long long)g * t.n;
     for (uint32_t k = threadIdx.x; k < t.M; k += blockDim.x) sc[k] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    for (uint32_t j = r0 + threadIdx.x; j < r1; j += blockDim.x) {
-        const unsigned long long slot = (unsigned long long)g * t.n + j;
-        const uint32_t key = keys[slot];
-        const uint32_t kl = key - kb;
-        const bool local = kl < t.M;
-        const unsigned mask = __activemask();
-        const uint32_t up = __shfl_down_sync(mask, key, 1);
-        const bool dup = (lane < 31) && ((mask >> (lane + 1)) & 1u) && up == key && key != KEY_SENTINEL;
-        uint32_t r = 0;
-        if (!__any_sync(mask, dup)) {
-            if (key != KEY_SENTINEL) r = local ? atomicAdd(&sc[kl], 1u) : (atomicAdd(&counts[key], 1u) | RANK_GLOBAL);
-        } else {
-            // repeated keys between neighbouring lanes (skewed scalars): one
-            // atomic per group of equal keys
-            const unsigned peers = __match_any_sync(mask, key);
-            const int leader = __ffs(peers) - 1;
-            uint32_t b = 0;
-            if (lane == leader && key != KEY_SENTINEL) {
-                const uint32_t cnt = (uint32_t)__popc(peers);
-                b = local ? atomicAdd(&sc[kl], cnt) : atomicAdd(&counts[key], cnt);
-            }
-            b = __shfl_sync(peers, b, leader);
-            r = b + __popc(peers & ((1u << lane) - 1u));
-            if (!local) r |= RANK_GLOBAL;
-            if (key == KEY_SENTINEL) r = 0;
+    constexpr uint32_t STEP = RANK_TILE_THREADS * RANK_TILE_U;
+    // local ranks (or global ones, flagged); every lane of a warp runs every
+    // round (lanes past the tile's end carry the sentinel key)
+    for (uint32_t j0 = r0; j0 < r1; j0 += STEP) {
+        uint32_t key[RANK_TILE_U];
+#pragma unroll
+        for (int u = 0; u < RANK_TILE_U; ++u) {
+            const uint32_t j = j0 + u * RANK_TILE_THREADS + threadIdx.x;
+            key[u] = j < r1 ? keys[gbase + j] : KEY_SENTINEL;
         }
-        ranks[slot] = r;
+#pragma unroll
+        for (int u = 0; u < RANK_TILE_U; ++u) {
+            const uint32_t j = j0 + u * RANK_TILE_THREADS + threadIdx.x;
+            const uint32_t kl = key[u] - kb;
+            const bool local = kl < t.M;
+            const uint32_t up = __shfl_down_sync(0xffffffffu, key[u], 1);
+            const bool dup = lane < 31 && up == key[u] && key[u] != KEY_SENTINEL;
+            uint32_t r = 0;
+            if (!__any_sync(0xffffffffu, dup)) {
+                if (key[u] != KEY_SENTINEL)
+                    r = local ? atomicAdd(&sc[kl], 1u) : (atomicAdd(&counts[key[u]], 1u) | RANK_GLOBAL);
+            } else {
+                // repeated keys between neighbouring lanes (skewed scalars):
+                // one atomic per group of equal keys
+                const unsigned peers = __match_any_sync(0xffffffffu, key[u]);
+                const int leader = __ffs(peers) - 1;
+                uint32_t b = 0;
+                if (lane == leader && key[u] != KEY_SENTINEL) {
+                    const uint32_t cnt = (uint32_t)__popc(peers);
+                    b = local ? atomicAdd(&sc[kl], cnt) : atomicAdd(&counts[key[u]], cnt);
+                }
+                b = __shfl_sync(0xffffffffu, b, leader);
+                r = b + __popc(peers & ((1u << lane) - 1u));
+                if (!local) r |= RANK_GLOBAL;
+            }
+            if (j < r1) ranks[gbase + j] = r;
+        }
     }
     __syncthreads();
-    // one reservation per bucket the tile uses
-    uint32_t* tb = base + (size_t)tile * t.M;
+    // one reservation per bucket the tile uses; the counter becomes its base
     for (uint32_t k = threadIdx.x; k < t.M; k += blockDim.x) {
         const uint32_t cnt = sc[k];
-        if (cnt) tb[k] = atomicAdd(&counts[kb + k], cnt);
+        sc[k] = cnt ? atomicAdd(&counts[kb + k], cnt) : 0u;
     }
-}
-
-// Scatter of a tiled ranking: position offsets[key] + the tile's reserved
-// base for the key + the local rank (or the global rank for RANK_GLOBAL).
-__global__ void k_scatter_tiles(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
-                                const uint32_t* __restrict__ ranks, uint32_t total,
-                                const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ base,
-                                RankTiles t, uint32_t* __restrict__ sorted) {
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= total) return;
-    const uint32_t key = keys[s];
-    if (key == KEY_SENTINEL) return;
-    const uint32_t r = ranks[s];
-    uint32_t pos = offsets[key];
-    if (r & RANK_GLOBAL) {
-        pos += r & ~RANK_GLOBAL;
-    } else {
-        const uint32_t g = s / t.n, j = s - g * t.n;
-        const uint32_t c = j / t.TS, q = (j - c * t.TS) / t.R;
-        const uint32_t tile = (c * t.G + g) * t.Q + q;
-        pos += base[(size_t)tile * t.M + (key - tile_key_base(t, c, g))] + r;
+    __syncthreads();
+    // rank within the bucket's run
+    for (uint32_t j0 = r0; j0 < r1; j0 += STEP) {
+        uint32_t key[RANK_TILE_U], r[RANK_TILE_U];
+#pragma unroll
+        for (int u = 0; u < RANK_TILE_U; ++u) {
+            const uint32_t j = j0 + u * RANK_TILE_THREADS + threadIdx.x;
+            key[u] = j < r1 ? keys[gbase + j] : KEY_SENTINEL;
+            r[u] = j < r1 ? ranks[gbase + j] : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < RANK_TILE_U; ++u) {
+            const uint32_t j = j0 + u * RANK_TILE_THREADS + threadIdx.x;
+            if (j >= r1 || key[u] == KEY_SENTINEL) continue;
+            ranks[gbase + j] = (r[u] & RANK_GLOBAL) ? (r[u] & ~RANK_GLOBAL) : sc[key[u] - kb] + r[u];
+        }
     }
-    sorted[pos] = vals[s];
 }
 
 __global__ void k_scatter(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
@@ -438,10 +439,9 @@ class MsmBatchPlan {
     uint32_t chunks = 1, B_sort = 0, chunk_rows = 0;
     bool red_quad = false;  // stage-1 reduction by quads of lanes (k_reduce_blocks_quad)
     // Tiled ranking (k_rank_tiles): one MSM, windows of at most RANK_TILE_M
-    // buckets, at least 2^20 entries; rt_chunks: the most row chunks the
-    // launch may split the rows into (tile bases reserved for that many).
+    // buckets, at least 2^20 entries.
     bool rank_tiles = false;
-    uint32_t rt_G = 0, rt_Q = 0, rt_M = 0, rt_chunks = 1;
+    uint32_t rt_G = 0, rt_Q = 0, rt_M = 0;
     std::vector<unsigned long long> chunk_len;
     DevBuf d_items, d_wins, d_blks;
     ~MsmBatchPlan() {
@@ -689,7 +689,6 @@ static void build_plan_host(MsmBatchPlan& P, int curve, const MsmItem* items, si
             P.rt_G = (uint32_t)(P.L / d.n);
             P.rt_Q = std::max<uint32_t>(1, ((uint32_t)device_sms() + P.rt_G - 1) / P.rt_G);
             P.rt_M = d.M;
-            P.rt_chunks = std::max<uint32_t>(P.chunks, (uint32_t)std::max(1, opt.point_chunks));
         }
     }
     // Chunk length: long chunks amortise the per-chunk records, but there must
@@ -770,7 +769,7 @@ class MsmEngine {
    public:
     int curve = 0;
     DevBuf table, keys, vals, counts, offsets, cursor, sorted, rec_first, rec_last, fold_buf,
-        buckets, blk_out, win_out, win_done, rank_base, scan_tmp, queue, fold_counts, fold_prefix, ranks, pair_off[2],
+        buckets, blk_out, win_out, win_done, scan_tmp, queue, fold_counts, fold_prefix, ranks, pair_off[2],
         pair_rows[2], pair_scratch, pair_cntT, pair_dst, pair_in1;
     std::map<std::tuple<size_t, bool, int, int, int, size_t, bool, size_t, int>, MsmBatchPlan*> single_plans;
     cudaEvent_t ev[N_STAGE_EVENTS] = {};
@@ -816,8 +815,7 @@ class MsmEngine {
             for (auto& c : ev_scal) cudaEventDestroy(c);
         }
         for (DevBuf* b : {&table, &keys, &vals, &counts, &offsets, &cursor, &sorted, &rec_first,
-                          &rec_last, &fold_buf, &buckets, &blk_out, &win_out, &win_done, &rank_base,
-                          &scan_tmp, &queue,
+                          &rec_last, &fold_buf, &buckets, &blk_out, &win_out, &win_done, &scan_tmp, &queue,
                           &fold_counts, &fold_prefix, &ranks, &pair_off[0], &pair_off[1], &pair_rows[0],
                           &pair_rows[1], &pair_scratch, &pair_cntT, &pair_dst, &pair_in1})
             b->release();
@@ -890,8 +888,6 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
     e->blk_out.reserve(std::max<size_t>(1, P.blks.size()) * 2 * PW * 4, st);
     e->win_out.reserve(std::max<size_t>(1, P.wins.size()) * PW * 4, st);
     e->win_done.reserve(std::max<size_t>(1, P.wins.size()) * 4, st);
-    if (P.rank_tiles)
-        e->rank_base.reserve((size_t)P.rt_chunks * P.rt_G * P.rt_Q * P.rt_M * 4, st);
     e->scan_tmp.reserve(
         scan_tmp_words(std::max<size_t>(BS, (size_t)std::max(1, P.levels) * P.big_cap) + 1) * 4, st);
     const size_t fold_all = (size_t)std::max(1, P.levels) * P.big_cap;
@@ -956,9 +952,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
         rt.bucket_base = d.bucket_base;
         rt.chunk_rows = d.chunk_rows;
         rt.chunk_stride = d.chunk_stride;
-        const bool fits = rt_chunks <= P.rt_chunks && (!d.chunk_rows || d.chunk_rows == rt.TS) &&
-                          e->rank_base.bytes >= (size_t)rt_chunks * rt.G * rt.Q * rt.M * 4;
-        if (!fits) rt_chunks = 0;
+        if (d.chunk_rows && d.chunk_rows != rt.TS) rt_chunks = 0;  // tiles must not straddle key chunks
     }
     const bool tiled = rt_chunks > 0;
     const size_t tile_smem = (size_t)rt.M * 4;
@@ -974,7 +968,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
             if (tiled) {
                 k_rank_tiles<<<dim3(rt.G * rt.Q, 1), RANK_TILE_THREADS, tile_smem, st>>>(
                     e->keys.as<uint32_t>(), rt, (uint32_t)c, e->counts.as<uint32_t>(),
-                    e->ranks.as<uint32_t>(), e->rank_base.as<uint32_t>());
+                    e->ranks.as<uint32_t>());
             } else {
                 k_rank_rows<<<ceil_div_u(G * (hi - lo), 256), 256, 0, st>>>(
                     e->keys.as<uint32_t>(), (uint32_t)n0, (uint32_t)G, (uint32_t)lo,
@@ -988,8 +982,7 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
                  e->vals.as<uint32_t>(), st);
         if (tiled) {
             k_rank_tiles<<<dim3(rt.G * rt.Q, rt_chunks), RANK_TILE_THREADS, tile_smem, st>>>(
-                e->keys.as<uint32_t>(), rt, 0u, e->counts.as<uint32_t>(), e->ranks.as<uint32_t>(),
-                e->rank_base.as<uint32_t>());
+                e->keys.as<uint32_t>(), rt, 0u, e->counts.as<uint32_t>(), e->ranks.as<uint32_t>());
         } else {
             k_rank<<<ceil_div_u(P.L, 256), 256, 0, st>>>(e->keys.as<uint32_t>(), P.L,
                                                         e->counts.as<uint32_t>(),
@@ -1002,16 +995,9 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
     exclusive_scan_u32(e->counts.as<uint32_t>(), e->offsets.as<uint32_t>(), BS, 0,
                        e->scan_tmp.as<uint32_t>(), st);
     if (P.L > 0) {
-        if (tiled) {
-            k_scatter_tiles<<<ceil_div_u(P.L, 256), 256, 0, st>>>(
-                e->keys.as<uint32_t>(), e->vals.as<uint32_t>(), e->ranks.as<uint32_t>(),
-                (uint32_t)P.L, e->offsets.as<uint32_t>(), e->rank_base.as<uint32_t>(), rt,
-                e->sorted.as<uint32_t>());
-        } else {
-            k_scatter<<<ceil_div_u(P.L, 256), 256, 0, st>>>(
-                e->keys.as<uint32_t>(), e->vals.as<uint32_t>(), e->ranks.as<uint32_t>(), P.L,
-                e->offsets.as<uint32_t>(), e->sorted.as<uint32_t>());
-        }
+        k_scatter<<<ceil_div_u(P.L, 256), 256, 0, st>>>(
+            e->keys.as<uint32_t>(), e->vals.as<uint32_t>(), e->ranks.as<uint32_t>(), P.L,
+            e->offsets.as<uint32_t>(), e->sorted.as<uint32_t>());
         KB_LAUNCH_CHECK();
     }
     e->mark(3, st);
