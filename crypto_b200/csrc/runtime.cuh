@@ -106,7 +106,9 @@ struct DevBuf {
             ptr = nullptr;
             bytes = 0;
         }
-        size_t want = need + need / 8 + 256;
+        // 1/8 headroom; on a deferring thread (a server under load, where an
+        // allocation can stall it) half again, so a buffer grows fewer times
+        size_t want = need + (t_devbuf_defer ? need / 2 : need / 8) + 256;
         KB_CUDA(cudaMalloc(&ptr, want));
         bytes = want;
         if (tr)

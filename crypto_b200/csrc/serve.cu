@@ -343,25 +343,42 @@ void* kzg_server_create(size_t max_batch, int slots, size_t mem_budget_bytes) {
             for (size_t n = 1; n <= s->srs_n; n <<= 1) cs.insert(shift_c_for(&n, 1));
             for (int c : cs) shift_tables_get(sh, c, s->slots[0].stream);
         }
-        // Warm every slot with one batch of the largest shape it is likely to
-        // see (a full-SRS commit plus max_batch - 1 commits of up to 2^16), so
-        // its engines and staging reach their working size before the first
-        // request instead of growing (and synchronising) under load.
+        // Warm every slot with the largest batches it is likely to see, so
+        // its engines, plans and staging reach their working size before the
+        // first request instead of growing under load (an allocation there
+        // waits on the device and, on a busy device, at times for hundreds
+        // of milliseconds): a full-SRS commit plus max_batch - 1 commits of up
+        // to 2^16, and for every window-size class the batcher groups commits
+        // by, max_batch commits of the class's largest size (at most 2^22
+        // evaluations in all).
         {
-            std::vector<size_t> sizes{s->srs_n};
-            const size_t mid = std::min<size_t>(s->srs_n, (size_t)1 << 16);
-            for (size_t k = 1; k < s->max_batch; ++k) sizes.push_back(mid);
-            size_t total = 0;
-            for (size_t v : sizes) total += v;
-            for (Slot& sl : s->slots) {
-                uint8_t* d_in = commit_batch_device_input(sl.batcher, sizes.data(), sizes.size(), s->srs,
-                                                          s->srs_n, sl.stream);
-                KB_CUDA(cudaMemsetAsync(d_in, 0, total * 32, sl.stream));
-                commit_batch_device(sl.batcher, sizes.data(), sizes.size(), s->srs, s->srs_n, sl.stream,
-                                    /*use_graph=*/false);
-                sl.h_out.reserve(s->max_batch * 48, sl.stream);
-                KB_CUDA(cudaStreamSynchronize(sl.stream));
+            std::vector<std::vector<size_t>> shapes;
+            {
+                std::vector<size_t> mixed{s->srs_n};
+                const size_t mid = std::min<size_t>(s->srs_n, (size_t)1 << 16);
+                for (size_t k = 1; k < s->max_batch; ++k) mixed.push_back(mid);
+                shapes.push_back(mixed);
             }
+            std::map<int, size_t> largest;  // window class -> largest size in it
+            for (size_t n = 1; n <= s->srs_n; n <<= 1) largest[shift_c_for(&n, 1)] = n;
+            for (const auto& kv : largest) {
+                const size_t n = kv.second;
+                const size_t cnt = std::max<size_t>(1, std::min(s->max_batch, ((size_t)1 << 22) / n));
+                shapes.push_back(std::vector<size_t>(cnt, n));
+            }
+            for (const auto& sizes : shapes) {
+                size_t total = 0;
+                for (size_t v : sizes) total += v;
+                for (Slot& sl : s->slots) {
+                    uint8_t* d_in = commit_batch_device_input(sl.batcher, sizes.data(), sizes.size(),
+                                                              s->srs, s->srs_n, sl.stream);
+                    KB_CUDA(cudaMemsetAsync(d_in, 0, total * 32, sl.stream));
+                    commit_batch_device(sl.batcher, sizes.data(), sizes.size(), s->srs, s->srs_n,
+                                        sl.stream, /*use_graph=*/false);
+                    KB_CUDA(cudaStreamSynchronize(sl.stream));
+                }
+            }
+            for (Slot& sl : s->slots) sl.h_out.reserve(s->max_batch * 48, sl.stream);
         }
         s->device_free();  // first admission snapshot, device idle after the warm-up
         s->worker = std::thread([s] { s->loop(); });
