@@ -757,6 +757,108 @@ __device__ __noinline__ void xyzz_add(const SmXyzz<F, S> p, const Q q) {
     p.put(1, U1);
 }
 
+// p += q (add-2008-s) for points in shared memory, the products spread over
+// the four lanes of a quad in four dependent levels as in xyzz_add_quad, but
+// with every operand and product passing through shared memory (t0, t1: two
+// scratch points of the quad, not aliasing p or q), so no lane holds a whole
+// point: for kernels whose register budget is tight, where the quad's latency
+// (four product latencies instead of fourteen) matters.  All four lanes of
+// the quad call it with the same arguments; q must not alias p.
+template <class F, int S>
+__device__ __noinline__ void xyzz_add_quad_sm(const SmXyzz<F, S> p, const SmXyzz<F, S> q,
+                                              const SmXyzz<F, S> t0, const SmXyzz<F, S> t1) {
+    const int ql = threadIdx.x & 3;
+    const unsigned qm = 0xFu << (threadIdx.x & 28);
+    if (q.is_inf()) return;
+    if (p.is_inf()) {
+        Fe<F> c;
+        q.get(ql, c);
+        p.put(ql, c);
+        __syncwarp(qm);
+        return;
+    }
+    Fe<F> a, b, r;
+    // level 1: U1 = X1 ZZ2 (0), U2 = X2 ZZ1 (1), S1 = Y1 ZZZ2 (2), S2 = Y2 ZZZ1 (3) -> t0
+    ((ql & 1) ? q : p).get(ql < 2 ? 0 : 1, a);
+    ((ql & 1) ? p : q).get(ql < 2 ? 2 : 3, b);
+    fe_mul(r, a, b);
+    t0.put(ql, r);
+    __syncwarp(qm);
+    Fe<F> P, R;
+    t0.get(0, a);
+    t0.get(1, P);
+    fe_sub(P, P, a);  // P = U2 - U1
+    t0.get(2, a);
+    t0.get(3, R);
+    fe_sub(R, R, a);  // R = S2 - S1
+    if (fe_is_zero(P)) {
+        __syncwarp(qm);
+        if (ql == 0) {
+            if (fe_is_zero(R))
+                xyzz_dbl(p);
+            else
+                p.set_inf();
+        }
+        __syncwarp(qm);
+        return;
+    }
+    // level 2: PP (0), RR (1), ZZ1 ZZ2 (2), ZZZ1 ZZZ2 (3) -> t1
+    if (ql >= 2) {
+        p.get(ql, a);
+        q.get(ql, b);
+    } else {
+        a = ql ? R : P;
+        b = a;
+    }
+    fe_mul(r, a, b);
+    t1.put(ql, r);
+    __syncwarp(qm);
+    // level 3: PPP = P PP (0) -> t0[1], Q = U1 PP (1) -> t0[3], ZZ3 = ZZ1 ZZ2 PP (2) -> p.ZZ
+    t1.get(0, b);
+    if (ql == 1)
+        t0.get(0, a);
+    else if (ql == 2)
+        t1.get(2, a);
+    else
+        a = P;
+    fe_mul(r, a, b);
+    if (ql == 0) t0.put(1, r);
+    if (ql == 1) t0.put(3, r);
+    if (ql == 2) p.put(2, r);
+    __syncwarp(qm);
+    // X3 = RR - PPP - 2Q
+    Fe<F> X3, QmX;
+    t1.get(1, X3);
+    t0.get(1, a);
+    fe_sub(X3, X3, a);
+    t0.get(3, QmX);
+    fe_sub(X3, X3, QmX);
+    fe_sub(X3, X3, QmX);
+    fe_sub(QmX, QmX, X3);
+    // level 4: R (Q - X3) (0), S1 PPP (1) -> t1[0], ZZZ3 = ZZZ1 ZZZ2 PPP (2) -> p.ZZZ
+    if (ql == 0) {
+        a = R;
+        b = QmX;
+    } else {
+        t0.get(1, b);
+        if (ql == 1)
+            t0.get(2, a);
+        else
+            t1.get(3, a);
+    }
+    fe_mul(r, a, b);
+    if (ql == 1) t1.put(0, r);
+    if (ql == 2) p.put(3, r);
+    __syncwarp(qm);
+    if (ql == 0) {
+        t1.get(0, a);
+        fe_sub(r, r, a);  // Y3 = R (Q - X3) - S1 PPP
+        p.put(0, X3);
+        p.put(1, r);
+    }
+    __syncwarp(qm);
+}
+
 // mdbl-2008-s-1 into a shared-memory point: p = 2 * (affine a).
 template <class F, int S>
 KB_DEV void xyzz_mdbl_sm(const SmXyzz<F, S>& p, const Affine<F>& a) {

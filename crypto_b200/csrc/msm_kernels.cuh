@@ -1073,6 +1073,26 @@ __device__ __forceinline__ void smem_tree_sum_quad(uint32_t* sm, int width) {
     }
 }
 
+// One level of a tree sum over shared-memory points (slot t += slot t + d
+// for t < d; every thread of the block calls it, a barrier follows): one
+// thread per slot while d > RED_QSLOTS, else one quad per slot with the
+// quad addition, its scratch in slots 2d + 2t and 2d + 2t + 1 (free at this
+// level of a tree over 4d or fewer live slots).
+template <class F>
+__device__ __forceinline__ void smem_tree_level(uint32_t* sm, int d) {
+    using SP = SmXyzz<F, RED_THREADS>;
+    const int me = threadIdx.x;
+    if (d > RED_QSLOTS) {
+        if (me < d) xyzz_add(SP{sm + me}, SP{sm + me + d});
+    } else {
+        const int sl = me >> 2;
+        if (sl < d)
+            xyzz_add_quad_sm(SP{sm + sl}, SP{sm + sl + d}, SP{sm + 2 * d + 2 * sl},
+                             SP{sm + 2 * d + 2 * sl + 1});
+    }
+    __syncthreads();
+}
+
 // Reduction stage 2 of window w over its nb <= RED_THREADS stage-1 results
 // (Fb, Sb):  V = sum_b Fb + BLK * sum_{b>=1} Y_b + Y_0, Y_b = sum_{b'>=b} Sb',
 // then the window weight 2^shift.  Run by all threads of the stage-1 block
@@ -1221,19 +1241,30 @@ __device__ __forceinline__ void reduce_window_sm(const RedArgs& a, uint32_t w, u
     }
     __syncthreads();
     // sum of Fb -> stash 0
-    for (int d = width >> 1; d >= 1; d >>= 1) {
-        if (me < d) xyzz_add(SP{sB + me}, SP{sB + me + d});
-        __syncthreads();
-    }
+    for (int d = width >> 1; d >= 1; d >>= 1) smem_tree_level<F>(sB, d);
     if (me == 0) xyzz_copy(S1{sX}, SP{sB});
     // suffix scan of Sb over the width slots, ping-pong between sA and sB
     uint32_t* src = sA;
     uint32_t* dst = sB;
     for (int d = 1; d < width; d <<= 1) {
-        if (me < width) {
-            const SP o{dst + me};
-            xyzz_copy(o, SP{src + me});
-            if (me + d < width) xyzz_add(o, SP{src + me + d});
+        if (width > RED_QSLOTS) {
+            if (me < width) {
+                const SP o{dst + me};
+                xyzz_copy(o, SP{src + me});
+                if (me + d < width) xyzz_add(o, SP{src + me + d});
+            }
+        } else {
+            // one quad per slot; scratch in dst slots width + 2 sl, + 1
+            const int sl = me >> 2, ql = me & 3;
+            if (sl < width) {
+                Fe<F> c;
+                SP{src + sl}.get(ql, c);
+                SP{dst + sl}.put(ql, c);
+                __syncwarp(0xFu << (me & 28));
+                if (sl + d < width)
+                    xyzz_add_quad_sm(SP{dst + sl}, SP{src + sl + d}, SP{dst + width + 2 * sl},
+                                     SP{dst + width + 2 * sl + 1});
+            }
         }
         __syncthreads();
         uint32_t* tmp = src;
@@ -1245,10 +1276,7 @@ __device__ __forceinline__ void reduce_window_sm(const RedArgs& a, uint32_t w, u
         SP{src}.set_inf();                // the tree below sums Y_b for b >= 1
     }
     __syncthreads();
-    for (int d = width >> 1; d >= 1; d >>= 1) {
-        if (me < d) xyzz_add(SP{src + me}, SP{src + me + d});
-        __syncthreads();
-    }
+    for (int d = width >> 1; d >= 1; d >>= 1) smem_tree_level<F>(src, d);
     // Warp 0: V = [blk] (sum over b >= 1 of Y_b) + sum Fb + Y_0, then the
     // window weight 2^shift; dst is free scratch now.
     if (me < 32) {
@@ -1391,10 +1419,7 @@ __global__ void __launch_bounds__(RED_THREADS, 2) k_reduce_blocks(RedArgs a) {
     }
     __syncthreads();
     // sum of T_t -> stash 0
-    for (int d = RED_THREADS >> 1; d >= 1; d >>= 1) {
-        if (me < d) xyzz_add(SP{sB + me}, SP{sB + me + d});
-        __syncthreads();
-    }
+    for (int d = RED_THREADS >> 1; d >= 1; d >>= 1) smem_tree_level<F>(sB, d);
     if (me == 0) xyzz_copy(S1{sX}, SP{sB});
     // suffix scan of R_t, ping-pong between sA and sB (8 steps: ends in sA)
     uint32_t* src = sA;
@@ -1413,10 +1438,7 @@ __global__ void __launch_bounds__(RED_THREADS, 2) k_reduce_blocks(RedArgs a) {
         SP{src}.set_inf();                // the tree below sums Y_t for t >= 1
     }
     __syncthreads();
-    for (int d = RED_THREADS >> 1; d >= 1; d >>= 1) {
-        if (me < d) xyzz_add(SP{src + me}, SP{src + me + d});
-        __syncthreads();
-    }
+    for (int d = RED_THREADS >> 1; d >= 1; d >>= 1) smem_tree_level<F>(src, d);
     if (me == 0) {
         // Fb = [S] (sum of Y_t, t >= 1) + sum of T_t, by double-and-add
         const SP Fb{src};
