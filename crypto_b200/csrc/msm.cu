@@ -125,13 +125,13 @@ __global__ void k_rank_rows(const uint32_t* __restrict__ keys, uint32_t n, uint3
 // A tile is a row range of one entry group (window, or window of a GLV half)
 // within one row chunk: all its keys lie in one window's bucket range, so its
 // block counts them in shared memory (local ranks), reserves each bucket's
-// places with one global atomic per distinct bucket (at the 2^22 headline a
-// tile of ~440 K entries over 32 K buckets: ~14x fewer global atomics than
-// one per entry), then adds the reserved base to every local rank, so the
-// plain scatter (offsets[key] + rank) follows.  Entries whose key falls
-// outside the tile's counter range (the GLV top window's buckets past M)
-// take a global atomic each.  Each thread handles RANK_TILE_U entries per
-// round, their loads issued together.
+// places with one global atomic per distinct bucket (at n = 2^22 with 16-bit
+// windows, a tile of ~440 K entries over 32 K buckets: ~14x fewer global
+// atomics than one per entry), then adds the reserved base to every local
+// rank, so the plain scatter (offsets[key] + rank) follows.  Entries whose
+// key falls outside the tile's counter range (the GLV top window's buckets
+// past M) take a global atomic each.  Each thread handles RANK_TILE_U
+// entries per round, their loads issued together.
 constexpr uint32_t RANK_TILE_M = 32768;          // shared-memory counters per tile (128 KiB)
 constexpr uint32_t RANK_GLOBAL = 0x80000000u;    // rank taken from the global count
 constexpr int RANK_TILE_THREADS = 1024;
