@@ -238,6 +238,67 @@ __global__ void k_scatter(const uint32_t* __restrict__ keys, const uint32_t* __r
     sorted[offsets[key] + ranks[t]] = vals[t];
 }
 
+// k_scatter over the entries of scalar rows [lo, lo + len) of one MSM of n
+// scalars (slots g * n + j, as k_rank_rows).
+__global__ void k_scatter_rows(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                               const uint32_t* __restrict__ ranks, uint32_t n, uint32_t G, uint32_t lo,
+                               uint32_t len, const uint32_t* __restrict__ offsets,
+                               uint32_t* __restrict__ sorted) {
+    const unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (unsigned long long)G * len) return;
+    const uint32_t g = (uint32_t)(t / len), j = lo + (uint32_t)(t % len);
+    const unsigned long long slot = (unsigned long long)g * n + j;
+    const uint32_t key = keys[slot];
+    if (key == KEY_SENTINEL) return;
+    sorted[offsets[key] + ranks[slot]] = vals[slot];
+}
+
+// Host-input pipeline, level 1 after the per-chunk first level: chunk c's
+// first-level sums of bucket b sit at rows off[c B + b] .. + ceil(len / 2)
+// (the sub-run's own entry positions).  tot[b] = the bucket's sums over the
+// chunks; idx lists them bucket by bucket (chunk by chunk inside a bucket),
+// so level 1 reads ordinary bucket runs through idx.
+__global__ void k_l1_totals(const uint32_t* __restrict__ off, uint32_t B, uint32_t CH,
+                            uint32_t* __restrict__ tot) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    uint32_t s = 0;
+    for (uint32_t c = 0; c < CH; ++c) s += (off[(size_t)c * B + b + 1] - off[(size_t)c * B + b] + 1) >> 1;
+    tot[b] = s;
+}
+
+// PAIR_J consecutive positions of idx per thread (the level's total is
+// in1[B]); in1 holds B + 1 run offsets.
+__global__ void k_l1_index(const uint32_t* __restrict__ off, const uint32_t* __restrict__ in1,
+                           uint32_t B, uint32_t CH, uint32_t* __restrict__ idx) {
+    const uint32_t total = in1[B];
+    const unsigned long long s0 = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) * PAIR_J;
+    if (s0 >= total) return;
+    const uint32_t send = (uint32_t)min((unsigned long long)total, s0 + PAIR_J);
+    uint32_t lo = 0, hi = B;  // largest b with in1[b] <= s0
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (in1[mid] <= (uint32_t)s0)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    uint32_t b = lo;
+    for (uint32_t s = (uint32_t)s0; s < send; ++s) {
+        while (in1[b + 1] <= s) ++b;
+        uint32_t p = s - in1[b];
+        for (uint32_t c = 0; c < CH; ++c) {
+            const uint32_t o = off[(size_t)c * B + b];
+            const uint32_t cnt = (off[(size_t)c * B + b + 1] - o + 1) >> 1;
+            if (p < cnt) {
+                idx[s] = o + p;
+                break;
+            }
+            p -= cnt;
+        }
+    }
+}
+
 // Lists buckets spanning more than K2 + 1 chunks (list = {count, ids});
 // only they go through the fold levels.
 __global__ void k_list_big(const uint32_t* __restrict__ offsets, uint32_t B, uint32_t K, int K2,
@@ -769,7 +830,7 @@ class MsmEngine {
    public:
     int curve = 0;
     DevBuf table, keys, vals, counts, offsets, cursor, sorted, rec_first, rec_last, fold_buf,
-        buckets, blk_out, win_out, win_done, scan_tmp, queue, fold_counts, fold_prefix, ranks, pair_off[2],
+        buckets, blk_out, win_out, win_done, l1_idx, chunk_base, scan_tmp, queue, fold_counts, fold_prefix, ranks, pair_off[2],
         pair_rows[2], pair_scratch, pair_cntT, pair_dst, pair_in1;
     std::map<std::tuple<size_t, bool, int, int, int, size_t, bool, size_t, int>, MsmBatchPlan*> single_plans;
     cudaEvent_t ev[N_STAGE_EVENTS] = {};
@@ -815,7 +876,8 @@ class MsmEngine {
             for (auto& c : ev_scal) cudaEventDestroy(c);
         }
         for (DevBuf* b : {&table, &keys, &vals, &counts, &offsets, &cursor, &sorted, &rec_first,
-                          &rec_last, &fold_buf, &buckets, &blk_out, &win_out, &win_done, &scan_tmp, &queue,
+                          &rec_last, &fold_buf, &buckets, &blk_out, &win_out, &win_done, &l1_idx,
+                          &chunk_base, &scan_tmp, &queue,
                           &fold_counts, &fold_prefix, &ranks, &pair_off[0], &pair_off[1], &pair_rows[0],
                           &pair_rows[1], &pair_scratch, &pair_cntT, &pair_dst, &pair_in1})
             b->release();
@@ -900,10 +962,18 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
             e->pair_cntT.reserve((BS + 1) * 4, st);
             e->pair_dst.reserve((BS + 1) * 4, st);
             e->pair_in1.reserve(((size_t)P.B + 1) * 4, st);
+            // host-input pipeline: per-chunk first-level offsets, level 1's
+            // index, the chunks' running totals
+            e->l1_idx.reserve((P.pair_len[0] + 1) * 4, st);
+            e->chunk_base.reserve(((size_t)P.chunks + 1) * 4, st);
         }
         for (int k = 0; k < 2 && k < P.pair_levels; ++k) {
-            e->pair_off[k].reserve((BS + 1) * 4, st);
-            e->pair_rows[k].reserve(std::max<unsigned long long>(1, P.pair_len[k]) * TW * 4, st);
+            e->pair_off[k].reserve((BS + P.chunks + 1) * 4, st);
+            // chunked: the first level writes each sub-run's sums at its own
+            // entry positions (up to L rows)
+            const unsigned long long rows =
+                (k == 0 && P.chunks > 1) ? std::max<unsigned long long>(P.pair_len[0], P.L) : P.pair_len[k];
+            e->pair_rows[k].reserve(std::max<unsigned long long>(1, rows) * TW * 4, st);
         }
         e->pair_scratch.reserve(pair_scratch_words(pair_threads(P.pair_len[0]), (int)TW / 2) * 4, st);
     }
@@ -957,24 +1027,63 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
     const bool tiled = rt_chunks > 0;
     const size_t tile_smem = (size_t)rt.M * 4;
     if (tiled) set_smem_attr((const void*)k_rank_tiles, tile_smem);
+    // Host-input pipeline with the first pairing level per row chunk: every
+    // chunk is sorted (its keys are its own range, chunk-major), scanned from
+    // the previous chunk's total and paired as soon as its own scalars and
+    // points are resident, instead of after every scalar; level 1 then reads
+    // the chunks' sums through an index (k_l1_index).
+    const size_t S_rows = n_ready > 0 ? (n0 + n_ready - 1) / n_ready : 0;
+    const bool pipelined = by_rows && P.chunks > 1 && P.pair_levels > 0 && table_ready &&
+                           n_ready == (int)P.chunks && P.chunk_rows == S_rows &&
+                           P.items[0].chunk_stride == P.B;
     if (by_rows) {
-        const size_t G = P.L / n0, S = (n0 + n_ready - 1) / n_ready;
+        const size_t G = P.L / n0, S = S_rows;
         for (int c = 0; c < n_ready; ++c) {
             const size_t lo = std::min(n0, (size_t)c * S), hi = std::min(n0, lo + S);
             KB_CUDA(cudaStreamWaitEvent(st, scalars_ready[c], 0));
-            if (hi == lo) continue;
+            if (hi == lo && !pipelined) continue;
             K.recode(items, nitems, lo, hi - lo, scal, rec_table, e->keys.as<uint32_t>(),
                      e->vals.as<uint32_t>(), st);
             if (tiled) {
                 k_rank_tiles<<<dim3(rt.G * rt.Q, 1), RANK_TILE_THREADS, tile_smem, st>>>(
                     e->keys.as<uint32_t>(), rt, (uint32_t)c, e->counts.as<uint32_t>(),
                     e->ranks.as<uint32_t>());
-            } else {
+            } else if (hi > lo) {
                 k_rank_rows<<<ceil_div_u(G * (hi - lo), 256), 256, 0, st>>>(
                     e->keys.as<uint32_t>(), (uint32_t)n0, (uint32_t)G, (uint32_t)lo,
                     (uint32_t)(hi - lo), e->counts.as<uint32_t>(), e->ranks.as<uint32_t>());
             }
             KB_LAUNCH_CHECK();
+            if (!pipelined) continue;
+            // chunk c: bucket offsets (keys c B .. c B + B - 1) from the
+            // previous chunk's total, scatter, first pairing level
+            const uint32_t B = P.B;
+            uint32_t* offs = e->offsets.as<uint32_t>() + (size_t)c * B;
+            uint32_t* cnt = e->counts.as<uint32_t>() + (size_t)c * B;
+            uint32_t* bases = e->chunk_base.as<uint32_t>();
+            exclusive_scan_u32_chained(cnt, offs, B, 0, c ? bases + c : nullptr, bases + c + 1,
+                                       e->scan_tmp.as<uint32_t>(), st);
+            if (hi > lo) {
+                k_scatter_rows<<<ceil_div_u(G * (hi - lo), 256), 256, 0, st>>>(
+                    e->keys.as<uint32_t>(), e->vals.as<uint32_t>(), e->ranks.as<uint32_t>(),
+                    (uint32_t)n0, (uint32_t)G, (uint32_t)lo, (uint32_t)(hi - lo),
+                    e->offsets.as<uint32_t>(), e->sorted.as<uint32_t>());
+                KB_LAUNCH_CHECK();
+            }
+            uint32_t* out0 = e->pair_off[0].as<uint32_t>() + (size_t)c * (B + 1);
+            k_pair_counts<<<ceil_div_u(B, 256), 256, 0, st>>>(offs, B, cnt);
+            KB_LAUNCH_CHECK();
+            exclusive_scan_u32(cnt, out0, B, 0, e->scan_tmp.as<uint32_t>(), st);
+            KB_CUDA(cudaStreamWaitEvent(st, table_ready[c], 0));
+            PairArgs pa;
+            pa.in_off = offs;
+            pa.out_off = out0;
+            pa.B = B;
+            pa.sorted = e->sorted.as<uint32_t>();
+            pa.src = d_table;
+            pa.dst = e->pair_rows[0].as<uint32_t>();
+            pa.dst_off = offs;  // a sub-run's sums at its own entry positions
+            K.pair_level(pa, pair_threads(P.chunk_len[c]), e->pair_scratch.as<uint32_t>(), st);
         }
     } else if (P.L > 0) {
         if (scalars_ready && n_ready > 0) KB_CUDA(cudaStreamWaitEvent(st, scalars_ready[n_ready - 1], 0));
@@ -992,9 +1101,10 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
     }
     e->mark(2, st);
     lap(2);
-    exclusive_scan_u32(e->counts.as<uint32_t>(), e->offsets.as<uint32_t>(), BS, 0,
-                       e->scan_tmp.as<uint32_t>(), st);
-    if (P.L > 0) {
+    if (!pipelined)
+        exclusive_scan_u32(e->counts.as<uint32_t>(), e->offsets.as<uint32_t>(), BS, 0,
+                           e->scan_tmp.as<uint32_t>(), st);
+    if (P.L > 0 && !pipelined) {
         k_scatter<<<ceil_div_u(P.L, 256), 256, 0, st>>>(
             e->keys.as<uint32_t>(), e->vals.as<uint32_t>(), e->ranks.as<uint32_t>(), P.L,
             e->offsets.as<uint32_t>(), e->sorted.as<uint32_t>());
@@ -1005,13 +1115,30 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
     const bool per_chunk = P.chunks > 1 && table_ready && n_ready == (int)P.chunks && P.L > 0;
     if (table_ready && n_ready > 0 && !per_chunk)
         KB_CUDA(cudaStreamWaitEvent(st, table_ready[n_ready - 1], 0));
+    if (pipelined) {
+        // level 1's runs: bucket by bucket over the chunks' first-level sums
+        const uint32_t CH = P.chunks, B = P.B;
+        k_l1_totals<<<ceil_div_u(B, 256), 256, 0, st>>>(e->offsets.as<uint32_t>(), B, CH,
+                                                       e->counts.as<uint32_t>());
+        KB_LAUNCH_CHECK();
+        exclusive_scan_u32(e->counts.as<uint32_t>(), e->pair_in1.as<uint32_t>(), B, 0,
+                           e->scan_tmp.as<uint32_t>(), st);
+        k_l1_index<<<ceil_div_u(pair_threads(P.pair_len[0]), 256), 256, 0, st>>>(
+            e->offsets.as<uint32_t>(), e->pair_in1.as<uint32_t>(), B, CH, e->l1_idx.as<uint32_t>());
+        KB_LAUNCH_CHECK();
+    }
     // Pairing levels: the sorted runs shrink to about half per level, the
     // accumulation then reads the last level's rows directly.
     const uint32_t* off = e->offsets.as<uint32_t>();
     const uint32_t* acc_sorted = e->sorted.as<uint32_t>();
     const uint32_t* acc_table = d_table;
     int l0 = 0;
-    if (P.chunks > 1 && P.pair_levels > 0 && P.L > 0) {
+    if (pipelined) {
+        off = e->pair_in1.as<uint32_t>();
+        acc_sorted = e->l1_idx.as<uint32_t>();
+        acc_table = e->pair_rows[0].as<uint32_t>();
+        l0 = 1;
+    } else if (P.chunks > 1 && P.pair_levels > 0 && P.L > 0) {
         // Level 0 per chunk of points: sub-run (c, b) pairs only the points of
         // chunk c, so chunk c runs as soon as its rows exist; its sums land
         // at bucket-major rows, so level 1 reads ordinary bucket runs.
@@ -1228,19 +1355,22 @@ void msm_run_host_wire(MsmEngine* e, const uint8_t* h_scalars, const uint8_t* h_
     KB_CUDA(cudaStreamWaitEvent(e->st_conv, e->ev_start, 0));
     // chunk c = rows [c S, (c + 1) S), S = ceil(n / chunks): the rows the
     // plan's chunk-major sort keys (when it pairs per chunk) assign to c.
-    // One copy stream, all scalars first: the sort needs every scalar before
-    // the first pairing level, the points only chunk by chunk after it; each
-    // scalar chunk's recode and ranking run while the next chunk copies.
+    // One copy stream.  When the plan pairs per chunk, chunk by chunk (its
+    // scalars, then its points): each chunk is sorted and paired once both
+    // are resident.  Otherwise all scalars first (the sort needs every key
+    // before the first pairing level), each scalar chunk recoded and ranked
+    // as it lands, then the points.
     const size_t S = (n + chunks - 1) / chunks;
-    for (size_t c = 0; c < chunks; ++c) {
+    const bool interleave = p->chunks == chunks && p->pair_levels > 0 && chunks > 1;
+    auto copy_scalars = [&](size_t c) {
         const size_t lo = std::min(n, c * S), hi = std::min(n, lo + S);
         if (hi > lo) {
             KB_CUDA(cudaMemcpyAsync(d_scalars + lo * 32, h_scalars + lo * 32, (hi - lo) * 32,
                                     cudaMemcpyHostToDevice, e->st_copy));
         }
         KB_CUDA(cudaEventRecord(e->ev_scal[c], e->st_copy));
-    }
-    for (size_t c = 0; c < chunks; ++c) {
+    };
+    auto copy_points = [&](size_t c) {
         const size_t lo = std::min(n, c * S), hi = std::min(n, lo + S);
         if (hi > lo) {
             KB_CUDA(cudaMemcpyAsync(d_points + lo * WB, h_points + lo * WB, (hi - lo) * WB,
@@ -1250,6 +1380,15 @@ void msm_run_host_wire(MsmEngine* e, const uint8_t* h_scalars, const uint8_t* h_
         KB_CUDA(cudaStreamWaitEvent(e->st_conv, e->ev_chunk[c], 0));
         K.wire_to_table(d_points + lo * WB, table + lo * TW, hi - lo, glv ? n : 0, e->st_conv);
         KB_CUDA(cudaEventRecord(e->ev_conv[c], e->st_conv));
+    };
+    if (interleave) {
+        for (size_t c = 0; c < chunks; ++c) {
+            copy_scalars(c);
+            copy_points(c);
+        }
+    } else {
+        for (size_t c = 0; c < chunks; ++c) copy_scalars(c);
+        for (size_t c = 0; c < chunks; ++c) copy_points(c);
     }
     e->mark(0, st);
     e->mark(1, st);

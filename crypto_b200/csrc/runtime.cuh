@@ -162,6 +162,12 @@ struct HostBuf {
 size_t scan_tmp_words(size_t n);
 void exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t div,
                         uint32_t* tmp, cudaStream_t stream);
+// The same starting from the device value *init (0 if null), the total also
+// written to *total_copy (if not null): consecutive ranges of one array
+// scanned in turn, each from the previous range's total, without the host.
+void exclusive_scan_u32_chained(const uint32_t* in, uint32_t* out, size_t n, uint32_t div,
+                                const uint32_t* init, uint32_t* total_copy, uint32_t* tmp,
+                                cudaStream_t stream);
 
 inline unsigned ceil_div_u(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
 

@@ -65,12 +65,13 @@ __global__ void k_scan_tiles(const uint32_t* __restrict__ in, uint32_t* __restri
     if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
 }
 
-// Single block: exclusive scan of the tile totals in place; writes the grand
-// total to out[n].
+// Single block: exclusive scan of the tile totals in place, starting from
+// *init (0 if null); writes the grand total to out[n] (and to *total_copy).
 __global__ void k_scan_sums(uint32_t* __restrict__ sums, unsigned nt, uint32_t* __restrict__ out,
-                            size_t n) {
+                            size_t n, const uint32_t* __restrict__ init,
+                            uint32_t* __restrict__ total_copy) {
     __shared__ uint32_t carry;
-    if (threadIdx.x == 0) carry = 0;
+    if (threadIdx.x == 0) carry = init ? *init : 0u;
     __syncthreads();
     for (unsigned base = 0; base < nt; base += blockDim.x) {
         unsigned i = base + threadIdx.x;
@@ -82,7 +83,10 @@ __global__ void k_scan_sums(uint32_t* __restrict__ sums, unsigned nt, uint32_t* 
         if (threadIdx.x == 0) carry += total;
         __syncthreads();
     }
-    if (threadIdx.x == 0) out[n] = carry;
+    if (threadIdx.x == 0) {
+        out[n] = carry;
+        if (total_copy) *total_copy = carry;
+    }
 }
 
 __global__ void k_scan_fix(uint32_t* __restrict__ out, size_t n, const uint32_t* __restrict__ sums) {
@@ -99,14 +103,25 @@ size_t scan_tmp_words(size_t n) { return (n + SCAN_TILE - 1) / SCAN_TILE + 1; }
 
 void exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t div,
                         uint32_t* tmp, cudaStream_t stream) {
+    exclusive_scan_u32_chained(in, out, n, div, nullptr, nullptr, tmp, stream);
+}
+
+void exclusive_scan_u32_chained(const uint32_t* in, uint32_t* out, size_t n, uint32_t div,
+                                const uint32_t* init, uint32_t* total_copy, uint32_t* tmp,
+                                cudaStream_t stream) {
     const unsigned nt = (unsigned)((n + SCAN_TILE - 1) / SCAN_TILE);
     if (nt == 0) {
-        KB_CUDA(cudaMemsetAsync(out, 0, sizeof(uint32_t), stream));
+        if (init || total_copy) {
+            k_scan_sums<<<1, SCAN_THREADS, 0, stream>>>(tmp, 0, out, 0, init, total_copy);
+            KB_LAUNCH_CHECK();
+        } else {
+            KB_CUDA(cudaMemsetAsync(out, 0, sizeof(uint32_t), stream));
+        }
         return;
     }
     k_scan_tiles<<<nt, SCAN_THREADS, 0, stream>>>(in, out, n, div, tmp);
     KB_LAUNCH_CHECK();
-    k_scan_sums<<<1, SCAN_THREADS, 0, stream>>>(tmp, nt, out, n);
+    k_scan_sums<<<1, SCAN_THREADS, 0, stream>>>(tmp, nt, out, n, init, total_copy);
     KB_LAUNCH_CHECK();
     k_scan_fix<<<nt, SCAN_THREADS, 0, stream>>>(out, n, tmp);
     KB_LAUNCH_CHECK();
