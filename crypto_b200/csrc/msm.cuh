@@ -159,11 +159,13 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
 void msm_run_wire(MsmEngine* e, const uint8_t* d_scalars, const uint8_t* d_points, size_t n,
                   uint8_t* d_out_wire, uint8_t* d_out_comp, cudaStream_t stream,
                   const MsmOptions& opt);
-// From host buffers: one copy stream brings the scalars, then the points,
-// in row chunks; each scalar chunk is recoded and ranked on `stream` as it
-// lands, each point chunk converted to table rows on a third stream and
-// paired (first level) as soon as the sort is done; d_scalars (n * 32
-// bytes) and d_points (n * WIRE bytes) are the staging.
+// From host buffers: one copy stream brings the scalars and the points in
+// row chunks, each point chunk converted to table rows on a third stream.
+// When the plan pairs per chunk, chunk by chunk: each chunk is sorted and
+// paired (first level) on `stream` once its own scalars and points are
+// resident; otherwise all scalars first, each chunk recoded and ranked as it
+// lands.  d_scalars (n * 32 bytes) and d_points (n * WIRE bytes) are the
+// staging.
 void msm_run_host_wire(MsmEngine* e, const uint8_t* h_scalars, const uint8_t* h_points, size_t n,
                        uint8_t* d_scalars, uint8_t* d_points, uint8_t* d_out_wire,
                        cudaStream_t stream, const MsmOptions& opt);

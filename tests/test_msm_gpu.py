@@ -342,9 +342,9 @@ print("ok")
 @pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("curve,logn", [(2, 20), (1, 17), (1, 20)])
 def test_host_pipeline_with_infinity_points(cuda_lib, curve, logn, path):
-    """gpukit_multi_pippenger copies the scalars and then the points in row
-    chunks (four at these sizes), recodes and ranks each scalar chunk as it
-    lands and converts each point chunk on its own stream, so infinity
+    """gpukit_multi_pippenger copies the scalars and the points in row chunks
+    (four at these sizes), sorting and pairing each chunk as it lands when the
+    plan pairs, and converts each point chunk on its own stream, so infinity
     points reach the buckets and are skipped there: one point in eight is
     the identity (and, at 2^20 on BLS12-381, with pairing levels)."""
     n = 1 << logn
