@@ -454,3 +454,44 @@ print("ok")
     out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True,
                          text=True, timeout=900)
     assert out.returncode == 0 and "ok" in out.stdout, out.stdout + out.stderr
+
+
+@pytest.mark.parametrize("chunks", [3, 7])
+@pytest.mark.parametrize("curve", [1, 2])
+def test_host_pipeline_pairs_per_uneven_chunk(cuda_lib, curve, chunks):
+    """At a size whose plan pairs (2^20 + 3 points) the host pipeline sorts
+    and pairs each row chunk once its own scalars and points are resident:
+    chunk scans chained on the device, first-level sums at their entry
+    positions, level 1 through the chunks' index.  Row chunks that do not
+    divide n, infinity points and repeated points among the inputs; the
+    bytes equal the reference's."""
+    import os
+    import subprocess
+    import sys
+    code = r'''
+import random, sys
+sys.path.insert(0, "tests")
+import crypto_b200 as kb, _oracle as O
+from test_msm_gpu import rand_points
+curve = %d
+n = (1 << 20) + 3
+pb = O.PB[curve]
+pts = bytearray(rand_points(curve, n, seed=170 + curve))
+rng = random.Random(170 + curve)
+for j in rng.sample(range(n), 64):
+    pts[pb * j:pb * (j + 1)] = bytes(pb)
+for j in rng.sample(range(1, n), 64):
+    pts[pb * j:pb * (j + 1)] = pts[pb * (j - 1):pb * j]
+pts = bytes(pts)
+S = b"".join(rng.randrange(O.FR[curve]).to_bytes(32, "little") for _ in range(n))
+want = O.ref_msm(curve, S, pts, n, threads=16) if O.ref_available() else O.msm(curve, S, pts, n)
+for path in ("plain", "subgroup"):
+    f = kb.gpukit_multi_pippenger if path == "plain" else kb.gpukit_multi_pippenger_subgroup
+    assert f(curve, S, pts, n) == want, path
+print("ok")
+''' % curve
+    env = dict(os.environ, KB200_MSM_HOST_CHUNKS=str(chunks))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True,
+                         text=True, timeout=1200)
+    assert out.returncode == 0 and "ok" in out.stdout, out.stdout + out.stderr
