@@ -315,19 +315,37 @@ KB_DEV void mont_reduce_wide(Fe<F>& r, uint32_t* T) {
     uint32_t pc[N + 1];
 #pragma unroll
     for (int k = 0; k <= N; ++k) pc[k] = 0;
+    // A modulus with low words 1 and 2^32 - 1 (the BLS12-381 scalar field r)
+    // needs no multiply for them: m_i = -T[i] (as -p^-1 = 2^32 - 1), m_i * 1
+    // = m_i makes word i zero with a carry iff T[i] != 0, and m_i (2^32 - 1)
+    // = (T[i], T[i] ? ~T[i] : 0) as (low, high) words.  Five integer
+    // multiply-adds fewer per row, 40 of 232 per product for N = 8.
+    constexpr bool LOW_ONE = F::P(0) == 1u && F::P(1) == 0xffffffffu;
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-        const uint32_t m = T[i] * F::M0;
-        T[i] = mad_lo_cc(m, F::P(0), T[i]);
-        T[i + 1] = madc_hi_cc(m, F::P(0), T[i + 1]);
+        const uint32_t t = T[i];
+        const uint32_t m = LOW_ONE ? 0u - t : t * F::M0;
+        if constexpr (LOW_ONE) {
+            T[i] = add_cc(t, m);
+            T[i + 1] = addc_cc(T[i + 1], 0u);
+        } else {
+            T[i] = mad_lo_cc(m, F::P(0), T[i]);
+            T[i + 1] = madc_hi_cc(m, F::P(0), T[i + 1]);
+        }
 #pragma unroll
         for (int j = 2; j < N; j += 2) {
             T[i + j] = madc_lo_cc(m, F::P(j), T[i + j]);
             T[i + j + 1] = madc_hi_cc(m, F::P(j), T[i + j + 1]);
         }
         pc[i] = addc_u32(pc[i], 0);
-        T[i + 1] = mad_lo_cc(m, F::P(1), T[i + 1]);
-        T[i + 2] = madc_hi_cc(m, F::P(1), T[i + 2]);
+        if constexpr (LOW_ONE) {
+            const uint32_t hi = t ? ~t : 0u;
+            T[i + 1] = add_cc(T[i + 1], t);
+            T[i + 2] = addc_cc(T[i + 2], hi);
+        } else {
+            T[i + 1] = mad_lo_cc(m, F::P(1), T[i + 1]);
+            T[i + 2] = madc_hi_cc(m, F::P(1), T[i + 2]);
+        }
 #pragma unroll
         for (int j = 3; j < N - 1; j += 2) {
             T[i + j] = madc_lo_cc(m, F::P(j), T[i + j]);
