@@ -373,7 +373,10 @@ KB_DEV void mont_reduce_wide(Fe<F>& r, uint32_t* T) {
 // on the BLS12-381 MSM at 2^22: every product in the Karatsuba form but the
 // two inlined recovery products of the pairing levels 27.19 ms; those two
 // in the Karatsuba form too 27.11 ms (more registers); all in this form
-// 28.21 ms; the two recovery products out of line 28.03 ms.
+// 28.21 ms; the two recovery products out of line 28.03 ms.  With the later
+// kernels (tiled ranking, fused reduction) the Karatsuba recovery products
+// lost on both curves: pair stage 20.35 -> 20.61 ms (BLS12-381 2^22), 39.57
+// -> 39.70 ms (BN254 2^24), with BLS12-381 spills of 260 bytes.
 template <class F>
 KB_DEV void fe_mul_inl(Fe<F>& r, const Fe<F>& a, const Fe<F>& b) {
     constexpr int N = F::N;
