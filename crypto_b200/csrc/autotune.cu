@@ -34,6 +34,31 @@ static std::string device_key() {
     return name + "|" + std::to_string(drv);
 }
 
+// The choice among candidates: the default (the cost model's) unless the
+// fastest candidate beats it by more than TUNE_MARGIN, so that timing noise
+// on short runs does not move the choice from run to run.
+constexpr float TUNE_MARGIN = 0.03f;
+static int pick_fastest(int def, const std::vector<int>& cands, const std::function<float(int)>& time_of,
+                        float* best_ms) {
+    const float t_def = time_of(def);
+    int best = def;
+    float best_t = t_def;
+    for (int c : cands) {
+        if (c == def) continue;
+        const float t = time_of(c);
+        if (t < best_t) {
+            best_t = t;
+            best = c;
+        }
+    }
+    if (best_t < t_def * (1.0f - TUNE_MARGIN)) {
+        *best_ms = best_t;
+        return best;
+    }
+    *best_ms = t_def;
+    return def;
+}
+
 static float time_ms(cudaStream_t st, const std::function<void()>& fn, int reps) {
     cudaEvent_t a, b;
     KB_CUDA(cudaEventCreate(&a));
@@ -88,21 +113,18 @@ int kb200_autotune(uint32_t curve, int log_lo, int log_hi, const char* cache_pat
             const size_t n = (size_t)1 << lg;
             MsmOptions base;
             const int c0 = make_msm_plan((int)curve, n, base).c;
-            int best_c = c0;
-            float best = 1e30f;
-            for (int c = std::max(4, c0 - 2); c <= std::min(20, c0 + 2); ++c) {
+            const int reps = lg >= 20 ? 2 : (lg >= 16 ? 5 : 20);
+            std::vector<int> cs;
+            for (int c = std::max(4, c0 - 2); c <= std::min(20, c0 + 2); ++c) cs.push_back(c);
+            float best = 0;
+            const int best_c = pick_fastest(c0, cs, [&](int c) {
                 MsmOptions o;
                 o.force_c = c;
-                const int reps = lg >= 20 ? 2 : 5;
-                const float ms = time_ms(st, [&] {
+                return time_ms(st, [&] {
                     msm_run_table(eng, sc.as<uint8_t>(), table.as<uint32_t>(), n,
                                   out.as<uint8_t>(), nullptr, st, o);
                 }, reps);
-                if (ms < best) {
-                    best = ms;
-                    best_c = c;
-                }
-            }
+            }, &best);
             msm_tune_set((int)curve, lg, best_c, false);
             log << key << " msm " << curve << " " << lg << " " << best_c << " " << best << "\n";
             // windows of the GLV halves (the wire path with the G1 promise:
@@ -111,45 +133,37 @@ int kb200_autotune(uint32_t curve, int log_lo, int log_hi, const char* cache_pat
                 MsmOptions g;
                 g.points_in_g1 = true;
                 const int g0 = make_msm_plan_glv((int)curve, n, g).c;
-                int best_g = g0;
-                float best_gt = 1e30f;
-                for (int c = std::max(4, g0 - 2); c <= std::min(20, g0 + 2); ++c) {
+                std::vector<int> gs;
+                for (int c = std::max(4, g0 - 2); c <= std::min(20, g0 + 2); ++c) gs.push_back(c);
+                float best_gt = 0;
+                const int best_g = pick_fastest(g0, gs, [&](int c) {
                     MsmOptions o;
                     o.force_c = c;
                     o.points_in_g1 = true;
-                    const int reps = lg >= 20 ? 2 : 5;
-                    const float ms = time_ms(st, [&] {
+                    return time_ms(st, [&] {
                         msm_run_wire(eng, sc.as<uint8_t>(), pts.as<uint8_t>(), n, out.as<uint8_t>(),
                                      nullptr, st, o);
                     }, reps);
-                    if (ms < best_gt) {
-                        best_gt = ms;
-                        best_g = c;
-                    }
-                }
+                }, &best_gt);
                 msm_tune_set((int)curve, lg, best_g, true);
                 log << key << " msm_glv " << curve << " " << lg << " " << best_g << " " << best_gt << "\n";
             }
             // NTT first-pass radix (two- and three-pass sizes)
             if (lg > 12) {
                 KB_CUDA(cudaMemcpyAsync(nt.ptr, sc.ptr, n * 32, cudaMemcpyDeviceToDevice, st));
-                int best_r = 0;
-                float best_t = 1e30f;
                 std::vector<int> cands;
                 for (int r1 = 3; r1 <= 10; ++r1) {
                     const int rest = lg - r1;
                     if (lg <= 20 ? (rest >= 3 && rest <= 10) : (rest >= 6 && rest <= 20)) cands.push_back(r1);
                 }
-                for (int r1 : cands) {
+                // 0 = the planner's own split; short transforms get enough
+                // repetitions for about a millisecond of work each
+                const int nreps = lg <= 16 ? 40 : (lg <= 20 ? 8 : 3);
+                float best_t = 0;
+                const int best_r = pick_fastest(0, cands, [&](int r1) {
                     ntt_tune_set((int)curve, lg, r1);
-                    const float ms = time_ms(st, [&] {
-                        ntt_run(ntt, nt.as<uint32_t>(), n, 0, 0, 1, st);
-                    }, 3);
-                    if (ms < best_t) {
-                        best_t = ms;
-                        best_r = r1;
-                    }
-                }
+                    return time_ms(st, [&] { ntt_run(ntt, nt.as<uint32_t>(), n, 0, 0, 1, st); }, nreps);
+                }, &best_t);
                 ntt_tune_set((int)curve, lg, best_r);
                 log << key << " ntt " << curve << " " << lg << " " << best_r << " " << best_t << "\n";
             }
