@@ -264,7 +264,16 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(PassArgs a) {
             st_elt(p0, t);
             st_elt(p1, v);
         }
-        __syncthreads();
+        // From half-length 32 down, the 32 butterflies of a warp (32
+        // consecutive b, block size a multiple of 32) touch only their own 64
+        // consecutive elements of one sub-vector (or whole sub-vectors when
+        // R <= 32), at this stage and the next: the warp alone consumes what
+        // it wrote, so only the warp synchronises; every other stage, and the
+        // last (the store reads any element), synchronise the block.
+        if (log_half <= 5 && s + 1 < a.log_R)
+            __syncwarp();
+        else
+            __syncthreads();
     }
 
     // Store: DFT output j of sub-vector c sits at bitrev(j).
