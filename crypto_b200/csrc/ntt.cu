@@ -239,38 +239,49 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(PassArgs a) {
     }
     __syncthreads();
 
-    // Radix-2 DIF stages on each of the cb sub-vectors of length R.
+    // Radix-2 DIF stages on each of the cb sub-vectors of length R.  When
+    // every thread has the same number `per` of butterflies per stage, warp w
+    // takes butterflies [32 per w, 32 per (w + 1)), so from half-length
+    // 32 per down a warp's butterflies touch only its own 64 per consecutive
+    // elements of one sub-vector (or whole sub-vectors when R / 2 <= 32 per),
+    // at that stage and the next: the warp alone consumes what it wrote, and
+    // only the warp synchronises.  Every other stage, and the last (the store
+    // reads any element), synchronise the block.
     const int half_total = tot >> 1;
+    const int per = (half_total >= (int)blockDim.x && half_total % (int)blockDim.x == 0)
+                        ? half_total / (int)blockDim.x
+                        : 0;
+    const int log_local = 5 + (per > 1 ? 31 - __clz(per) : 0);
+    auto butterfly = [&](int s, int log_half, int b) {
+        const int c = b >> (a.log_R - 1);
+        const int bb = b & ((R >> 1) - 1);
+        const int j = bb & ((1 << log_half) - 1);
+        const int i0 = ((bb >> log_half) << (log_half + 1)) + j;
+        const int i1 = i0 + (1 << log_half);
+        uint32_t* p0 = sm + (size_t)((c << a.log_R) + i0) * 8;
+        uint32_t* p1 = sm + (size_t)((c << a.log_R) + i1) * 8;
+        Fe<F> u, v, t;
+        ld_elt(u, p0);
+        ld_elt(v, p1);
+        fe_add(t, u, v);
+        fe_sub(v, u, v);
+        if (j) {
+            Fe<F> w;
+            ld_elt(w, stw + (size_t)(j << s) * 8);
+            fe_mul(v, v, w);
+        }
+        st_elt(p0, t);
+        st_elt(p1, v);
+    };
     for (int s = 0; s < a.log_R; ++s) {
         const int log_half = a.log_R - 1 - s;
-        for (int b = threadIdx.x; b < half_total; b += blockDim.x) {
-            const int c = b >> (a.log_R - 1);
-            const int bb = b & ((R >> 1) - 1);
-            const int j = bb & ((1 << log_half) - 1);
-            const int i0 = ((bb >> log_half) << (log_half + 1)) + j;
-            const int i1 = i0 + (1 << log_half);
-            uint32_t* p0 = sm + (size_t)((c << a.log_R) + i0) * 8;
-            uint32_t* p1 = sm + (size_t)((c << a.log_R) + i1) * 8;
-            Fe<F> u, v, t;
-            ld_elt(u, p0);
-            ld_elt(v, p1);
-            fe_add(t, u, v);
-            fe_sub(v, u, v);
-            if (j) {
-                Fe<F> w;
-                ld_elt(w, stw + (size_t)(j << s) * 8);
-                fe_mul(v, v, w);
-            }
-            st_elt(p0, t);
-            st_elt(p1, v);
+        if (per) {
+            const int b0 = (int)(threadIdx.x >> 5) * per * 32 + (int)(threadIdx.x & 31);
+            for (int k = 0; k < per; ++k) butterfly(s, log_half, b0 + 32 * k);
+        } else {
+            for (int b = threadIdx.x; b < half_total; b += blockDim.x) butterfly(s, log_half, b);
         }
-        // From half-length 32 down, the 32 butterflies of a warp (32
-        // consecutive b, block size a multiple of 32) touch only their own 64
-        // consecutive elements of one sub-vector (or whole sub-vectors when
-        // R <= 32), at this stage and the next: the warp alone consumes what
-        // it wrote, so only the warp synchronises; every other stage, and the
-        // last (the store reads any element), synchronise the block.
-        if (log_half <= 5 && s + 1 < a.log_R)
+        if (log_half <= (per ? log_local : 5) && s + 1 < a.log_R)
             __syncwarp();
         else
             __syncthreads();
