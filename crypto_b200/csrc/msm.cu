@@ -240,9 +240,11 @@ __global__ void k_scatter(const uint32_t* __restrict__ keys, const uint32_t* __r
 
 // k_scatter over the entries of scalar rows [lo, lo + len) of one MSM of n
 // scalars (slots g * n + j, as k_rank_rows).
+// offsets is indexed by key + shift (the pipeline's chunk c keeps its B + 1
+// offsets at c (B + 1), its keys being c B .. c B + B - 1: shift = c).
 __global__ void k_scatter_rows(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                                const uint32_t* __restrict__ ranks, uint32_t n, uint32_t G, uint32_t lo,
-                               uint32_t len, const uint32_t* __restrict__ offsets,
+                               uint32_t len, const uint32_t* __restrict__ offsets, uint32_t shift,
                                uint32_t* __restrict__ sorted) {
     const unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (unsigned long long)G * len) return;
@@ -250,12 +252,13 @@ __global__ void k_scatter_rows(const uint32_t* __restrict__ keys, const uint32_t
     const unsigned long long slot = (unsigned long long)g * n + j;
     const uint32_t key = keys[slot];
     if (key == KEY_SENTINEL) return;
-    sorted[offsets[key] + ranks[slot]] = vals[slot];
+    sorted[offsets[key + shift] + ranks[slot]] = vals[slot];
 }
 
 // Host-input pipeline, level 1 after the per-chunk first level: chunk c's
-// first-level sums of bucket b sit at rows off[c B + b] .. + ceil(len / 2)
-// (the sub-run's own entry positions).  tot[b] = the bucket's sums over the
+// offsets are off[c (B + 1) + b], b <= B, and its first-level sums of
+// bucket b sit at rows off[c (B + 1) + b] .. + ceil(len / 2) (the sub-run's
+// own entry positions).  tot[b] = the bucket's sums over the
 // chunks; idx lists them bucket by bucket (chunk by chunk inside a bucket),
 // so level 1 reads ordinary bucket runs through idx.
 __global__ void k_l1_totals(const uint32_t* __restrict__ off, uint32_t B, uint32_t CH,
@@ -263,7 +266,8 @@ __global__ void k_l1_totals(const uint32_t* __restrict__ off, uint32_t B, uint32
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= B) return;
     uint32_t s = 0;
-    for (uint32_t c = 0; c < CH; ++c) s += (off[(size_t)c * B + b + 1] - off[(size_t)c * B + b] + 1) >> 1;
+    for (uint32_t c = 0; c < CH; ++c)
+        s += (off[(size_t)c * (B + 1) + b + 1] - off[(size_t)c * (B + 1) + b] + 1) >> 1;
     tot[b] = s;
 }
 
@@ -288,8 +292,8 @@ __global__ void k_l1_index(const uint32_t* __restrict__ off, const uint32_t* __r
         while (in1[b + 1] <= s) ++b;
         uint32_t p = s - in1[b];
         for (uint32_t c = 0; c < CH; ++c) {
-            const uint32_t o = off[(size_t)c * B + b];
-            const uint32_t cnt = (off[(size_t)c * B + b + 1] - o + 1) >> 1;
+            const uint32_t o = off[(size_t)c * (B + 1) + b];
+            const uint32_t cnt = (off[(size_t)c * (B + 1) + b + 1] - o + 1) >> 1;
             if (p < cnt) {
                 idx[s] = o + p;
                 break;
@@ -842,13 +846,16 @@ class MsmEngine {
     // first pairing level pays its own inversion tree and launches).
     static constexpr int HOST_CHUNKS_MAX = 8;
     static constexpr int HOST_CHUNKS = 4;
-    cudaStream_t st_copy = nullptr, st_conv = nullptr;
+    cudaStream_t st_copy = nullptr, st_conv = nullptr, st_sort = nullptr;
     cudaEvent_t ev_start = nullptr, ev_chunk[HOST_CHUNKS_MAX] = {}, ev_conv[HOST_CHUNKS_MAX] = {},
-                ev_scal[HOST_CHUNKS_MAX] = {};
+                ev_scal[HOST_CHUNKS_MAX] = {}, ev_sorted[HOST_CHUNKS_MAX] = {}, ev_fork = nullptr;
     void host_streams() {
         if (st_copy) return;
         KB_CUDA(cudaStreamCreateWithFlags(&st_copy, cudaStreamNonBlocking));
         KB_CUDA(cudaStreamCreateWithFlags(&st_conv, cudaStreamNonBlocking));
+        KB_CUDA(cudaStreamCreateWithFlags(&st_sort, cudaStreamNonBlocking));
+        KB_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        for (auto& c : ev_sorted) KB_CUDA(cudaEventCreateWithFlags(&c, cudaEventDisableTiming));
         KB_CUDA(cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming));
         for (auto& c : ev_chunk) KB_CUDA(cudaEventCreateWithFlags(&c, cudaEventDisableTiming));
         for (auto& c : ev_conv) KB_CUDA(cudaEventCreateWithFlags(&c, cudaEventDisableTiming));
@@ -874,6 +881,9 @@ class MsmEngine {
             for (auto& c : ev_chunk) cudaEventDestroy(c);
             for (auto& c : ev_conv) cudaEventDestroy(c);
             for (auto& c : ev_scal) cudaEventDestroy(c);
+            cudaStreamDestroy(st_sort);
+            cudaEventDestroy(ev_fork);
+            for (auto& c : ev_sorted) cudaEventDestroy(c);
         }
         for (DevBuf* b : {&table, &keys, &vals, &counts, &offsets, &cursor, &sorted, &rec_first,
                           &rec_last, &fold_buf, &buckets, &blk_out, &win_out, &win_done, &l1_idx,
@@ -940,7 +950,8 @@ void msm_engine_reserve(MsmEngine* e, const MsmBatchPlan* p, cudaStream_t st) {
     e->ranks.reserve(L * 4, st);
     const size_t BS = std::max<size_t>(P.B, P.B_sort);
     e->counts.reserve((BS + 1) * 4, st);
-    e->offsets.reserve((BS + 1) * 4, st);
+    // the host-input pipeline keeps each row chunk's B + 1 offsets apart
+    e->offsets.reserve(std::max(BS + 1, (size_t)P.chunks * ((size_t)P.B + 1) + 1) * 4, st);
     e->cursor.reserve((BS + 1) * 4, st);
     const size_t nch = std::max<size_t>(1, P.nchunks);
     e->rec_first.reserve(nch * PW * 4, st);
@@ -1038,42 +1049,55 @@ void msm_engine_launch(MsmEngine* e, const MsmBatchPlan* p, const uint8_t* d_sca
                            P.items[0].chunk_stride == P.B;
     if (by_rows) {
         const size_t G = P.L / n0, S = S_rows;
+        // pipelined: the chunks' sorts run on a stream of their own, so chunk
+        // c + 1 sorts while chunk c pairs
+        cudaStream_t ss = st;
+        if (pipelined) {
+            e->host_streams();
+            ss = e->st_sort;
+            KB_CUDA(cudaEventRecord(e->ev_fork, st));
+            KB_CUDA(cudaStreamWaitEvent(ss, e->ev_fork, 0));
+        }
         for (int c = 0; c < n_ready; ++c) {
             const size_t lo = std::min(n0, (size_t)c * S), hi = std::min(n0, lo + S);
-            KB_CUDA(cudaStreamWaitEvent(st, scalars_ready[c], 0));
+            KB_CUDA(cudaStreamWaitEvent(ss, scalars_ready[c], 0));
             if (hi == lo && !pipelined) continue;
             K.recode(items, nitems, lo, hi - lo, scal, rec_table, e->keys.as<uint32_t>(),
-                     e->vals.as<uint32_t>(), st);
+                     e->vals.as<uint32_t>(), ss);
             if (tiled) {
-                k_rank_tiles<<<dim3(rt.G * rt.Q, 1), RANK_TILE_THREADS, tile_smem, st>>>(
+                k_rank_tiles<<<dim3(rt.G * rt.Q, 1), RANK_TILE_THREADS, tile_smem, ss>>>(
                     e->keys.as<uint32_t>(), rt, (uint32_t)c, e->counts.as<uint32_t>(),
                     e->ranks.as<uint32_t>());
             } else if (hi > lo) {
-                k_rank_rows<<<ceil_div_u(G * (hi - lo), 256), 256, 0, st>>>(
+                k_rank_rows<<<ceil_div_u(G * (hi - lo), 256), 256, 0, ss>>>(
                     e->keys.as<uint32_t>(), (uint32_t)n0, (uint32_t)G, (uint32_t)lo,
                     (uint32_t)(hi - lo), e->counts.as<uint32_t>(), e->ranks.as<uint32_t>());
             }
             KB_LAUNCH_CHECK();
             if (!pipelined) continue;
-            // chunk c: bucket offsets (keys c B .. c B + B - 1) from the
-            // previous chunk's total, scatter, first pairing level
+            // chunk c: bucket offsets (keys c B .. c B + B - 1, kept at
+            // c (B + 1) so that no word is shared with the chunk pairing
+            // meanwhile) from the previous chunk's total, scatter, first
+            // pairing level
             const uint32_t B = P.B;
-            uint32_t* offs = e->offsets.as<uint32_t>() + (size_t)c * B;
+            uint32_t* offs = e->offsets.as<uint32_t>() + (size_t)c * (B + 1);
             uint32_t* cnt = e->counts.as<uint32_t>() + (size_t)c * B;
             uint32_t* bases = e->chunk_base.as<uint32_t>();
             exclusive_scan_u32_chained(cnt, offs, B, 0, c ? bases + c : nullptr, bases + c + 1,
-                                       e->scan_tmp.as<uint32_t>(), st);
+                                       e->scan_tmp.as<uint32_t>(), ss);
             if (hi > lo) {
-                k_scatter_rows<<<ceil_div_u(G * (hi - lo), 256), 256, 0, st>>>(
+                k_scatter_rows<<<ceil_div_u(G * (hi - lo), 256), 256, 0, ss>>>(
                     e->keys.as<uint32_t>(), e->vals.as<uint32_t>(), e->ranks.as<uint32_t>(),
                     (uint32_t)n0, (uint32_t)G, (uint32_t)lo, (uint32_t)(hi - lo),
-                    e->offsets.as<uint32_t>(), e->sorted.as<uint32_t>());
+                    e->offsets.as<uint32_t>(), (uint32_t)c, e->sorted.as<uint32_t>());
                 KB_LAUNCH_CHECK();
             }
             uint32_t* out0 = e->pair_off[0].as<uint32_t>() + (size_t)c * (B + 1);
-            k_pair_counts<<<ceil_div_u(B, 256), 256, 0, st>>>(offs, B, cnt);
+            k_pair_counts<<<ceil_div_u(B, 256), 256, 0, ss>>>(offs, B, cnt);
             KB_LAUNCH_CHECK();
-            exclusive_scan_u32(cnt, out0, B, 0, e->scan_tmp.as<uint32_t>(), st);
+            exclusive_scan_u32(cnt, out0, B, 0, e->scan_tmp.as<uint32_t>(), ss);
+            KB_CUDA(cudaEventRecord(e->ev_sorted[c], ss));
+            KB_CUDA(cudaStreamWaitEvent(st, e->ev_sorted[c], 0));
             KB_CUDA(cudaStreamWaitEvent(st, table_ready[c], 0));
             PairArgs pa;
             pa.in_off = offs;
