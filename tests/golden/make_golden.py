@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import gzip
 import json
+import os
 import random
 import sys
 from pathlib import Path
@@ -108,7 +109,9 @@ def kzg_cases(rng: random.Random) -> list[dict]:
 
 CYC_Q, CYC_ROOT = 998244353, 629671588
 GOLD_Q = 0xFFFFFFFF00000001
-KAT = Path("/root/reference/ntt/test/vectors/ntt_kat.json")
+# the reference tree: KINET_REFERENCE, else where the oracle's Makefile looks (REF ?=)
+REF_ROOT = Path(os.environ.get("KINET_REFERENCE", "/root/reference"))
+KAT = REF_ROOT / "ntt/test/vectors/ntt_kat.json"
 
 
 def word_ntt_inputs(seed: int, n: int, q: int, canonical: bool):
